@@ -1,0 +1,336 @@
+"""Generates the golden fixtures of tests/golden/ by running the reference itself (FP64, CPU).
+
+Run in a container that holds the reference checkout (default /root/reference, or $LPM_REFERENCE):
+
+    python tests/golden/make_golden.py            # all parts, each in a fresh interpreter
+
+The reference is imported read-only: Numba's cache goes to a temporary directory, and the two modules that create
+folders inside the reference tree at import time (timing/t2d/a2common.py, timing/t3d/common.py) are replaced by stubs.
+Parts:
+  sc     3D simple-cubic: the arrays of coarse3d/dev/export_check.py (n = 12, seed 5), SuperLU block means for
+         s = 2, 3 and the 9 loads, PCG / plain-CG iteration counts, masked-lattice connectivity, BCs, generators
+  sq     2D square: timing/t2d/solver2d.py kernels, cg2plain / pcg_mf solves, SuperLU, masked connectivity, BCs
+  grad   gradients: torch_lpm3d autograd of lam . K u, LinSolve through CoarseT.run (as coarse3d/check_torch3d.py),
+         torch_lpm dense-assembly gradient of lam^T K u and of the CoarseT.run losses (as coarse2d/check_gradient.py)
+"""
+import os
+import subprocess
+import sys
+import tempfile
+import types
+
+REF = os.environ.get("LPM_REFERENCE", "/root/reference")
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _env():
+    os.environ["NUMBA_CACHE_DIR"] = os.path.join(tempfile.gettempdir(), "lpm_golden_numba")
+    os.environ.setdefault("NUMBA_NUM_THREADS", "8")
+    sys.dont_write_bytecode = True
+
+
+def _stub(name):
+    sys.modules[name] = types.ModuleType(name)
+
+
+def part_sc():
+    _env()
+    sys.path.insert(0, os.path.join(REF, "coarse3d"))
+    import numpy as np
+    import geom3d as G
+    import lin3d as L3
+    import micro3d
+    sys.path.insert(0, os.path.join(REF, "timing", "t3d"))
+    _stub("common")
+    from cgplain import cg3
+
+    out = {}
+    # ---- export_check.py arrays (n = 12, rng(5)) ----
+    n = 12
+    rng = np.random.default_rng(5)
+    ph, E, nu, info = micro3d.sample(n, rng)
+    lat = L3.Lattice3D(n, n, n, 1.0)
+    C = G.iso_C(E, nu)
+    Kn, Tv = G.bond_params_two_end_mean(lat, G.sc_params_from_C(C, 0.5))
+    u = rng.standard_normal((lat.N, 3))
+    out.update(phase=ph.astype(np.int8), E=E, nu=nu, Kn=Kn, Tv=Tv, u=u, Ku=lat.apply(u, Kn, Tv),
+               st=lat.stress(u, Kn, Tv), U=lat.energy_per_particle(u, Kn, Tv), D=lat.block_diag(Kn, Tv),
+               nbr=lat.nbr.astype(np.int32))
+    dL, F = lat.bond_forces(u, Kn, Tv)
+    out.update(F_row=F[::97], dL_row=dL[::97])
+    K = lat.stiffness(Kn, Tv)
+    for s in (2, 3):
+        nc = n // s
+        IJK = lat.ijk // s
+        cid = G.block_index(lat.ijk, s, (nc,) * 3)
+        for ld in G.LOADS:
+            fixed, up, mov = G.prescribed(ld, lat.x, IJK, (nc,) * 3, s)
+            uu, _ = L3.solve_direct(K, fixed, up)
+            st = lat.stress(uu, Kn, Tv)
+            out["u_%d_%s" % (s, ld)] = np.stack([np.bincount(cid, uu[:, k]) for k in range(3)], 1) / s ** 3
+            out["s_%d_%s" % (s, ld)] = np.stack([np.bincount(cid, st[:, k]) for k in range(6)], 1) / s ** 3
+            out["w_%d_%s" % (s, ld)] = np.bincount(cid, lat.energy_per_particle(uu, Kn, Tv)) / s ** 3
+            P = lat.apply(uu, Kn, Tv)
+            out["F_%d_%s" % (s, ld)] = P[mov, G.GDIR[ld]].sum() if mov is not None else 0.0
+            if (s, ld) in ((2, "k_xx"), (3, "tb_tz"), (2, "lr_tx")):
+                out["ufull_%d_%s" % (s, ld)] = uu
+    # ---- iterative solvers on (s = 2, k_xx) and (s = 2, tb_sx) ----
+    for ld in ("k_xx", "tb_sx"):
+        fixed, up, _ = G.prescribed(ld, lat.x, lat.ijk // 2, (6,) * 3, 2)
+        u_p, info_p = L3.solve_pcg(lat, Kn, Tv, fixed, up, tol=1e-8)
+        out["pcg_u_%s" % ld] = u_p
+        out["pcg_it_%s" % ld] = info_p["iters"]
+        out["pcg_rel_%s" % ld] = info_p["relres"]
+        free = ~fixed
+        upm = np.zeros((lat.N, 3))
+        upm[fixed] = up[fixed]
+        b = -L3.k_apply(upm, lat.nbr, lat.ndir, Kn, Tv)
+        b[fixed] = 0.0
+        x = np.zeros((lat.N, 3))
+        it, rr = cg3(lat.nbr, lat.ndir, Kn, Tv, free, b, x, 1e-8, 200000)
+        out["cg_u_%s" % ld] = upm + x
+        out["cg_it_%s" % ld] = int(it)
+        out["cg_rel_%s" % ld] = float(rr)
+    # ---- masked lattice connectivity ----
+    mrng = np.random.default_rng(11)
+    act = mrng.random(7 * 5 * 4) < 0.7
+    lm = G.LatticeGeom(7, 5, 4, 1.5, origin=(0.1, -0.2, 0.3), active=act)
+    out.update(m_active=act, m_nbr=lm.nbr.astype(np.int32), m_ijk=lm.ijk.astype(np.int32), m_x=lm.x,
+               m_site_of=lm.site_of.astype(np.int32), m_nb_initial=lm.nb_initial.astype(np.int32))
+    # ---- BCs on a 6^3 lattice, s = 2 ----
+    lb = G.LatticeGeom(6, 6, 6, 1.0)
+    for ld in G.LOADS:
+        fixed, up, mov = G.prescribed(ld, lb.x, lb.ijk // 2, (3, 3, 3), 2)
+        out["bc_fixed_%s" % ld] = fixed
+        out["bc_up_%s" % ld] = up
+        out["bc_mov_%s" % ld] = np.zeros(lb.N, bool) if mov is None else mov
+    # ---- material maps ----
+    cpr = np.random.default_rng(3)
+    C66 = cpr.standard_normal((5, 6, 6))
+    out["cp_C66"] = C66
+    out["cp_params"] = G.cell_params_from_C66(C66, 0.7)
+    # ---- generators ----
+    out["gen_spheres"] = micro3d.spheres(16, 16, 16, 0.25, 4.0, np.random.default_rng(7), rjit=0.0)[0].astype(np.int8)
+    out["gen_ellip"] = micro3d.ellipsoids(16, 16, 16, 0.3, 3.0, np.random.default_rng(8), aspect=(3.0, 3.0),
+                                          rjit=0.0)[0].astype(np.int8)
+    out["gen_grf3"] = micro3d.grf(12, 12, 12, 2.0, 0.3, np.random.default_rng(9))[0].astype(np.int8)
+    np.savez_compressed(os.path.join(HERE, "golden_sc.npz"), **out)
+    print("golden_sc.npz:", len(out), "arrays")
+
+
+def part_sq():
+    _env()
+    sys.path.insert(0, os.path.join(REF, "timing", "t2d"))
+    _stub("a2common")
+    import numpy as np
+    import lin2d
+    import micro
+    import solver2d as S2
+    from cg2plain import cg_mf
+
+    out = {}
+    nx, ny = 16, 12
+    lat = lin2d.Lattice2D("square", nx, ny, 1.0)
+    ph = micro.grf_two_phase(nx, ny, 3.0, 0.3, 4)
+    E = np.where(ph == 1, 10.0, 1.0)
+    Cpix = lin2d.iso_C(E, 0.25, plane="stress")
+    Kn, Tv = lin2d.bond_params_two_end_mean(lat, lin2d.square_params_from_C(Cpix))
+    rng = np.random.default_rng(21)
+    # non-symmetric per-slot parameters: the g-form kernel is the exact Hessian for any values
+    Kn_ns = Kn * (1 + 0.2 * rng.random(Kn.shape)) * lat.valid
+    Tv_ns = Tv * (1 + 0.2 * rng.random(Tv.shape)) * lat.valid
+    u = rng.standard_normal(2 * lat.N)
+    arr = (np.where(lat.valid, lat.nbr, 0).astype(np.int64), lat.valid, np.ascontiguousarray(lat.ndir),
+           lat.shell.astype(np.int64), lat.opp.astype(np.int64))
+    g = np.empty((lat.N, 8))
+    f = np.empty(2 * lat.N)
+    S2._kmv(u, *arr, Kn_ns, Tv_ns, g, f)
+    K, _, _ = lat.stiffness(Kn_ns, Tv_ns)
+    out.update(phase=ph.astype(np.int8), Kn=Kn, Tv=Tv, Kn_ns=Kn_ns, Tv_ns=Tv_ns, u=u, f_ns=f, Ku_csr_ns=K @ u,
+               nbr=lat.nbr.astype(np.int32))
+    fixed_p = np.zeros(lat.N, bool)
+    fixed_p[lat.ij[:, 0] == 0] = True
+    Binv = np.empty((lat.N, 2, 2))
+    S2._diag_inv(*arr, Kn, Tv, fixed_p, Binv)
+    out.update(diag_fixed=fixed_p, Binv=Binv)
+    out["stress"] = S2.stress(lat, u, Kn, Tv)
+    out["energy"] = lat.energy_per_particle(u, Kn, Tv)
+    # ---- per-DOF uniaxial tension, plain CG (cg2plain) and pcg_mf, SuperLU ----
+    fd = np.zeros((lat.N, 2), bool)
+    up = np.zeros((lat.N, 2))
+    left, right = lat.ij[:, 0] == 0, lat.ij[:, 0] == nx - 1
+    fd[left, 0] = fd[right, 0] = True
+    fd[left & (lat.ij[:, 1] == 0), 1] = True
+    up[right, 0] = 1e-3 * (nx - 1)
+    mask = (~fd).astype(np.float64).ravel()
+    ub = up.ravel()
+    fk = np.empty(2 * lat.N)
+    S2._kmv(ub, *arr, Kn, Tv, g, fk)
+    b = -fk * mask
+    x = np.zeros(2 * lat.N)
+    it = cg_mf(*arr, Kn, Tv, mask, b, x, 1e-10, 200000, g)
+    out.update(cg_fixed=fd, cg_up=up, cg_u=x + ub, cg_it=int(it))
+    Ks, _, _ = lat.stiffness(Kn, Tv)
+    fdofs = np.nonzero(fd.ravel())[0]
+    usol, _ = lin2d.solve_disp(Ks, fdofs, ub[fdofs])
+    out["lu_u"] = usol
+    # pcg_mf on a particle-fixed problem (left column clamped, right column pulled)
+    fixed = left | right
+    mask_p = np.repeat((~fixed).astype(np.float64), 2)
+    ub2 = np.zeros((lat.N, 2))
+    ub2[right, 0] = 1e-3 * (nx - 1)
+    ub2 = ub2.ravel()
+    S2._kmv(ub2, *arr, Kn, Tv, g, fk)
+    b2 = -fk * mask_p
+    B2 = np.empty((lat.N, 2, 2))
+    S2._diag_inv(*arr, Kn, Tv, fixed, B2)
+    x2 = np.zeros(2 * lat.N)
+    snaps = np.empty((1, 2 * lat.N))
+    iters = np.zeros(1, np.int64)
+    S2.pcg_mf(*arr, Kn, Tv, B2, mask_p, b2, x2, np.array([1e-10]), 20000, snaps, iters, g)
+    out.update(pcg_fixed=fixed, pcg_up=ub2.reshape(-1, 2), pcg_u=snaps[0] + ub2, pcg_it=int(iters[0]))
+    # ---- masked connectivity ----
+    mrng = np.random.default_rng(12)
+    act = mrng.random(9 * 7) < 0.65
+    lm = lin2d.Lattice2D("square", 9, 7, 0.5, origin=(0.3, 0.1), active=act)
+    out.update(m_active=act, m_nbr=lm.nbr.astype(np.int32), m_ij=lm.ij.astype(np.int32), m_x=lm.x)
+    # ---- BCs (el_prob / torch_lpm convention, L = 1 and 2) ----
+    import el_prob as EP
+    lb = lin2d.Lattice2D("square", 8, 8, 1.0)
+    for L in (1, 2):
+        for ld in EP.LOADS:
+            fixed, upb, mov = EP.prescribed(ld, lb.x, lb.ij // 2, 4, 4, 2, 1.0, L)
+            out["bc_fixed_%d_%s" % (L, ld)] = fixed
+            out["bc_up_%d_%s" % (L, ld)] = upb
+    # ---- generators ----
+    out["gen_grf"] = micro.grf_two_phase(40, 32, 6.0, 0.30, 3).astype(np.int8)
+    np.savez_compressed(os.path.join(HERE, "golden_sq.npz"), **out)
+    print("golden_sq.npz:", len(out), "arrays")
+
+
+def part_grad():
+    _env()
+    sys.path.insert(0, os.path.join(REF, "coarse3d"))
+    import numpy as np
+    import torch
+    import geom3d as G
+    import torch_lpm3d as T3
+    torch.set_default_dtype(torch.float64)
+    out = {}
+    # ---- 3D: autograd of lam . apply(u; Kn, Tv) on a coarse 4^3 lattice with symmetric random bonds ----
+    nc, s = 4, 2
+    lat = G.LatticeGeom(nc, nc, nc, s)
+    rng = np.random.default_rng(1)
+    Kn0 = np.zeros((lat.N, 18))
+    Tv0 = np.zeros((lat.N, 18))
+    for i in range(lat.N):
+        for k in range(0, 18, 2):
+            q = lat.nbr[i, k]
+            if q >= 0:
+                Kn0[i, k] = Kn0[q, k ^ 1] = rng.uniform(0.8, 1.2)
+                Tv0[i, k] = Tv0[q, k ^ 1] = rng.uniform(-0.03, 0.03)
+    op = T3.SCT(lat, "cpu")
+    u = rng.standard_normal((lat.N, 3))
+    lam = rng.standard_normal((lat.N, 3))
+    Kt = torch.tensor(Kn0, requires_grad=True)
+    Tt = torch.tensor(Tv0, requires_grad=True)
+    e = (torch.tensor(lam) * op.apply(torch.tensor(u), Kt, Tt)).sum()
+    gK, gT = torch.autograd.grad(e, (Kt, Tt))
+    out.update(g3_Kn=Kn0, g3_Tv=Tv0, g3_u=u, g3_lam=lam, g3_gK=gK.numpy(), g3_gT=gT.numpy())
+    # non-symmetric parameters too (the closed form does not assume symmetry)
+    Kns = Kn0 * (1 + 0.3 * rng.random(Kn0.shape))
+    Tvs = Tv0 + 0.01 * rng.standard_normal(Tv0.shape) * lat.valid
+    Kt = torch.tensor(Kns, requires_grad=True)
+    Tt = torch.tensor(Tvs, requires_grad=True)
+    e = (torch.tensor(lam) * op.apply(torch.tensor(u), Kt, Tt)).sum()
+    gK, gT = torch.autograd.grad(e, (Kt, Tt))
+    out.update(g3n_Kn=Kns, g3n_Tv=Tvs, g3n_gK=gK.numpy(), g3n_gT=gT.numpy())
+    # ---- 3D: full differentiable coarse solve (LinSolve through CoarseT.run), 9 loads, tol 1e-13 ----
+    cm = T3.CoarseT(nc, s, device="cpu")
+    torch.manual_seed(0)
+    Wsig = torch.randn(1, len(G.LOADS), lat.N, 6)
+    Wu = torch.randn(1, len(G.LOADS), lat.N, 3)
+    kn = torch.tensor(Kn0)[None].requires_grad_(True)
+    tv = torch.tensor(Tv0)[None].requires_grad_(True)
+    o = cm.run(kn, tv, tol=1e-13)
+    L = (o["sig"] * Wsig).sum() + 1e3 * (o["u"] * Wu).sum() + o["F"].sum() + o["w"].sum()
+    L.backward()
+    out.update(c3_Wsig=Wsig.numpy(), c3_Wu=Wu.numpy(), c3_loss=float(L), c3_gK=kn.grad.numpy()[0],
+               c3_gT=tv.grad.numpy()[0], c3_u=o["u"].detach().numpy()[0], c3_sig=o["sig"].detach().numpy()[0],
+               c3_w=o["w"].detach().numpy()[0], c3_F=o["F"].detach().numpy()[0])
+    # fine reference on the n = 6 box (s = 2), PCG tol 1e-12
+    fr = T3.FineRefT(6, 2, device="cpu")
+    rf = np.random.default_rng(2)
+    Knf = np.zeros((fr.lat.N, 18))
+    Tvf = np.zeros((fr.lat.N, 18))
+    for i in range(fr.lat.N):
+        for k in range(0, 18, 2):
+            q = fr.lat.nbr[i, k]
+            if q >= 0:
+                Knf[i, k] = Knf[q, k ^ 1] = rf.uniform(0.5, 1.5)
+                Tvf[i, k] = Tvf[q, k ^ 1] = rf.uniform(-0.05, 0.05)
+    r = fr.run(torch.tensor(Knf)[None], torch.tensor(Tvf)[None], tol=1e-12)
+    out.update(f3_Kn=Knf, f3_Tv=Tvf, f3_u=r["u"].numpy()[0], f3_sig=r["sig"].numpy()[0], f3_w=r["w"].numpy()[0],
+               f3_F=r["F"].numpy()[0])
+
+    # ---- 2D: torch_lpm dense assembly ----
+    sys.path.insert(0, os.path.join(REF, "coarse2d"))
+    import torch_lpm as T2
+    m = T2.CoarseT(6, 5, 2, device="cpu")
+    lat2 = m.lat
+    N = lat2.N
+    r2 = np.random.default_rng(0)
+    Kn2 = np.where(lat2.shell[None, :] == 0, 0.38, 0.19) * (1 + 0.3 * r2.random((N, 8)))
+    Kn2 = Kn2 * lat2.valid
+    Tv2 = (0.03 + 0.01 * r2.standard_normal((N, 8))) * lat2.valid
+    u2 = r2.standard_normal(2 * N)
+    l2 = r2.standard_normal(2 * N)
+    Kt = torch.tensor(Kn2, requires_grad=True)
+    Tt = torch.tensor(Tv2, requires_grad=True)
+    Kd = m.assemble(Kt[None], Tt[None])[0]
+    e = torch.tensor(l2) @ (Kd @ torch.tensor(u2))
+    gK, gT = torch.autograd.grad(e, (Kt, Tt))
+    out.update(g2_Kn=Kn2, g2_Tv=Tv2, g2_u=u2, g2_lam=l2, g2_gK=gK.numpy(), g2_gT=gT.numpy(),
+               g2_Ku=(Kd @ torch.tensor(u2)).detach().numpy())
+    # full CoarseT.run + losses gradient (check_gradient.py style; nc = 8, s = 2, B = 2)
+    m8 = T2.CoarseT(8, 8, 2, device="cpu")
+    lat8 = m8.lat
+    N8 = lat8.N
+    r8 = np.random.default_rng(0)
+    B = 2
+    K0 = np.where(lat8.shell[None, None, :] == 0, 0.38, 0.19) * (1 + 0.3 * r8.random((B, N8, 8)))
+    q = np.where(lat8.valid, lat8.nbr, 0)
+    opp = lat8.opp[None, :].repeat(N8, 0)
+    K0 = 0.5 * (K0 + K0[:, q, opp]) * lat8.valid
+    T0 = np.full((B, N8, 8), 0.03) * lat8.valid
+    ref = m8.run(torch.tensor(K0) * 1.1, torch.tensor(T0))
+    ref = {k: {kk: (vv.detach() if vv is not None else None) for kk, vv in v.items()} for k, v in ref.items()}
+    th = torch.tensor(0.1 * r8.standard_normal((B, N8, 8)), requires_grad=True)
+    qt = torch.as_tensor(q)
+    ot = torch.as_tensor(opp)
+    Kn8 = torch.tensor(K0) * torch.exp(0.5 * (th + th[:, qt, ot]))
+    Tv8 = torch.tensor(T0)
+    o8 = m8.run(Kn8, Tv8)
+    a, b_, c = T2.losses(m8, o8, ref)
+    Lg = (a + b_ + c).sum()
+    Lg.backward()
+    out.update(c2_K0=K0, c2_T0=T0, c2_th=th.detach().numpy(), c2_loss=float(Lg), c2_gth=th.grad.numpy())
+    for ld in T2.LOADS:
+        out["c2_u_%s" % ld] = o8[ld]["u"].detach().numpy()
+        out["c2_sig_%s" % ld] = o8[ld]["sig"].detach().numpy()
+        out["c2_w_%s" % ld] = o8[ld]["w"].detach().numpy()
+        if o8[ld]["F"] is not None:
+            out["c2_F_%s" % ld] = o8[ld]["F"].detach().numpy()
+        out["c2_refu_%s" % ld] = ref[ld]["u"].numpy()
+    np.savez_compressed(os.path.join(HERE, "golden_grad.npz"), **out)
+    print("golden_grad.npz:", len(out), "arrays")
+
+
+PARTS = {"sc": part_sc, "sq": part_sq, "grad": part_grad}
+
+if __name__ == "__main__":
+    if len(sys.argv) > 1 and sys.argv[1] in PARTS:
+        PARTS[sys.argv[1]]()
+    else:
+        for p in PARTS:
+            subprocess.run([sys.executable, os.path.abspath(__file__), p], check=True)
