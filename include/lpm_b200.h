@@ -1,0 +1,186 @@
+/*
+ * lpm_b200.h -- C ABI of the B200 LPM linear-solve library (liblpm_b200.so).
+ *
+ * Matrix-free K.u of the linearised lattice particle model on the square (2D, 8 slots, 2 DOF) and simple-cubic (3D,
+ * 18 slots, 3 DOF) lattices, batched CG / block-Jacobi PCG, FP32-inner / FP64-refinement solves, per-bond adjoint
+ * gradients and stress / energy post-processing.
+ *
+ * Conventions
+ *  - Every array argument is a DEVICE pointer owned by the caller (e.g. the data_ptr() of a torch tensor).  No entry
+ *    point allocates device memory; scratch and workspace buffers are passed in, sized by the *_bytes queries.
+ *  - Functions return 0 on success, a negative LPM_ERR_* code for a bad argument, or a positive cudaError_t value.
+ *  - Work is enqueued on `stream` (a cudaStream_t; NULL = legacy default stream).  Solver entry points synchronise
+ *    the stream every `poll` iterations to read one convergence counter; all other entry points are asynchronous.
+ *  - No global mutable state: calls on distinct streams with distinct buffers are thread-safe.
+ *  - Slot order, bond directions and particle numbering are those of the reference (coarse3d/geom3d.py:16-65,
+ *    coarse2d/lin2d.py:21-74): slots in reverse pairs (k, k^1), shell 0 = axial bonds, n_k = -o_k/|o_k|.
+ *  - Batches: nsys systems (right-hand sides); system s uses coefficient set s / rhs_per_set and DOF mask s % nmask.
+ *    Vectors are (nsys, n, d) contiguous; coefficient sets (nset, n, slots) in the reference layout
+ *    (LPM_LAYOUT_REF) or (nset, slots, n) packed (LPM_LAYOUT_SOA); masks (nmask, n, d) uint8, 1 = free DOF.
+ */
+#ifndef LPM_B200_H
+#define LPM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LPM_ABI_VERSION 1
+
+/* return codes */
+#define LPM_OK 0
+#define LPM_ERR_ARG (-1)         /* invalid argument (null pointer, bad size, unsupported combination) */
+#define LPM_ERR_WORKSPACE (-2)   /* workspace / scratch buffer too small */
+#define LPM_ERR_UNSUPPORTED (-3) /* lattice or precision not supported by this entry point */
+
+/* per-system solver status */
+#define LPM_STATUS_OK 0
+#define LPM_STATUS_NOT_CONVERGED 1 /* maxit reached (mirrors lin3d._pcg returning maxit, solver2d's iters = -1) */
+#define LPM_STATUS_BREAKDOWN 2     /* p.Ap < 0 or a non-finite scalar (mirrors torch_lpm's FloatingPointError) */
+
+/* precisions and coefficient layouts */
+#define LPM_F64 0
+#define LPM_F32 1
+#define LPM_LAYOUT_REF 0 /* (nset, n, slots): the reference's Kn / Tv arrays */
+#define LPM_LAYOUT_SOA 1 /* (nset, slots, n): packed by lpm_pack_coef_* */
+
+typedef struct lpm_lattice {
+    int32_t dim;        /* 2: square lattice, 3: simple cubic */
+    int32_t nx, ny, nz; /* box size in sites (nz = 1 in 2D) */
+    int64_t n;          /* number of particles (= nx*ny*nz for a full box) */
+    const int32_t* nbr; /* NULL: full box, implicit neighbours.  Else (n, slots) int32 table, -1 = no bond. */
+} lpm_lattice;
+
+typedef struct lpm_batch {
+    int32_t nsys;        /* systems (right-hand sides) */
+    int32_t rhs_per_set; /* consecutive systems sharing one coefficient set */
+    int32_t nmask;       /* number of DOF masks; system s uses mask s % nmask */
+    int32_t reserved;
+} lpm_batch;
+
+typedef struct lpm_cg_opts {
+    double tol;       /* stop a system when |r| <= tol |b| */
+    int32_t maxit;    /* iteration limit */
+    int32_t check;    /* convergence test every `check` iterations (1 = lin3d._pcg, 10 = torch_lpm3d.SCT.pcg) */
+    int32_t poll;     /* host reads the converged count every `poll` iterations */
+    int32_t precheck; /* 1: test the initial residual before iterating (cg2plain.cg_mf / solver2d.pcg_mf) */
+    double* prof;     /* optional HOST array of 4: K.u ms / launches, and the same for full-batch launches */
+} lpm_cg_opts;
+
+typedef struct lpm_ir_opts {
+    double tol;          /* FP64 true relative residual target |b - Kx| <= tol |b| */
+    double inner_tol;    /* relative tolerance of each FP32 correction solve */
+    int32_t maxit;       /* limit on the total inner iterations per system */
+    int32_t max_outer;   /* limit on refinement steps */
+    int32_t check;       /* inner convergence-test interval */
+    int32_t poll;        /* inner host polling interval */
+    double* prof;        /* optional HOST array of 4, as lpm_cg_opts.prof, for the FP32 inner solves */
+} lpm_ir_opts;
+
+int lpm_abi_version(void);
+const char* lpm_status_string(int code);
+
+/* ------------------------------------------------------------------------------------------------ coefficients */
+/* Pack (nset, n, slots) FP64 coefficients into the (nset, slots, n) layout in FP32 or FP64.
+ * Replaces the per-solve casts of timing/t2d/solver2d.py:570-575 (Sys.mf_arrays(fp32=True)). */
+int lpm_pack_coef_f32(const double* src, float* dst, int64_t n, int32_t slots, int32_t nset, void* stream);
+int lpm_pack_coef_f64(const double* src, double* dst, int64_t n, int32_t slots, int32_t nset, void* stream);
+
+/* ----------------------------------------------------------------------------------------------------- K . u */
+/* Scratch bytes of one lpm_kmv_* call for `nsys` systems. */
+int64_t lpm_kmv_scratch_bytes(const lpm_lattice* lat, int32_t precision, int32_t nsys);
+
+/* out = K u.  SC: code-force operator of coarse3d/lin3d.py:126-149 (k_apply) and coarse3d/torch_lpm3d.py:63-83
+ * (SCT.apply, batched).  SQ: exact-Hessian operator of timing/t2d/solver2d.py:269-305 (_kmv). */
+int lpm_kmv_sc_f64(const lpm_lattice* lat, const double* u, const double* Kn, const double* Tv, int32_t coef_layout,
+                   const lpm_batch* batch, double* out, void* scratch, size_t scratch_bytes, void* stream);
+int lpm_kmv_sc_f32(const lpm_lattice* lat, const float* u, const float* Kn, const float* Tv, int32_t coef_layout,
+                   const lpm_batch* batch, float* out, void* scratch, size_t scratch_bytes, void* stream);
+int lpm_kmv_sq_f64(const lpm_lattice* lat, const double* u, const double* Kn, const double* Tv, int32_t coef_layout,
+                   const lpm_batch* batch, double* out, void* scratch, size_t scratch_bytes, void* stream);
+int lpm_kmv_sq_f32(const lpm_lattice* lat, const float* u, const float* Kn, const float* Tv, int32_t coef_layout,
+                   const lpm_batch* batch, float* out, void* scratch, size_t scratch_bytes, void* stream);
+
+/* --------------------------------------------------------------------------------------------- preconditioner */
+/* Diagonal blocks D (nset, n, d, d) of K (optional output, FP64) and their inverses Minv (nset, n, d, d).
+ * SC: coarse3d/lin3d.py:239-301 (k_block_diag, k_block_jacobi), coarse3d/torch_lpm3d.py:22-33,94-106 (inv3,
+ * block_diag, precond).  SQ: timing/t2d/solver2d.py:308-346 (_diag_inv).  Fixed particles are handled by the DOF mask
+ * when the preconditioner is applied (z = mask (Minv r)), so Minv itself is not masked. */
+int lpm_block_jacobi_f64(const lpm_lattice* lat, const double* Kn, const double* Tv, int32_t coef_layout,
+                         int32_t nset, double* Minv, double* D_or_null, void* stream);
+int lpm_block_jacobi_f32(const lpm_lattice* lat, const double* Kn, const double* Tv, int32_t coef_layout,
+                         int32_t nset, float* Minv, double* D_or_null, void* stream);
+
+/* ------------------------------------------------------------------------------------------------ batched CG */
+/* Workspace bytes of lpm_cg_batched_* (precond: 1 if Minv will be passed). */
+int64_t lpm_cg_workspace_bytes(const lpm_lattice* lat, int32_t nsys, int32_t precision, int32_t precond);
+
+/* Batched (P)CG on the free DOFs: K_ff x_f = b_f for every system, x updated in place (x must be zero on fixed DOFs;
+ * x_is_zero = 1 skips the initial K x).  Replaces coarse3d/lin3d.py:464-532 (_pcg / solve_pcg),
+ * timing/t3d/cgplain.py:11-55 (cg3), timing/t2d/cg2plain.py:11-49 (cg_mf), timing/t2d/solver2d.py:349-421
+ * (pcg_mf) and coarse3d/torch_lpm3d.py:109-140 (SCT.pcg).  Minv NULL = plain CG.  Outputs per system: iterations,
+ * relative residual |r|/|b| at the last test, LPM_STATUS_*.  coef_layout applies to Kn/Tv. */
+int lpm_cg_batched_f64(const lpm_lattice* lat, const double* Kn, const double* Tv, int32_t coef_layout,
+                       const lpm_batch* batch, const double* Minv, const uint8_t* mask, const double* b, double* x,
+                       int32_t x_is_zero, const lpm_cg_opts* opts, void* workspace, size_t workspace_bytes,
+                       int32_t* iters, double* relres, int32_t* status, void* stream);
+int lpm_cg_batched_f32(const lpm_lattice* lat, const float* Kn, const float* Tv, int32_t coef_layout,
+                       const lpm_batch* batch, const float* Minv, const uint8_t* mask, const float* b, float* x,
+                       int32_t x_is_zero, const lpm_cg_opts* opts, void* workspace, size_t workspace_bytes,
+                       int32_t* iters, double* relres, int32_t* status, void* stream);
+
+/* ------------------------------------------------------------------------------- mixed-precision refinement */
+int64_t lpm_ir_workspace_bytes(const lpm_lattice* lat, int32_t nsys, int32_t precond);
+
+/* FP32 inner PCG + FP64 iterative refinement to |b - K x| <= tol |b| on the FP64 operator.
+ * Kn64/Tv64: FP64 coefficients (coef_layout64); Kn32/Tv32: the same packed to FP32 SoA (lpm_pack_coef_f32);
+ * Minv32: FP32 block-Jacobi inverse or NULL.  x (FP64) updated in place, zero on fixed DOFs on entry.
+ * Outputs: total inner iterations, final FP64 relative residual, status per system (device arrays); outer_steps is a
+ * HOST pointer (may be NULL) that receives the number of refinement steps. */
+int lpm_ir_batched(const lpm_lattice* lat, const double* Kn64, const double* Tv64, int32_t coef_layout64,
+                   const float* Kn32, const float* Tv32, const float* Minv32, const lpm_batch* batch,
+                   const uint8_t* mask, const double* b, double* x, const lpm_ir_opts* opts, void* workspace,
+                   size_t workspace_bytes, int32_t* iters, double* relres, int32_t* status, int32_t* outer_steps,
+                   void* stream);
+
+/* ------------------------------------------------------------------------------------------------ gradients */
+int64_t lpm_grad_scratch_bytes(const lpm_lattice* lat, int32_t nsys);
+
+/* Per-slot derivatives of sum_s lam_s . K(Kn, Tv) u_s, summed over the systems of each coefficient set, written (or
+ * added, accumulate = 1) to gKn, gTv (nset, n, slots) in the reference layout; zero on missing bonds.
+ * SC (code-force operator): the autograd pass of coarse3d/torch_lpm3d.py:165-175 (LinSolve.backward) in closed form.
+ * SQ (exact Hessian): the gradient of coarse2d/torch_lpm.py:173-191 (assemble) through 34-51 (SPDSolve.backward).
+ * The adjoint solve's loss gradient is minus these values. */
+int lpm_bond_grad_sc(const lpm_lattice* lat, const double* u, const double* lam, const double* Kn, const double* Tv,
+                     int32_t coef_layout, const lpm_batch* batch, double* gKn, double* gTv, int32_t accumulate,
+                     void* scratch, size_t scratch_bytes, void* stream);
+int lpm_bond_grad_sq(const lpm_lattice* lat, const double* u, const double* lam, const double* Kn, const double* Tv,
+                     int32_t coef_layout, const lpm_batch* batch, double* gKn, double* gTv, int32_t accumulate,
+                     void* scratch, size_t scratch_bytes, void* stream);
+
+/* ------------------------------------------------------------------------------------------ post-processing */
+/* Particle stress with the opp-flag surface rule: SC (nsys, n, 6) xx yy zz yz xz xy (coarse3d/lin3d.py:170-210);
+ * SQ (nsys, n, 3) xx yy xy (timing/t2d/solver2d.py:220-256).  l0: bond length per slot (slots,), V: particle volume.
+ * scratch: lpm_kmv_scratch_bytes(lat, LPM_F64, nsys). */
+int lpm_stress_f64(const lpm_lattice* lat, const double* u, const double* Kn, const double* Tv, int32_t coef_layout,
+                   const lpm_batch* batch, const double* l0, double V, double* sig, void* scratch,
+                   size_t scratch_bytes, void* stream);
+/* Particle energy (nsys, n) (coarse3d/lin3d.py:213-236, coarse2d/lin2d.py:156-163). */
+int lpm_energy_f64(const lpm_lattice* lat, const double* u, const double* Kn, const double* Tv, int32_t coef_layout,
+                   const lpm_batch* batch, double* w, void* stream);
+
+/* ------------------------------------------------------------------------------------------------ geometry */
+/* Neighbour table of a (possibly masked) box, identical to LatticeGeom.nbr / Lattice2D.nbr
+ * (coarse3d/geom3d.py:38-65, coarse2d/lin2d.py:32-74): site_of (nx*ny*nz) int64 = particle id or -1,
+ * sites (n) int64 = site of each particle; nbr (n, slots) int64 out. */
+int lpm_build_nbr(int32_t dim, int32_t nx, int32_t ny, int32_t nz, int64_t n, const int64_t* site_of,
+                  const int64_t* sites, int64_t* nbr, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LPM_B200_H */

@@ -1,0 +1,315 @@
+// extern "C" entry points of liblpm_b200.so (declared in include/lpm_b200.h).
+#include <cstdint>
+
+#include "../../include/lpm_b200.h"
+#include "lpm_cg.h"
+#include "lpm_kernels.h"
+
+using namespace lpm;
+
+namespace {
+
+inline cudaStream_t S(void* p) { return static_cast<cudaStream_t>(p); }
+
+// Validates a lattice descriptor and converts it.  Returns LPM_OK or LPM_ERR_ARG.
+int to_lattice(const lpm_lattice* in, Lattice& L)
+{
+    if (!in) return LPM_ERR_ARG;
+    if (in->dim != 2 && in->dim != 3) return LPM_ERR_ARG;
+    if (in->nx < 1 || in->ny < 1 || in->nz < 1 || in->n < 1) return LPM_ERR_ARG;
+    if (in->dim == 2 && in->nz != 1) return LPM_ERR_ARG;
+    if (!in->nbr && in->n != (int64_t)in->nx * in->ny * in->nz) return LPM_ERR_ARG;
+    if (in->n > INT64_C(1) << 40) return LPM_ERR_ARG;
+    L.dim = in->dim;
+    L.nx = in->nx;
+    L.ny = in->ny;
+    L.nz = in->nz;
+    L.N = in->n;
+    L.nbr = in->nbr;
+    return LPM_OK;
+}
+
+int to_batch(const lpm_batch* in, Batch& b)
+{
+    if (!in || in->nsys < 1 || in->rhs_per_set < 1 || in->nmask < 1) return LPM_ERR_ARG;
+    b.nsys = in->nsys;
+    b.rhs_per_set = in->rhs_per_set;
+    b.nmask = in->nmask;
+    return LPM_OK;
+}
+
+int to_layout(int layout, const Lattice& L, CoefLayout& cl)
+{
+    const int NN = slots_of(L);
+    cl.set_stride = L.N * NN;
+    if (layout == LPM_LAYOUT_REF) {
+        cl.slot_stride = 1;
+        cl.site_stride = NN;
+    } else if (layout == LPM_LAYOUT_SOA) {
+        cl.slot_stride = L.N;
+        cl.site_stride = 1;
+    } else {
+        return LPM_ERR_ARG;
+    }
+    return LPM_OK;
+}
+
+// Scratch handed to kernels is re-aligned to 256 bytes (vector loads of the shell sums need 16/32-byte alignment).
+template <typename T>
+T* aligned(void* p, size_t bytes, size_t need, int& rc)
+{
+    const size_t shift = (256 - (reinterpret_cast<uintptr_t>(p) & 255)) & 255;
+    if (!p || bytes < need + shift) {
+        rc = LPM_ERR_WORKSPACE;
+        return nullptr;
+    }
+    rc = LPM_OK;
+    return reinterpret_cast<T*>(static_cast<char*>(p) + shift);
+}
+
+inline int ret(cudaError_t e) { return e == cudaSuccess ? LPM_OK : (int)e; }
+
+template <typename T>
+int kmv_impl(int dim, const lpm_lattice* lat, const T* u, const T* Kn, const T* Tv, int32_t layout,
+             const lpm_batch* batch, T* out, void* scratch, size_t scratch_bytes, void* stream)
+{
+    Lattice L;
+    Batch bt;
+    CoefLayout cl;
+    int rc = to_lattice(lat, L);
+    if (rc) return rc;
+    if (L.dim != dim) return LPM_ERR_UNSUPPORTED;
+    if ((rc = to_batch(batch, bt)) || (rc = to_layout(layout, L, cl))) return rc;
+    if (!u || !Kn || !Tv || !out) return LPM_ERR_ARG;
+    T* st = aligned<T>(scratch, scratch_bytes, (size_t)bt.nsys * L.N * 4 * sizeof(T), rc);
+    if (rc) return rc;
+    return ret(launch_kmv<T>(L, u, Kn, Tv, cl, bt, out, st, nullptr, S(stream)));
+}
+
+template <typename T>
+int cg_impl(const lpm_lattice* lat, const T* Kn, const T* Tv, int32_t layout, const lpm_batch* batch, const T* Minv,
+            const uint8_t* mask, const T* b, T* x, int32_t x_is_zero, const lpm_cg_opts* opts, void* ws,
+            size_t ws_bytes, int32_t* iters, double* relres, int32_t* status, void* stream)
+{
+    Lattice L;
+    Batch bt;
+    CoefLayout cl;
+    int rc = to_lattice(lat, L);
+    if (rc || (rc = to_batch(batch, bt)) || (rc = to_layout(layout, L, cl))) return rc;
+    if (!Kn || !Tv || !b || !x || !opts || !ws || !iters || !relres || !status) return LPM_ERR_ARG;
+    if (!(opts->tol >= 0.0)) return LPM_ERR_ARG;
+    return cg_solve<T>(L, Kn, Tv, cl, bt, Minv, mask, b, x, x_is_zero, *opts, ws, ws_bytes, iters, relres, status,
+                       S(stream));
+}
+
+}  // namespace
+
+extern "C" {
+
+int lpm_abi_version(void) { return LPM_ABI_VERSION; }
+
+const char* lpm_status_string(int code)
+{
+    switch (code) {
+    case LPM_OK: return "ok";
+    case LPM_ERR_ARG: return "invalid argument";
+    case LPM_ERR_WORKSPACE: return "workspace or scratch buffer too small";
+    case LPM_ERR_UNSUPPORTED: return "unsupported lattice or precision for this entry point";
+    default: return code > 0 ? cudaGetErrorString((cudaError_t)code) : "unknown error";
+    }
+}
+
+int lpm_pack_coef_f32(const double* src, float* dst, int64_t n, int32_t slots, int32_t nset, void* stream)
+{
+    if (!src || !dst || n < 1 || (slots != 8 && slots != 18) || nset < 1) return LPM_ERR_ARG;
+    return ret(launch_pack<float>(src, dst, n, slots, nset, S(stream)));
+}
+
+int lpm_pack_coef_f64(const double* src, double* dst, int64_t n, int32_t slots, int32_t nset, void* stream)
+{
+    if (!src || !dst || n < 1 || (slots != 8 && slots != 18) || nset < 1) return LPM_ERR_ARG;
+    return ret(launch_pack<double>(src, dst, n, slots, nset, S(stream)));
+}
+
+int64_t lpm_kmv_scratch_bytes(const lpm_lattice* lat, int32_t precision, int32_t nsys)
+{
+    Lattice L;
+    if (to_lattice(lat, L) || nsys < 1) return LPM_ERR_ARG;
+    const size_t es = precision == LPM_F32 ? 4 : 8;
+    return (int64_t)((size_t)nsys * L.N * 4 * es + 256);
+}
+
+int lpm_kmv_sc_f64(const lpm_lattice* lat, const double* u, const double* Kn, const double* Tv, int32_t coef_layout,
+                   const lpm_batch* batch, double* out, void* scratch, size_t scratch_bytes, void* stream)
+{
+    return kmv_impl<double>(3, lat, u, Kn, Tv, coef_layout, batch, out, scratch, scratch_bytes, stream);
+}
+int lpm_kmv_sc_f32(const lpm_lattice* lat, const float* u, const float* Kn, const float* Tv, int32_t coef_layout,
+                   const lpm_batch* batch, float* out, void* scratch, size_t scratch_bytes, void* stream)
+{
+    return kmv_impl<float>(3, lat, u, Kn, Tv, coef_layout, batch, out, scratch, scratch_bytes, stream);
+}
+int lpm_kmv_sq_f64(const lpm_lattice* lat, const double* u, const double* Kn, const double* Tv, int32_t coef_layout,
+                   const lpm_batch* batch, double* out, void* scratch, size_t scratch_bytes, void* stream)
+{
+    return kmv_impl<double>(2, lat, u, Kn, Tv, coef_layout, batch, out, scratch, scratch_bytes, stream);
+}
+int lpm_kmv_sq_f32(const lpm_lattice* lat, const float* u, const float* Kn, const float* Tv, int32_t coef_layout,
+                   const lpm_batch* batch, float* out, void* scratch, size_t scratch_bytes, void* stream)
+{
+    return kmv_impl<float>(2, lat, u, Kn, Tv, coef_layout, batch, out, scratch, scratch_bytes, stream);
+}
+
+int lpm_block_jacobi_f64(const lpm_lattice* lat, const double* Kn, const double* Tv, int32_t coef_layout,
+                         int32_t nset, double* Minv, double* D_or_null, void* stream)
+{
+    Lattice L;
+    CoefLayout cl;
+    int rc = to_lattice(lat, L);
+    if (rc || (rc = to_layout(coef_layout, L, cl))) return rc;
+    if (!Kn || !Tv || !Minv || nset < 1) return LPM_ERR_ARG;
+    return ret(launch_block_jacobi<double>(L, Kn, Tv, cl, nset, Minv, D_or_null, S(stream)));
+}
+
+int lpm_block_jacobi_f32(const lpm_lattice* lat, const double* Kn, const double* Tv, int32_t coef_layout,
+                         int32_t nset, float* Minv, double* D_or_null, void* stream)
+{
+    Lattice L;
+    CoefLayout cl;
+    int rc = to_lattice(lat, L);
+    if (rc || (rc = to_layout(coef_layout, L, cl))) return rc;
+    if (!Kn || !Tv || !Minv || nset < 1) return LPM_ERR_ARG;
+    return ret(launch_block_jacobi<float>(L, Kn, Tv, cl, nset, Minv, D_or_null, S(stream)));
+}
+
+int64_t lpm_cg_workspace_bytes(const lpm_lattice* lat, int32_t nsys, int32_t precision, int32_t precond)
+{
+    Lattice L;
+    if (to_lattice(lat, L) || nsys < 1) return LPM_ERR_ARG;
+    return (int64_t)cg_workspace_bytes(L, nsys, precision, precond) + 256;
+}
+
+int lpm_cg_batched_f64(const lpm_lattice* lat, const double* Kn, const double* Tv, int32_t coef_layout,
+                       const lpm_batch* batch, const double* Minv, const uint8_t* mask, const double* b, double* x,
+                       int32_t x_is_zero, const lpm_cg_opts* opts, void* workspace, size_t workspace_bytes,
+                       int32_t* iters, double* relres, int32_t* status, void* stream)
+{
+    return cg_impl<double>(lat, Kn, Tv, coef_layout, batch, Minv, mask, b, x, x_is_zero, opts, workspace,
+                           workspace_bytes, iters, relres, status, stream);
+}
+
+int lpm_cg_batched_f32(const lpm_lattice* lat, const float* Kn, const float* Tv, int32_t coef_layout,
+                       const lpm_batch* batch, const float* Minv, const uint8_t* mask, const float* b, float* x,
+                       int32_t x_is_zero, const lpm_cg_opts* opts, void* workspace, size_t workspace_bytes,
+                       int32_t* iters, double* relres, int32_t* status, void* stream)
+{
+    return cg_impl<float>(lat, Kn, Tv, coef_layout, batch, Minv, mask, b, x, x_is_zero, opts, workspace,
+                          workspace_bytes, iters, relres, status, stream);
+}
+
+int64_t lpm_ir_workspace_bytes(const lpm_lattice* lat, int32_t nsys, int32_t precond)
+{
+    Lattice L;
+    if (to_lattice(lat, L) || nsys < 1) return LPM_ERR_ARG;
+    return (int64_t)ir_workspace_bytes(L, nsys, precond) + 256;
+}
+
+int lpm_ir_batched(const lpm_lattice* lat, const double* Kn64, const double* Tv64, int32_t coef_layout64,
+                   const float* Kn32, const float* Tv32, const float* Minv32, const lpm_batch* batch,
+                   const uint8_t* mask, const double* b, double* x, const lpm_ir_opts* opts, void* workspace,
+                   size_t workspace_bytes, int32_t* iters, double* relres, int32_t* status, int32_t* outer_steps,
+                   void* stream)
+{
+    Lattice L;
+    Batch bt;
+    CoefLayout cl64, cl32;
+    int rc = to_lattice(lat, L);
+    if (rc || (rc = to_batch(batch, bt)) || (rc = to_layout(coef_layout64, L, cl64)) ||
+        (rc = to_layout(LPM_LAYOUT_SOA, L, cl32)))
+        return rc;
+    if (!Kn64 || !Tv64 || !Kn32 || !Tv32 || !b || !x || !opts || !workspace || !iters || !relres || !status)
+        return LPM_ERR_ARG;
+    if (!(opts->tol >= 0.0) || !(opts->inner_tol > 0.0)) return LPM_ERR_ARG;
+    return ir_solve(L, Kn64, Tv64, cl64, Kn32, Tv32, cl32, Minv32, bt, mask, b, x, *opts, workspace,
+                    workspace_bytes, iters, relres, status, outer_steps, S(stream));
+}
+
+int64_t lpm_grad_scratch_bytes(const lpm_lattice* lat, int32_t nsys)
+{
+    Lattice L;
+    if (to_lattice(lat, L) || nsys < 1) return LPM_ERR_ARG;
+    return (int64_t)(2 * (size_t)nsys * L.N * 4 * sizeof(double) + 256);
+}
+
+static int grad_impl(int dim, const lpm_lattice* lat, const double* u, const double* lam, const double* Kn,
+                     const double* Tv, int32_t layout, const lpm_batch* batch, double* gKn, double* gTv,
+                     int32_t accumulate, void* scratch, size_t scratch_bytes, void* stream)
+{
+    Lattice L;
+    Batch bt;
+    CoefLayout cl;
+    int rc = to_lattice(lat, L);
+    if (rc) return rc;
+    if (L.dim != dim) return LPM_ERR_UNSUPPORTED;
+    if ((rc = to_batch(batch, bt)) || (rc = to_layout(layout, L, cl))) return rc;
+    if (!u || !lam || !Kn || !Tv || !gKn || !gTv) return LPM_ERR_ARG;
+    double* st = nullptr;
+    if (dim == 3) {
+        st = aligned<double>(scratch, scratch_bytes, 2 * (size_t)bt.nsys * L.N * 4 * sizeof(double), rc);
+        if (rc) return rc;
+    }
+    return ret(launch_grad(L, u, lam, Kn, Tv, cl, bt, gKn, gTv, st, accumulate, S(stream)));
+}
+
+int lpm_bond_grad_sc(const lpm_lattice* lat, const double* u, const double* lam, const double* Kn, const double* Tv,
+                     int32_t coef_layout, const lpm_batch* batch, double* gKn, double* gTv, int32_t accumulate,
+                     void* scratch, size_t scratch_bytes, void* stream)
+{
+    return grad_impl(3, lat, u, lam, Kn, Tv, coef_layout, batch, gKn, gTv, accumulate, scratch, scratch_bytes,
+                     stream);
+}
+
+int lpm_bond_grad_sq(const lpm_lattice* lat, const double* u, const double* lam, const double* Kn, const double* Tv,
+                     int32_t coef_layout, const lpm_batch* batch, double* gKn, double* gTv, int32_t accumulate,
+                     void* scratch, size_t scratch_bytes, void* stream)
+{
+    return grad_impl(2, lat, u, lam, Kn, Tv, coef_layout, batch, gKn, gTv, accumulate, scratch, scratch_bytes,
+                     stream);
+}
+
+int lpm_stress_f64(const lpm_lattice* lat, const double* u, const double* Kn, const double* Tv, int32_t coef_layout,
+                   const lpm_batch* batch, const double* l0, double V, double* sig, void* scratch,
+                   size_t scratch_bytes, void* stream)
+{
+    Lattice L;
+    Batch bt;
+    CoefLayout cl;
+    int rc = to_lattice(lat, L);
+    if (rc || (rc = to_batch(batch, bt)) || (rc = to_layout(coef_layout, L, cl))) return rc;
+    if (!u || !Kn || !Tv || !l0 || !sig || !(V > 0.0)) return LPM_ERR_ARG;
+    double* st = aligned<double>(scratch, scratch_bytes, (size_t)bt.nsys * L.N * 4 * sizeof(double), rc);
+    if (rc) return rc;
+    return ret(launch_stress(L, u, Kn, Tv, cl, bt, l0, V, sig, st, S(stream)));
+}
+
+int lpm_energy_f64(const lpm_lattice* lat, const double* u, const double* Kn, const double* Tv, int32_t coef_layout,
+                   const lpm_batch* batch, double* w, void* stream)
+{
+    Lattice L;
+    Batch bt;
+    CoefLayout cl;
+    int rc = to_lattice(lat, L);
+    if (rc || (rc = to_batch(batch, bt)) || (rc = to_layout(coef_layout, L, cl))) return rc;
+    if (!u || !Kn || !Tv || !w) return LPM_ERR_ARG;
+    return ret(launch_energy(L, u, Kn, Tv, cl, bt, w, S(stream)));
+}
+
+int lpm_build_nbr(int32_t dim, int32_t nx, int32_t ny, int32_t nz, int64_t n, const int64_t* site_of,
+                  const int64_t* sites, int64_t* nbr, void* stream)
+{
+    if ((dim != 2 && dim != 3) || nx < 1 || ny < 1 || nz < 1 || n < 0 || (dim == 2 && nz != 1)) return LPM_ERR_ARG;
+    if (n > 0 && (!site_of || !sites || !nbr)) return LPM_ERR_ARG;
+    return ret(launch_build_nbr(dim, nx, ny, nz, n, site_of, sites, nbr, S(stream)));
+}
+
+}  // extern "C"

@@ -1,0 +1,257 @@
+// Matrix-free LPM operator K.u for the simple-cubic (3D, 18 slots) and square (2D, 8 slots) lattices.
+//
+// Two-pass form, batched over systems (right-hand sides) that share coefficient sets:
+//   pass 1: per particle i and shell c:  S_i^c = sum_{k in c} dL_ik,  TS_i^c = sum_{k in c} Tv_ik dL_ik
+//   pass 2 (SC, code-force form of coarse3d/lin3d.py:126-149):
+//       F_ik = 2 Kn_ik dL_ik + (TS_i^c + TS_q^c)/2 + Tv_ik (S_i^c + S_q^c)/2,     f_i = sum_k F_ik n_k
+//   pass 2 (SQ, exact-Hessian g-form of timing/t2d/solver2d.py:269-305):
+//       g_ik = Kn_ik dL_ik + (Tv_ik S_i^c + TS_i^c)/2,  f_i = sum_k (g_ik + g_{q,k^1}) n_k
+//     evaluated from the per-particle sums of q (no per-bond scratch): g_{q,k^1} needs Kn/Tv of q's slot k^1.
+// The optional CG epilogue masks the result with the per-DOF free mask and reduces in . out per system with a
+// deterministic last-block reduction.
+//
+// Structured boxes use implicit neighbours (site id (z*ny + y)*nx + x); other lattices (active-site masks) use an
+// int32 neighbour table.  The fused single-pass z-marching SC kernel for full boxes lives in kmv_fused.cu.
+#include "lpm_kernels.h"
+#include "lpm_stencil.cuh"
+
+namespace lpm {
+
+namespace {
+
+using namespace stencil;
+
+// ------------------------------------------------------------------------------------------------------ pass 1
+template <typename T, int DIM, class NB>
+__global__ void __launch_bounds__(256) k_shell_sums(NB nb, int nx, int ny, int nz, int64_t N, int sys0,
+                                                    const T* __restrict__ u, const T* __restrict__ Tv, CoefLayout cl,
+                                                    Batch bt, T* __restrict__ st, const int* __restrict__ act)
+{
+    using S = Slots<DIM>;
+    const Site p = locate<NB>(nx, ny, nz, N, sys0);
+    if (!p.ok || (act && !act[p.s])) return;
+    const T* us = u + (int64_t)p.s * N * DIM;
+    const T* tv = Tv + (int64_t)(p.s / bt.rhs_per_set) * cl.set_stride + p.i * cl.site_stride;
+    T ui[3];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) ui[a] = us[DIM * p.i + a];
+    T s0 = 0, s1 = 0, t0 = 0, t1 = 0;
+#pragma unroll
+    for (int k = 0; k < S::NN; ++k) {
+        int64_t q;
+        if (!nb.get(p, k, q)) continue;
+        const T d = dl_of<T, DIM>(us, p.i, q, k, ui);
+        const T tvk = tv[k * cl.slot_stride];
+        if (S::shell(k) == 0) {
+            s0 += d;
+            t0 += tvk * d;
+        } else {
+            s1 += d;
+            t1 += tvk * d;
+        }
+    }
+    T* o = st + ((int64_t)p.s * N + p.i) * 4;
+    o[0] = s0;
+    o[1] = s1;
+    o[2] = t0;
+    o[3] = t1;
+}
+
+// ------------------------------------------------------------------------------------------------------ pass 2
+template <typename T, int DIM, class NB, bool EPI>
+__global__ void __launch_bounds__(256) k_apply(NB nb, int nx, int ny, int nz, int64_t N, int sys0,
+                                               const T* __restrict__ u, const T* __restrict__ Kn,
+                                               const T* __restrict__ Tv, CoefLayout cl, Batch bt,
+                                               const T* __restrict__ st, T* __restrict__ out,
+                                               const uint8_t* __restrict__ mask, double* __restrict__ part,
+                                               double* __restrict__ dot_final, unsigned* __restrict__ counter,
+                                               const int* __restrict__ act, int nblk)
+{
+    using S = Slots<DIM>;
+    const Site p = locate<NB>(nx, ny, nz, N, sys0);
+    double dot = 0.0;
+    if (p.ok && (!act || act[p.s])) {
+        const T* us = u + (int64_t)p.s * N * DIM;
+        const int64_t cbase = (int64_t)(p.s / bt.rhs_per_set) * cl.set_stride;
+        const T* kn = Kn + cbase + p.i * cl.site_stride;
+        const T* tv = Tv + cbase + p.i * cl.site_stride;
+        const T* sts = st + (int64_t)p.s * N * 4;
+        T ui[3];
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) ui[a] = us[DIM * p.i + a];
+        T Si[2], TSi[2];
+        load4(sts + 4 * p.i, Si[0], Si[1], TSi[0], TSi[1]);
+        T f[3] = {T(0), T(0), T(0)};
+#pragma unroll
+        for (int k = 0; k < S::NN; ++k) {
+            int64_t q;
+            if (!nb.get(p, k, q)) continue;
+            const int c = S::shell(k);
+            const T d = dl_of<T, DIM>(us, p.i, q, k, ui);
+            T Sq[2], TSq[2];
+            load4(sts + 4 * q, Sq[0], Sq[1], TSq[0], TSq[1]);
+            const T knk = kn[k * cl.slot_stride], tvk = tv[k * cl.slot_stride];
+            T F;
+            if constexpr (DIM == 3) {
+                F = T(2) * knk * d + T(0.5) * (TSi[c] + TSq[c]) + T(0.5) * tvk * (Si[c] + Sq[c]);
+            } else {
+                const int64_t qo = (int64_t)q * cl.site_stride + (k ^ 1) * cl.slot_stride;
+                const T knq = Kn[cbase + qo], tvq = Tv[cbase + qo];
+                F = (knk + knq) * d + T(0.5) * (tvk * Si[c] + TSi[c]) + T(0.5) * (tvq * Sq[c] + TSq[c]);
+            }
+            // f += F n_k with n_k = -o_k w_k
+            const T Fw = F * bond_w<T>(c);
+            f[0] -= T(S::dx(k)) * Fw;
+            f[1] -= T(S::dy(k)) * Fw;
+            if constexpr (DIM == 3) f[2] -= T(S::dz(k)) * Fw;
+        }
+        T* o = out + ((int64_t)p.s * N + p.i) * DIM;
+        if (EPI && mask) {
+            const uint8_t* m = mask + ((int64_t)(p.s % bt.nmask) * N + p.i) * DIM;
+#pragma unroll
+            for (int a = 0; a < DIM; ++a) f[a] = m[a] ? f[a] : T(0);
+        }
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+            o[a] = f[a];
+            dot += (double)ui[a] * (double)f[a];
+        }
+    }
+    if constexpr (EPI) {
+        if (part == nullptr) return;
+        __shared__ double sh[32];
+        __shared__ bool last;
+        const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+        const int nthr = blockDim.x * blockDim.y;
+        const double v = block_sum(dot, sh);
+        const int s = NB::structured ? sys0 + blockIdx.z / nz : sys0 + blockIdx.y;
+        const int b = block_in_system<NB>(nz);
+        if (tid == 0) {
+            part[(int64_t)s * nblk + b] = v;
+            __threadfence();
+            last = atomicAdd(counter + s, 1u) == (unsigned)(nblk - 1);
+        }
+        __syncthreads();
+        if (last) {
+            double acc = 0.0;
+            for (int j = tid; j < nblk; j += nthr) acc += __ldcg(part + (int64_t)s * nblk + j);
+            acc = block_sum(acc, sh);
+            if (tid == 0) {
+                dot_final[s] = acc;
+                counter[s] = 0u;
+            }
+        }
+    }
+}
+
+template <typename T, int DIM, class NB>
+cudaError_t run_kmv(NB nb, const Lattice& L, const T* u, const T* Kn, const T* Tv, const CoefLayout& cl,
+                    const Batch& bt, T* out, T* scratch, const MvEpilogue* ep, cudaStream_t st)
+{
+    const int nz = DIM == 3 ? L.nz : 1;
+    const bool epi = ep && (ep->mask || ep->dot_part);  // act alone needs no epilogue
+    int chunk, nblk;
+    dim3 grid, block;
+    if constexpr (NB::structured) {
+        block = dim3(BX, BY, 1);
+        chunk = 65535 / nz;
+        grid = dim3((L.nx + BX - 1) / BX, (L.ny + BY - 1) / BY, 1);
+        nblk = grid.x * grid.y * nz;
+    } else {
+        block = dim3(TB, 1, 1);
+        chunk = 65535;
+        grid = dim3((unsigned)((L.N + TB - 1) / TB), 1, 1);
+        nblk = grid.x;
+    }
+    for (int s0 = 0; s0 < bt.nsys; s0 += chunk) {
+        const int ns = bt.nsys - s0 < chunk ? bt.nsys - s0 : chunk;
+        dim3 g = grid;
+        if constexpr (NB::structured)
+            g.z = nz * ns;
+        else
+            g.y = ns;
+        const int* act = ep ? ep->act : nullptr;
+        k_shell_sums<T, DIM, NB><<<g, block, 0, st>>>(nb, L.nx, L.ny, nz, L.N, s0, u, Tv, cl, bt, scratch, act);
+        if (epi) {
+            k_apply<T, DIM, NB, true><<<g, block, 0, st>>>(nb, L.nx, L.ny, nz, L.N, s0, u, Kn, Tv, cl, bt, scratch,
+                                                           out, ep->mask, ep->dot_part, ep->dot_final, ep->counter,
+                                                           act, nblk);
+        } else {
+            k_apply<T, DIM, NB, false><<<g, block, 0, st>>>(nb, L.nx, L.ny, nz, L.N, s0, u, Kn, Tv, cl, bt, scratch,
+                                                            out, nullptr, nullptr, nullptr, nullptr, act, nblk);
+        }
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+template <typename T, int DIM, class NB>
+cudaError_t run_sums(NB nb, const Lattice& L, const T* u, const T* Tv, const CoefLayout& cl, const Batch& bt,
+                     T* scratch, cudaStream_t st)
+{
+    const int nz = DIM == 3 ? L.nz : 1;
+    int chunk;
+    dim3 grid, block;
+    if constexpr (NB::structured) {
+        block = dim3(BX, BY, 1);
+        chunk = 65535 / nz;
+        grid = dim3((L.nx + BX - 1) / BX, (L.ny + BY - 1) / BY, 1);
+    } else {
+        block = dim3(TB, 1, 1);
+        chunk = 65535;
+        grid = dim3((unsigned)((L.N + TB - 1) / TB), 1, 1);
+    }
+    for (int s0 = 0; s0 < bt.nsys; s0 += chunk) {
+        const int ns = bt.nsys - s0 < chunk ? bt.nsys - s0 : chunk;
+        dim3 g = grid;
+        if constexpr (NB::structured)
+            g.z = nz * ns;
+        else
+            g.y = ns;
+        k_shell_sums<T, DIM, NB><<<g, block, 0, st>>>(nb, L.nx, L.ny, nz, L.N, s0, u, Tv, cl, bt, scratch, nullptr);
+    }
+    return cudaGetLastError();
+}
+
+int kmv_dot_blocks(const Lattice& L)
+{
+    if (L.nbr) return (int)((L.N + TB - 1) / TB);
+    const int nz = L.dim == 3 ? L.nz : 1;
+    return ((L.nx + BX - 1) / BX) * ((L.ny + BY - 1) / BY) * nz;
+}
+
+template <typename T>
+cudaError_t launch_kmv(const Lattice& L, const T* u, const T* Kn, const T* Tv, const CoefLayout& cl, const Batch& bt,
+                       T* out, T* scratch, const MvEpilogue* ep, cudaStream_t st)
+{
+    if (L.dim == 3) {
+        if (L.nbr) return run_kmv<T, 3>(TableNb<3>{L.nbr}, L, u, Kn, Tv, cl, bt, out, scratch, ep, st);
+        return run_kmv<T, 3>(GridNb<3>{L.nx, L.ny, L.nz}, L, u, Kn, Tv, cl, bt, out, scratch, ep, st);
+    }
+    if (L.nbr) return run_kmv<T, 2>(TableNb<2>{L.nbr}, L, u, Kn, Tv, cl, bt, out, scratch, ep, st);
+    return run_kmv<T, 2>(GridNb<2>{L.nx, L.ny, 1}, L, u, Kn, Tv, cl, bt, out, scratch, ep, st);
+}
+
+template <typename T>
+cudaError_t launch_kmv_sums(const Lattice& L, const T* u, const T* Tv, const CoefLayout& cl, const Batch& bt,
+                            T* scratch, cudaStream_t st)
+{
+    if (L.dim == 3) {
+        if (L.nbr) return run_sums<T, 3>(TableNb<3>{L.nbr}, L, u, Tv, cl, bt, scratch, st);
+        return run_sums<T, 3>(GridNb<3>{L.nx, L.ny, L.nz}, L, u, Tv, cl, bt, scratch, st);
+    }
+    if (L.nbr) return run_sums<T, 2>(TableNb<2>{L.nbr}, L, u, Tv, cl, bt, scratch, st);
+    return run_sums<T, 2>(GridNb<2>{L.nx, L.ny, 1}, L, u, Tv, cl, bt, scratch, st);
+}
+
+template cudaError_t launch_kmv_sums<double>(const Lattice&, const double*, const double*, const CoefLayout&,
+                                             const Batch&, double*, cudaStream_t);
+
+template cudaError_t launch_kmv<float>(const Lattice&, const float*, const float*, const float*, const CoefLayout&,
+                                       const Batch&, float*, float*, const MvEpilogue*, cudaStream_t);
+template cudaError_t launch_kmv<double>(const Lattice&, const double*, const double*, const double*,
+                                        const CoefLayout&, const Batch&, double*, double*, const MvEpilogue*,
+                                        cudaStream_t);
+
+}  // namespace lpm

@@ -59,3 +59,13 @@ def test_sq_params_and_bcs(gsq):
             assert np.allclose(up, gsq["bc_up_%d_%s" % (L, ld)], rtol=0, atol=1e-18)
     fd, up, _ = G.uniaxial_tension_2d(lat)
     assert np.array_equal(fd, gsq["cg_fixed"]) and np.allclose(up, gsq["cg_up"], rtol=0, atol=1e-18)
+
+
+def test_generators(gsc, gsq):
+    from lpm_b200 import micro
+    assert np.array_equal(micro.grf_two_phase(40, 32, 6.0, 0.30, 3), gsq["gen_grf"])
+    assert np.array_equal(micro.spheres(16, 16, 16, 0.25, 4.0, np.random.default_rng(7), rjit=0.0)[0],
+                          gsc["gen_spheres"])
+    assert np.array_equal(micro.ellipsoids(16, 16, 16, 0.3, 3.0, np.random.default_rng(8), aspect=(3.0, 3.0),
+                                           rjit=0.0)[0], gsc["gen_ellip"])
+    assert np.array_equal(micro.grf3(12, 12, 12, 2.0, 0.3, np.random.default_rng(9))[0], gsc["gen_grf3"])

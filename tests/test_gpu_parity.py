@@ -1,0 +1,270 @@
+"""GPU parity of the CUDA library (through the C ABI) against the CPU oracle and the reference's golden vectors.
+
+Tolerances: FP64 kernels 1e-13 (max-abs relative to the max of the reference array); FP32 kernels 2e-6; solves to
+rel. residual 1e-12 agree with SuperLU to 1e-9; mixed-precision solves to 1e-8 agree with the FP64 oracle to 1e-6
+(displacement, relative L2), the bar of the mixed-precision path.  Connectivity is bit-exact.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import relmax
+from lpm_b200 import core, geom as G
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda"
+
+
+def T(a, dt=torch.float64):
+    return torch.as_tensor(np.asarray(a), device=DEV, dtype=dt)
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, float).ravel()
+    b = np.asarray(b, float).ravel()
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def sym_params(lat, rng, kn=(0.8, 1.2), tv=(-0.03, 0.03)):
+    """Random symmetric per-bond parameters (same value on (i,k) and (q,k^1)), zero on missing bonds."""
+    Kn = np.zeros((lat.N, lat.NN))
+    Tv = np.zeros((lat.N, lat.NN))
+    i, k = np.nonzero(lat.valid & (np.arange(lat.NN)[None, :] % 2 == 0))
+    q = lat.nbr[i, k]
+    a = rng.uniform(*kn, size=i.size)
+    b = rng.uniform(*tv, size=i.size)
+    Kn[i, k] = a
+    Kn[q, k ^ 1] = a
+    Tv[i, k] = b
+    Tv[q, k ^ 1] = b
+    return Kn, Tv
+
+
+@pytest.fixture(scope="module")
+def sc12(gsc):
+    lat = G.LatticeGeom(12, 12, 12, 1.0)
+    return lat, core.DeviceLattice(lat), gsc["Kn"], gsc["Tv"]
+
+
+# ------------------------------------------------------------------------------------------------------- K . u
+def test_kmv_sc_golden(gsc, sc12):
+    lat, dl, Kn, Tv = sc12
+    f = core.kmv(dl, T(gsc["u"]), T(Kn), T(Tv)).cpu().numpy()
+    assert relmax(f, gsc["Ku"]) < 1e-13
+    f32 = core.kmv(dl, T(gsc["u"], torch.float32), T(Kn, torch.float32), T(Tv, torch.float32)).cpu().numpy()
+    assert relmax(f32, gsc["Ku"]) < 2e-6
+
+
+@pytest.mark.parametrize("shape", [(5, 7, 9), (33, 9, 3), (3, 3, 3), (40, 17, 6)])
+def test_kmv_sc_odd_sizes_batched(shape):
+    rng = np.random.default_rng(sum(shape))
+    lat = G.LatticeGeom(*shape)
+    dl = core.DeviceLattice(lat)
+    B, Lc = 2, 3
+    Kn = [sym_params(lat, rng)[0] for _ in range(B)]
+    Tv = [rng.uniform(-0.05, 0.05, (lat.N, 18)) * lat.valid for _ in range(B)]   # non-symmetric Tv
+    u = rng.standard_normal((B, Lc, lat.N, 3))
+    f = core.kmv(dl, T(u), T(np.array(Kn))[:, None], T(np.array(Tv))[:, None]).cpu().numpy()
+    for b in range(B):
+        for l in range(Lc):
+            assert relmax(f[b, l], O.sc_apply(lat, u[b, l], Kn[b], Tv[b])) < 1e-13
+    # packed SoA layout gives the same result
+    Kp = core.pack(T(np.array(Kn)), torch.float64)
+    Tp = core.pack(T(np.array(Tv)), torch.float64)
+    from lpm_b200 import _lib
+    fp = core.kmv(dl, T(u).reshape(B * Lc, lat.N, 3), Kp, Tp, layout=_lib.LAYOUT_SOA, rhs_per_set=Lc).cpu().numpy()
+    assert relmax(fp.reshape(f.shape), f) < 1e-15
+
+
+def test_kmv_sc_masked_lattice(gsc):
+    lat = G.LatticeGeom(7, 5, 4, 1.5, active=gsc["m_active"])
+    dl = core.DeviceLattice(lat)
+    rng = np.random.default_rng(3)
+    Kn, Tv = sym_params(lat, rng)
+    u = rng.standard_normal((2, lat.N, 3))
+    f = core.kmv(dl, T(u), T(Kn), T(Tv)).cpu().numpy()
+    for s in range(2):
+        assert relmax(f[s], O.sc_apply(lat, u[s], Kn, Tv)) < 1e-13
+
+
+def test_kmv_sq(gsq):
+    lat = G.Lattice2D("square", 16, 12, 1.0)
+    dl = core.DeviceLattice(lat)
+    u = gsq["u"].reshape(-1, 2)
+    f = core.kmv(dl, T(u), T(gsq["Kn_ns"]), T(gsq["Tv_ns"])).cpu().numpy().ravel()
+    assert relmax(f, gsq["f_ns"]) < 1e-13
+    f32 = core.kmv(dl, T(u, torch.float32), T(gsq["Kn_ns"], torch.float32), T(gsq["Tv_ns"], torch.float32))
+    assert relmax(f32.cpu().numpy().ravel(), gsq["f_ns"]) < 2e-6
+    # masked square lattice through the neighbour table
+    lm = G.Lattice2D("square", 9, 7, 0.5, active=gsq["m_active"])
+    dm = core.DeviceLattice(lm)
+    rng = np.random.default_rng(8)
+    Kn, Tv = rng.uniform(0.5, 1.5, (lm.N, 8)) * lm.valid, rng.uniform(-0.1, 0.1, (lm.N, 8)) * lm.valid
+    um = rng.standard_normal((lm.N, 2))
+    assert relmax(core.kmv(dm, T(um), T(Kn), T(Tv)).cpu().numpy().ravel(), O.sq_kmv(lm, um, Kn, Tv)) < 1e-13
+
+
+# ----------------------------------------------------------------------------------------- geometry on device
+def test_build_nbr_bit_exact(gsc, gsq):
+    lat = G.LatticeGeom(7, 5, 4, 1.5, active=gsc["m_active"])
+    nb = core.build_nbr(lat).cpu().numpy()
+    assert nb.dtype == np.int64 and np.array_equal(nb, gsc["m_nbr"].astype(np.int64))
+    full = G.LatticeGeom(12, 12, 12)
+    assert np.array_equal(core.build_nbr(full).cpu().numpy(), gsc["nbr"].astype(np.int64))
+    lm = G.Lattice2D("square", 9, 7, 0.5, active=gsq["m_active"])
+    assert np.array_equal(core.build_nbr(lm).cpu().numpy(), gsq["m_nbr"].astype(np.int64))
+
+
+# ---------------------------------------------------------------------------------------------- preconditioner
+def test_block_jacobi(gsc, gsq, sc12):
+    lat, dl, Kn, Tv = sc12
+    M, D = core.block_jacobi(dl, T(Kn), T(Tv), torch.float64, want_D=True)
+    assert relmax(D[0].cpu().numpy(), gsc["D"]) < 1e-13
+    I = torch.einsum("nab,nbc->nac", M[0], D[0]).cpu().numpy()
+    assert np.abs(I - np.eye(3)[None]).max() < 1e-10
+    lat2 = G.Lattice2D("square", 16, 12, 1.0)
+    d2 = core.DeviceLattice(lat2)
+    M2 = core.block_jacobi(d2, T(gsq["Kn"]), T(gsq["Tv"]), torch.float64)[0].cpu().numpy()
+    free = ~gsq["diag_fixed"]
+    assert relmax(M2[free], gsq["Binv"][free]) < 1e-13
+
+
+# ------------------------------------------------------------------------------------------------------- solves
+def _bc(lat, ld, s):
+    nc = lat.nx // s
+    fixed, up, mov = G.prescribed(ld, lat.x, lat.ijk // s, (nc,) * 3, s)
+    return fixed, up, mov
+
+
+def test_cg_fp64_matches_oracle(gsc, sc12):
+    """Plain FP64 CG (cgplain.cg3) and block-Jacobi PCG (lin3d.solve_pcg): same iterations, same answer."""
+    lat, dl, Kn, Tv = sc12
+    for ld in ("k_xx", "tb_sx"):
+        fixed, up, _ = _bc(lat, ld, 2)
+        free = ~fixed
+        upm = np.where(fixed[:, None], up, 0.0)
+        b = -O.sc_apply(lat, upm, Kn, Tv) * free[:, None]
+        x, info = core.cg(dl, T(Kn), T(Tv), T(b), free=T(free), tol=1e-8, maxit=5000, check=1)
+        assert abs(int(info.iters[0]) - int(gsc["cg_it_%s" % ld])) <= 1
+        assert relmax(x.cpu().numpy() + upm, gsc["cg_u_%s" % ld]) < 1e-6
+        M = core.block_jacobi(dl, T(Kn), T(Tv), torch.float64)
+        x, info = core.cg(dl, T(Kn), T(Tv), T(b), Minv=M, free=T(free), tol=1e-8, maxit=5000, check=1)
+        assert abs(int(info.iters[0]) - int(gsc["pcg_it_%s" % ld])) <= 1
+        assert relmax(x.cpu().numpy() + upm, gsc["pcg_u_%s" % ld]) < 1e-6
+
+
+def test_pcg_batched_vs_superlu(gsc, sc12):
+    """All 9 loads of s = 2 as one batch (3 BC sets, per-system masks) to 1e-12 vs the reference's SuperLU."""
+    lat, dl, Kn, Tv = sc12
+    free, ups = [], []
+    for ld in G.LOADS:
+        fixed, up, _ = _bc(lat, ld, 2)
+        free.append(~fixed)
+        ups.append(np.where(fixed[:, None], up, 0.0))
+    free, ups = np.array(free), np.array(ups)
+    Kt, Tt = T(Kn), T(Tv)
+    b = -core.kmv(dl, T(ups), Kt, Tt) * T(free)[..., None]
+    M = core.block_jacobi(dl, Kt, Tt, torch.float64)
+    x, info = core.cg(dl, Kt, Tt, b, Minv=M, free=T(free), tol=1e-12, maxit=5000, check=1)
+    assert (info.status == 0).all() and (info.relres <= 1e-12).all()
+    u = x.cpu().numpy() + ups
+    cid = G.block_index(lat.ijk, 2, (6, 6, 6))
+    for l, ld in enumerate(G.LOADS):
+        ub = np.stack([np.bincount(cid, u[l][:, k]) for k in range(3)], 1) / 8
+        assert relmax(ub, gsc["u_2_%s" % ld]) < 1e-9
+
+
+def test_mixed_precision_ir(gsc, sc12):
+    """FP32 inner PCG + FP64 refinement to 1e-8: FP64 true residual <= 1e-8 and <= 1e-6 rel. error vs SuperLU."""
+    lat, dl, Kn, Tv = sc12
+    for ld in ("k_xx", "lr_tx", "tb_tz"):
+        s = 3 if ld == "tb_tz" else 2
+        fixed, up, _ = _bc(lat, ld, s)
+        free = ~fixed
+        upm = np.where(fixed[:, None], up, 0.0)
+        b = -O.sc_apply(lat, upm, Kn, Tv) * free[:, None]
+        x, info = core.ir(dl, T(Kn), T(Tv), T(b), free=T(free), tol=1e-8, inner_tol=1e-5)
+        xn = x.cpu().numpy()
+        r = (b - O.sc_apply(lat, xn, Kn, Tv)) * free[:, None]
+        assert np.linalg.norm(r) <= 1.0000001e-8 * np.linalg.norm(b)
+        assert info.relres[0] <= 1e-8 and info.status[0] == 0
+        assert rel_l2(xn + upm, gsc["ufull_%d_%s" % (s, ld)]) < 1e-6
+
+
+def test_cg_2d_per_dof_mask(gsq):
+    """cg2plain.cg_mf semantics (per-DOF mask, initial-residual test) in FP64, and the mixed-precision path."""
+    lat = G.Lattice2D("square", 16, 12, 1.0)
+    dl = core.DeviceLattice(lat)
+    fd, up = gsq["cg_fixed"], gsq["cg_up"]
+    ub = np.where(fd, up, 0.0)
+    Kn, Tv = gsq["Kn"], gsq["Tv"]
+    b = (-O.sq_kmv(lat, ub, Kn, Tv) * (~fd).ravel()).reshape(-1, 2)
+    x, info = core.cg(dl, T(Kn), T(Tv), T(b), free=T(~fd), tol=1e-10, maxit=100000, check=1, precheck=True)
+    assert abs(int(info.iters[0]) - int(gsq["cg_it"])) <= 1
+    assert relmax(x.cpu().numpy().ravel() + ub.ravel(), gsq["cg_u"]) < 1e-8
+    x, info = core.ir(dl, T(Kn), T(Tv), T(b), free=T(~fd), tol=1e-10, inner_tol=1e-5, precond=False)
+    assert rel_l2(x.cpu().numpy().ravel() + ub.ravel(), gsq["lu_u"]) < 1e-6
+
+
+def test_cg_freezing_and_status():
+    """Systems converge independently; a zero right-hand side returns 0 iterations; maxit reports NOT_CONVERGED."""
+    lat = G.LatticeGeom(6, 6, 6)
+    dl = core.DeviceLattice(lat)
+    rng = np.random.default_rng(0)
+    Kn, Tv = sym_params(lat, rng)
+    fixed, up, _ = _bc(lat, "k_xx", 2)
+    free = ~fixed
+    b0 = -O.sc_apply(lat, np.where(fixed[:, None], up, 0.0), Kn, Tv) * free[:, None]
+    b = np.stack([b0, 0 * b0, 3 * b0])
+    x, info = core.cg(dl, T(Kn), T(Tv), T(b), free=T(free), tol=1e-10, maxit=2000)
+    assert info.iters[1] == 0 and info.relres[1] == 0.0
+    assert info.iters[0] == info.iters[2] and (info.status == 0).all()
+    xa = x.cpu().numpy()
+    assert relmax(xa[2], 3 * xa[0]) < 1e-9 and np.abs(xa[1]).max() == 0.0
+    _, info = core.cg(dl, T(Kn), T(Tv), T(b0), free=T(free), tol=1e-14, maxit=3)
+    assert info.status[0] == 1 and info.iters[0] == 3
+
+
+# ---------------------------------------------------------------------------------------------------- gradients
+def test_grad_sc(ggrad):
+    lat = G.LatticeGeom(4, 4, 4, 2.0)
+    dl = core.DeviceLattice(lat)
+    for pre in ("g3", "g3n"):
+        gK, gT = core.bond_grad(dl, T(ggrad["g3_u"]), T(ggrad["g3_lam"]), T(ggrad[pre + "_Kn"]),
+                                T(ggrad[pre + "_Tv"]))
+        assert relmax(gK[0].cpu().numpy(), ggrad[pre + "_gK"]) < 1e-13
+        assert relmax(gT[0].cpu().numpy(), ggrad[pre + "_gT"]) < 1e-13
+
+
+def test_grad_sq(ggrad):
+    lat = G.Lattice2D("square", 6, 5, 2.0)
+    dl = core.DeviceLattice(lat)
+    gK, gT = core.bond_grad(dl, T(ggrad["g2_u"].reshape(-1, 2)), T(ggrad["g2_lam"].reshape(-1, 2)),
+                            T(ggrad["g2_Kn"]), T(ggrad["g2_Tv"]))
+    assert relmax(gK[0].cpu().numpy(), ggrad["g2_gK"]) < 1e-13
+    assert relmax(gT[0].cpu().numpy(), ggrad["g2_gT"]) < 1e-13
+
+
+def test_grad_sums_over_loads(gsc, sc12):
+    lat, dl, Kn, Tv = sc12
+    rng = np.random.default_rng(4)
+    u = rng.standard_normal((3, lat.N, 3))
+    lam = rng.standard_normal((3, lat.N, 3))
+    gK, gT = core.bond_grad(dl, T(u), T(lam), T(Kn)[None], T(Tv)[None])
+    eK = sum(O.sc_grad(lat, Kn, Tv, u[l], lam[l])[0] for l in range(3))
+    assert relmax(gK[0].cpu().numpy(), eK) < 1e-13
+
+
+# ------------------------------------------------------------------------------------------------- post-process
+def test_stress_energy(gsc, gsq, sc12):
+    lat, dl, Kn, Tv = sc12
+    u = T(gsc["u"])
+    assert relmax(core.stress(dl, u, T(Kn), T(Tv)).cpu().numpy(), gsc["st"]) < 1e-13
+    assert relmax(core.energy(dl, u, T(Kn), T(Tv)).cpu().numpy(), gsc["U"]) < 1e-13
+    lat2 = G.Lattice2D("square", 16, 12, 1.0)
+    d2 = core.DeviceLattice(lat2)
+    u2 = T(gsq["u"].reshape(-1, 2))
+    assert relmax(core.stress(d2, u2, T(gsq["Kn"]), T(gsq["Tv"])).cpu().numpy(), gsq["stress"]) < 1e-13
+    assert relmax(core.energy(d2, u2, T(gsq["Kn"]), T(gsq["Tv"])).cpu().numpy(), gsq["energy"]) < 1e-13
