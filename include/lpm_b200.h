@@ -104,6 +104,19 @@ int lpm_kmv_sq_f64(const lpm_lattice* lat, const double* u, const double* Kn, co
 int lpm_kmv_sq_f32(const lpm_lattice* lat, const float* u, const float* Kn, const float* Tv, int32_t coef_layout,
                    const lpm_batch* batch, float* out, void* scratch, size_t scratch_bytes, void* stream);
 
+/* Size of the device array behind lpm_kmv_f64_static: 32 MiB on every GPU that loads the library, held until exit. */
+#define LPM_KMV_STATIC_SCRATCH_BYTES (32u * 1024u * 1024u)
+
+/* FP64 out = K u exactly as lpm_kmv_sc_f64 (lat->dim == 3) or lpm_kmv_sq_f64 (lat->dim == 2), but with no scratch
+ * argument and no device allocation: for callers that cannot allocate device memory or pass a buffer (an FFI host
+ * that only forwards device pointers it was given, a fixed memory budget, a path where a cudaMalloc would stall).
+ * No counterpart in the reference.  Limit: 4 * nsys * n doubles must fit LPM_KMV_STATIC_SCRATCH_BYTES (nsys * n <=
+ * 1,048,576, e.g. nine systems of a 48^3 box), else LPM_ERR_WORKSPACE.  The first call on a device looks up the
+ * array's device address with that device current, so make it before any stream capture.  Every call on a device
+ * shares the array: calls whose work overlaps on the GPU race and must be serialised by the caller. */
+int lpm_kmv_f64_static(const lpm_lattice* lat, const double* u, const double* Kn, const double* Tv,
+                       int32_t coef_layout, const lpm_batch* batch, double* out, void* stream);
+
 /* --------------------------------------------------------------------------------------------- preconditioner */
 /* Diagonal blocks D (nset, n, d, d) of K (optional output, FP64) and their inverses Minv (nset, n, d, d).
  * SC: coarse3d/lin3d.py:239-301 (k_block_diag, k_block_jacobi), coarse3d/torch_lpm3d.py:22-33,94-106 (inv3,
