@@ -35,6 +35,7 @@ extern "C" {
 #define LPM_ERR_ARG (-1)         /* invalid argument (null pointer, bad size, unsupported combination) */
 #define LPM_ERR_WORKSPACE (-2)   /* workspace / scratch buffer too small */
 #define LPM_ERR_UNSUPPORTED (-3) /* lattice or precision not supported by this entry point */
+#define LPM_ERR_TIMEOUT (-5)     /* a bounded device-side wait expired (the kernel stopped and returned) */
 
 /* per-system solver status */
 #define LPM_STATUS_OK 0
@@ -128,13 +129,14 @@ int lpm_block_jacobi_f32(const lpm_lattice* lat, const double* Kn, const double*
                          int32_t nset, float* Minv, double* D_or_null, void* stream);
 
 /* ------------------------------------------------------------------------------------------------ batched CG */
-/* Workspace bytes of lpm_cg_batched_* (precond: 1 if Minv will be passed). */
-int64_t lpm_cg_workspace_bytes(const lpm_lattice* lat, int32_t nsys, int32_t precision, int32_t precond);
+/* Workspace bytes of lpm_cg_batched_* for this lattice and batch (precond: 1 if Minv will be passed). */
+int64_t lpm_cg_workspace_bytes(const lpm_lattice* lat, const lpm_batch* batch, int32_t precision, int32_t precond);
 
 /* Batched (P)CG on the free DOFs: K_ff x_f = b_f for every system, x updated in place (x must be zero on fixed DOFs;
  * x_is_zero = 1 skips the initial K x).  Replaces coarse3d/lin3d.py:464-532 (_pcg / solve_pcg),
  * timing/t3d/cgplain.py:11-55 (cg3), timing/t2d/cg2plain.py:11-49 (cg_mf), timing/t2d/solver2d.py:349-421
- * (pcg_mf) and coarse3d/torch_lpm3d.py:109-140 (SCT.pcg).  Minv NULL = plain CG.  Outputs per system: iterations,
+ * (pcg_mf) and coarse3d/torch_lpm3d.py:109-140 (SCT.pcg).  Minv NULL = plain CG.  Full SC boxes with packed
+ * (LPM_LAYOUT_SOA) coefficients run on the fused single-pass operator.  Outputs per system: iterations,
  * relative residual |r|/|b| at the last test, LPM_STATUS_*.  coef_layout applies to Kn/Tv. */
 int lpm_cg_batched_f64(const lpm_lattice* lat, const double* Kn, const double* Tv, int32_t coef_layout,
                        const lpm_batch* batch, const double* Minv, const uint8_t* mask, const double* b, double* x,
@@ -146,7 +148,7 @@ int lpm_cg_batched_f32(const lpm_lattice* lat, const float* Kn, const float* Tv,
                        int32_t* iters, double* relres, int32_t* status, void* stream);
 
 /* ------------------------------------------------------------------------------- mixed-precision refinement */
-int64_t lpm_ir_workspace_bytes(const lpm_lattice* lat, int32_t nsys, int32_t precond);
+int64_t lpm_ir_workspace_bytes(const lpm_lattice* lat, const lpm_batch* batch, int32_t precond);
 
 /* FP32 inner PCG + FP64 iterative refinement to |b - K x| <= tol |b| on the FP64 operator.
  * Kn64/Tv64: FP64 coefficients (coef_layout64); Kn32/Tv32: the same packed to FP32 SoA (lpm_pack_coef_f32);

@@ -49,12 +49,12 @@ _SIGS = {
     "lpm_kmv_sq_f32": ([_P(Lattice), _c_p, _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p, _c_sz, _c_p], ctypes.c_int),
     "lpm_block_jacobi_f64": ([_P(Lattice), _c_p, _c_p, _c_i32, _c_i32, _c_p, _c_p, _c_p], ctypes.c_int),
     "lpm_block_jacobi_f32": ([_P(Lattice), _c_p, _c_p, _c_i32, _c_i32, _c_p, _c_p, _c_p], ctypes.c_int),
-    "lpm_cg_workspace_bytes": ([_P(Lattice), _c_i32, _c_i32, _c_i32], _c_i64),
+    "lpm_cg_workspace_bytes": ([_P(Lattice), _P(Batch), _c_i32, _c_i32], _c_i64),
     "lpm_cg_batched_f64": ([_P(Lattice), _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p, _c_p, _c_p, _c_i32, _P(CgOpts),
                             _c_p, _c_sz, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
     "lpm_cg_batched_f32": ([_P(Lattice), _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p, _c_p, _c_p, _c_i32, _P(CgOpts),
                             _c_p, _c_sz, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
-    "lpm_ir_workspace_bytes": ([_P(Lattice), _c_i32, _c_i32], _c_i64),
+    "lpm_ir_workspace_bytes": ([_P(Lattice), _P(Batch), _c_i32], _c_i64),
     "lpm_ir_batched": ([_P(Lattice), _c_p, _c_p, _c_i32, _c_p, _c_p, _c_p, _P(Batch), _c_p, _c_p, _c_p, _P(IrOpts),
                         _c_p, _c_sz, _c_p, _c_p, _c_p, _P(_c_i32), _c_p], ctypes.c_int),
     "lpm_grad_scratch_bytes": ([_P(Lattice), _c_i32], _c_i64),

@@ -230,13 +230,13 @@ def cg(dl, Kn, Tv, b, x=None, Minv=None, free=None, tol=1e-10, maxit=20000, chec
     xf = torch.zeros_like(bf) if x is None else _flat_vec(x, dl).to(dt).clone()
     lib = L.load()
     prec = L.LPM_F64 if dt == _F64 else L.LPM_F32
-    ws = _scratch(lib.lpm_cg_workspace_bytes(dl.ref, nsys, prec, int(Minv is not None)), bf.device)
+    b_ = _batch(nsys, rps, nmask)
+    ws = _scratch(lib.lpm_cg_workspace_bytes(dl.ref, ctypes.byref(b_), prec, int(Minv is not None)), bf.device)
     it = torch.zeros(nsys, dtype=torch.int32, device=bf.device)
     rel = torch.zeros(nsys, dtype=_F64, device=bf.device)
     st = torch.zeros(nsys, dtype=torch.int32, device=bf.device)
     opts = L.CgOpts(float(tol), int(maxit), int(check), int(poll or max(check, 10)), int(bool(precheck)),
                     _prof_ptr(prof))
-    b_ = _batch(nsys, rps, nmask)
     fn = lib.lpm_cg_batched_f64 if prec == L.LPM_F64 else lib.lpm_cg_batched_f32
     L.check(fn(dl.ref, L.ptr(Kc), L.ptr(Tc), layout, ctypes.byref(b_), L.ptr(Minv), L.ptr(m), L.ptr(bf), L.ptr(xf),
                int(x0_zero), ctypes.byref(opts), L.ptr(ws), ws.numel(), L.ptr(it), L.ptr(rel), L.ptr(st),
@@ -265,14 +265,14 @@ def ir(dl, Kn64, Tv64, b, x=None, free=None, tol=1e-8, inner_tol=1e-5, maxit=200
     m, nmask = dof_masks(free, dl, lead)
     xf = torch.zeros_like(bf) if x is None else _flat_vec(x, dl).to(_F64).clone()
     lib = L.load()
-    ws = _scratch(lib.lpm_ir_workspace_bytes(dl.ref, nsys, int(M32 is not None)), bf.device)
+    b_ = _batch(nsys, rps, nmask)
+    ws = _scratch(lib.lpm_ir_workspace_bytes(dl.ref, ctypes.byref(b_), int(M32 is not None)), bf.device)
     it = torch.zeros(nsys, dtype=torch.int32, device=bf.device)
     rel = torch.zeros(nsys, dtype=_F64, device=bf.device)
     st = torch.zeros(nsys, dtype=torch.int32, device=bf.device)
     outer = ctypes.c_int32(0)
     opts = L.IrOpts(float(tol), float(inner_tol), int(maxit), int(max_outer), int(check), int(poll),
                     _prof_ptr(prof))
-    b_ = _batch(nsys, rps, nmask)
     L.check(lib.lpm_ir_batched(dl.ref, L.ptr(Kc), L.ptr(Tc), L.LAYOUT_REF, L.ptr(K32), L.ptr(T32), L.ptr(M32),
                                ctypes.byref(b_), L.ptr(m), L.ptr(bf), L.ptr(xf), ctypes.byref(opts), L.ptr(ws),
                                ws.numel(), L.ptr(it), L.ptr(rel), L.ptr(st), ctypes.byref(outer),

@@ -3,6 +3,7 @@
 
 #include "../../include/lpm_b200.h"
 #include "lpm_cg.h"
+#include "lpm_tma.h"
 #include "lpm_kernels.h"
 
 using namespace lpm;
@@ -81,6 +82,24 @@ int kmv_impl(int dim, const lpm_lattice* lat, const T* u, const T* Kn, const T* 
     if (L.dim != dim) return LPM_ERR_UNSUPPORTED;
     if ((rc = to_batch(batch, bt)) || (rc = to_layout(layout, L, cl))) return rc;
     if (!u || !Kn || !Tv || !out) return LPM_ERR_ARG;
+    if (dim == 3 && !L.nbr && layout == LPM_LAYOUT_SOA && tma_supported(L.nx, (int)sizeof(T)) &&
+        tma_aligned(u, Kn, Tv)) {
+        // full SC box with packed coefficients: TMA-fed single-pass operator (needs no scratch)
+        TmaArgs<T> a{};
+        a.nx = L.nx;
+        a.ny = L.ny;
+        a.nz = L.nz;
+        a.N = L.N;
+        a.nsys = bt.nsys;
+        a.rhs_per_set = bt.rhs_per_set;
+        a.nmask = bt.nmask;
+        tma_configure(a);
+        a.u = u;
+        a.Kn = Kn;
+        a.Tv = Tv;
+        a.out = out;
+        return ret(launch_sc_tma<T>(a, false, S(stream)));
+    }
     T* st = aligned<T>(scratch, scratch_bytes, (size_t)bt.nsys * L.N * 4 * sizeof(T), rc);
     if (rc) return rc;
     return ret(launch_kmv<T>(L, u, Kn, Tv, cl, bt, out, st, nullptr, S(stream)));
@@ -115,6 +134,7 @@ const char* lpm_status_string(int code)
     case LPM_ERR_ARG: return "invalid argument";
     case LPM_ERR_WORKSPACE: return "workspace or scratch buffer too small";
     case LPM_ERR_UNSUPPORTED: return "unsupported lattice or precision for this entry point";
+    case LPM_ERR_TIMEOUT: return "a bounded device-side wait expired";
     default: return code > 0 ? cudaGetErrorString((cudaError_t)code) : "unknown error";
     }
 }
@@ -182,11 +202,12 @@ int lpm_block_jacobi_f32(const lpm_lattice* lat, const double* Kn, const double*
     return ret(launch_block_jacobi<float>(L, Kn, Tv, cl, nset, Minv, D_or_null, S(stream)));
 }
 
-int64_t lpm_cg_workspace_bytes(const lpm_lattice* lat, int32_t nsys, int32_t precision, int32_t precond)
+int64_t lpm_cg_workspace_bytes(const lpm_lattice* lat, const lpm_batch* batch, int32_t precision, int32_t precond)
 {
     Lattice L;
-    if (to_lattice(lat, L) || nsys < 1) return LPM_ERR_ARG;
-    return (int64_t)cg_workspace_bytes(L, nsys, precision, precond) + 256;
+    Batch bt;
+    if (to_lattice(lat, L) || to_batch(batch, bt)) return LPM_ERR_ARG;
+    return (int64_t)cg_workspace_bytes(L, bt, precision, precond) + 256;
 }
 
 int lpm_cg_batched_f64(const lpm_lattice* lat, const double* Kn, const double* Tv, int32_t coef_layout,
@@ -207,11 +228,12 @@ int lpm_cg_batched_f32(const lpm_lattice* lat, const float* Kn, const float* Tv,
                           workspace_bytes, iters, relres, status, stream);
 }
 
-int64_t lpm_ir_workspace_bytes(const lpm_lattice* lat, int32_t nsys, int32_t precond)
+int64_t lpm_ir_workspace_bytes(const lpm_lattice* lat, const lpm_batch* batch, int32_t precond)
 {
     Lattice L;
-    if (to_lattice(lat, L) || nsys < 1) return LPM_ERR_ARG;
-    return (int64_t)ir_workspace_bytes(L, nsys, precond) + 256;
+    Batch bt;
+    if (to_lattice(lat, L) || to_batch(batch, bt)) return LPM_ERR_ARG;
+    return (int64_t)ir_workspace_bytes(L, bt, precond) + 256;
 }
 
 int lpm_ir_batched(const lpm_lattice* lat, const double* Kn64, const double* Tv64, int32_t coef_layout64,

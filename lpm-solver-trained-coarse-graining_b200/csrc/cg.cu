@@ -13,10 +13,12 @@
 // Mixed precision (iterative refinement): the true residual r = mask(b - K x) is formed in FP64 with the FP64
 // coefficients; each correction solves K d = r / |r| with the FP32 PCG to a loose tolerance; x += |r| d in FP64; the
 // stopping test is on the FP64 true residual.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
 #include "lpm_cg.h"
+#include "lpm_tma.h"
 
 namespace lpm {
 
@@ -295,67 +297,6 @@ struct Carver {
 
 inline int vec_blocks(int64_t N) { return (int)((N + VB - 1) / VB); }
 
-// Optional CUDA-event timing of the operator launches of a solve (prof != nullptr).  prof[0] += ms and prof[1] += count
-// over all launches; prof[2] += ms and prof[3] += count over the launches issued while no system had yet left the
-// active set (as last seen by the host), i.e. launches that did the full batch's work.  Events are recorded on the
-// solve's stream and read back at the host synchronisation points of the loop.
-class KmvTimer {
-  public:
-    KmvTimer(double* prof, cudaStream_t st) : prof_(prof), st_(st)
-    {
-        if (!prof_) return;
-        for (int j = 0; j < kPairs; ++j) {
-            cudaEventCreate(&a_[j]);
-            cudaEventCreate(&b_[j]);
-        }
-    }
-    ~KmvTimer()
-    {
-        if (!prof_) return;
-        for (int j = 0; j < kPairs; ++j) {
-            cudaEventDestroy(a_[j]);
-            cudaEventDestroy(b_[j]);
-        }
-    }
-    void begin(bool full)
-    {
-        if (!prof_) return;
-        if (n_ == kPairs) collect();
-        full_[n_] = full;
-        cudaEventRecord(a_[n_], st_);
-    }
-    void end()
-    {
-        if (!prof_) return;
-        cudaEventRecord(b_[n_], st_);
-        ++n_;
-    }
-    void collect()  // call after the stream reached the last recorded event
-    {
-        if (!prof_ || n_ == 0) return;
-        if (cudaEventSynchronize(b_[n_ - 1]) != cudaSuccess) return;
-        for (int j = 0; j < n_; ++j) {
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, a_[j], b_[j]);
-            prof_[0] += ms;
-            prof_[1] += 1.0;
-            if (full_[j]) {
-                prof_[2] += ms;
-                prof_[3] += 1.0;
-            }
-        }
-        n_ = 0;
-    }
-
-  private:
-    static constexpr int kPairs = 64;
-    double* prof_;
-    cudaStream_t st_;
-    cudaEvent_t a_[kPairs], b_[kPairs];
-    bool full_[kPairs];
-    int n_ = 0;
-};
-
 template <typename T>
 struct CgWork {
     T *r, *z, *p, *Ap, *st;
@@ -402,8 +343,9 @@ struct IrWork {
     size_t cg_bytes;
 };
 
-void carve_ir(Carver& cv, const Lattice& L, int nsys, bool precond, IrWork<float>& w)
+void carve_ir(Carver& cv, const Lattice& L, const Batch& bt, bool precond, IrWork<float>& w)
 {
+    const int nsys = bt.nsys;
     const size_t nv = (size_t)nsys * L.N * L.dim;
     w.r64 = cv.take<double>(nv);
     w.Kx = cv.take<double>(nv);
@@ -416,7 +358,7 @@ void carve_ir(Carver& cv, const Lattice& L, int nsys, bool precond, IrWork<float
     w.it_in = cv.take<int>(nsys);
     w.st_in = cv.take<int>(nsys);
     w.rel_in = cv.take<double>(nsys);
-    w.cg_bytes = cg_workspace_bytes(L, nsys, LPM_F32, precond);
+    w.cg_bytes = cg_workspace_bytes(L, bt, LPM_F32, precond);
     w.cg_ws = cv.take<char>(w.cg_bytes);
 }
 
@@ -447,24 +389,34 @@ void launch_init(dim3 g, cudaStream_t st, bool precond, const Batch& bt, int64_t
 
 }  // namespace
 
-size_t cg_workspace_bytes(const Lattice& L, int nsys, int precision, int precond)
+static bool fused_ok(const Lattice& L, const CoefLayout& cl, int elem_bytes)
+{
+    return L.dim == 3 && L.nbr == nullptr && cl.slot_stride == L.N && cl.site_stride == 1 &&
+           tma_supported(L.nx, elem_bytes);
+}
+
+size_t cg_workspace_bytes(const Lattice& L, const Batch& bt, int precision, int precond)
 {
     Carver cv{nullptr, 0};
     if (precision == LPM_F32) {
         CgWork<float> w;
-        carve_cg<float>(cv, L, nsys, precond != 0, w);
+        carve_cg<float>(cv, L, bt.nsys, precond != 0, w);
     } else {
         CgWork<double> w;
-        carve_cg<double>(cv, L, nsys, precond != 0, w);
+        carve_cg<double>(cv, L, bt.nsys, precond != 0, w);
     }
-    return cv.off + 256;
+    size_t n = cv.off + 256;
+    const int es = precision == LPM_F32 ? 4 : 8;
+    if (L.dim == 3 && L.nbr == nullptr && tma_supported(L.nx, es))
+        n = std::max(n, cg_fused_workspace_bytes(L, bt.nsys, bt.rhs_per_set, es, precond));
+    return n;
 }
 
-size_t ir_workspace_bytes(const Lattice& L, int nsys, int precond)
+size_t ir_workspace_bytes(const Lattice& L, const Batch& bt, int precond)
 {
     Carver cv{nullptr, 0};
     IrWork<float> w;
-    carve_ir(cv, L, nsys, precond != 0, w);
+    carve_ir(cv, L, bt, precond != 0, w);
     return cv.off + 256;
 }
 
@@ -474,6 +426,9 @@ int cg_solve(const Lattice& L, const T* Kn, const T* Tv, const CoefLayout& cl, c
              int* iters, double* relres, int* status, cudaStream_t st)
 {
     if (o.maxit < 0 || o.check < 1 || o.poll < 1 || bt.nsys < 1) return LPM_ERR_ARG;
+    if (fused_ok(L, cl, (int)sizeof(T)) && tma_aligned(Kn, Tv, b))
+        return cg_solve_fused<T>(L, Kn, Tv, bt, Minv, mask, b, x, x_is_zero, o, ws, ws_bytes, iters, relres, status,
+                                 st);
     const bool precond = Minv != nullptr;
     // align the caller's buffer
     char* base = static_cast<char*>(ws);
@@ -554,7 +509,7 @@ int ir_solve(const Lattice& L, const double* Kn64, const double* Tv64, const Coe
     const size_t shift = (256 - (reinterpret_cast<uintptr_t>(base) & 255)) & 255;
     Carver cv{base + shift, 0};
     IrWork<float> w;
-    carve_ir(cv, L, bt.nsys, Minv32 != nullptr, w);
+    carve_ir(cv, L, bt, Minv32 != nullptr, w);
     if (cv.off + shift > ws_bytes) return LPM_ERR_WORKSPACE;
     const int ns = bt.nsys;
     const int64_t N = L.N;

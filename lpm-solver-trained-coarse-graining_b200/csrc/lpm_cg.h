@@ -24,8 +24,69 @@ struct CgScalars {
     int nblk;          // partial blocks per system of the vector kernels
 };
 
-size_t cg_workspace_bytes(const Lattice& L, int nsys, int precision, int precond);
-size_t ir_workspace_bytes(const Lattice& L, int nsys, int precond);
+// Optional CUDA-event timing of the operator launches of a solve (prof != nullptr).  prof[0] += ms and prof[1] += count
+// over all launches; prof[2] += ms and prof[3] += count over the launches issued while no system had yet left the
+// active set (as last seen by the host), i.e. launches that did the full batch's work.  Events are recorded on the
+// solve's stream and read back at the host synchronisation points of the loop.
+class KmvTimer {
+  public:
+    KmvTimer(double* prof, cudaStream_t st) : prof_(prof), st_(st)
+    {
+        if (!prof_) return;
+        for (int j = 0; j < kPairs; ++j) {
+            cudaEventCreate(&a_[j]);
+            cudaEventCreate(&b_[j]);
+        }
+    }
+    ~KmvTimer()
+    {
+        if (!prof_) return;
+        for (int j = 0; j < kPairs; ++j) {
+            cudaEventDestroy(a_[j]);
+            cudaEventDestroy(b_[j]);
+        }
+    }
+    void begin(bool full)
+    {
+        if (!prof_) return;
+        if (n_ == kPairs) collect();
+        full_[n_] = full;
+        cudaEventRecord(a_[n_], st_);
+    }
+    void end()
+    {
+        if (!prof_) return;
+        cudaEventRecord(b_[n_], st_);
+        ++n_;
+    }
+    void collect()  // call after the stream reached the last recorded event
+    {
+        if (!prof_ || n_ == 0) return;
+        if (cudaEventSynchronize(b_[n_ - 1]) != cudaSuccess) return;
+        for (int j = 0; j < n_; ++j) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, a_[j], b_[j]);
+            prof_[0] += ms;
+            prof_[1] += 1.0;
+            if (full_[j]) {
+                prof_[2] += ms;
+                prof_[3] += 1.0;
+            }
+        }
+        n_ = 0;
+    }
+
+  private:
+    static constexpr int kPairs = 64;
+    double* prof_;
+    cudaStream_t st_;
+    cudaEvent_t a_[kPairs], b_[kPairs];
+    bool full_[kPairs];
+    int n_ = 0;
+};
+
+size_t cg_workspace_bytes(const Lattice& L, const Batch& bt, int precision, int precond);
+size_t ir_workspace_bytes(const Lattice& L, const Batch& bt, int precond);
 
 template <typename T>
 int cg_solve(const Lattice& L, const T* Kn, const T* Tv, const CoefLayout& cl, const Batch& bt, const T* Minv,

@@ -43,12 +43,14 @@ def test_argument_validation():
     bad = L.Lattice(4, 8, 8, 8, 512, None)        # dim 4
     assert lib.lpm_kmv_scratch_bytes(ctypes.byref(bad), 0, 1) < 0
     wrong_n = L.Lattice(3, 8, 8, 8, 100, None)    # full box with n != nx*ny*nz
-    assert lib.lpm_cg_workspace_bytes(ctypes.byref(wrong_n), 1, 0, 0) < 0
+    one = L.Batch(1, 1, 1, 0)
+    assert lib.lpm_cg_workspace_bytes(ctypes.byref(wrong_n), ctypes.byref(one), 0, 0) < 0
     sq_nz = L.Lattice(2, 8, 8, 3, 192, None)      # 2D with nz != 1
-    assert lib.lpm_ir_workspace_bytes(ctypes.byref(sq_nz), 1, 1) < 0
+    assert lib.lpm_ir_workspace_bytes(ctypes.byref(sq_nz), ctypes.byref(one), 1) < 0
     ok = L.Lattice(3, 8, 8, 8, 512, None)
     assert lib.lpm_kmv_scratch_bytes(ctypes.byref(ok), 1, 2) >= 2 * 512 * 4 * 4
-    assert lib.lpm_cg_workspace_bytes(ctypes.byref(ok), 6, 1, 1) > 0
+    six = L.Batch(6, 6, 1, 0)
+    assert lib.lpm_cg_workspace_bytes(ctypes.byref(ok), ctypes.byref(six), 1, 1) > 0
     b = L.Batch(0, 1, 1, 0)                        # nsys 0
     rc = lib.lpm_kmv_sc_f64(ctypes.byref(ok), None, None, None, 0, ctypes.byref(b), None, None, 0, None)
     assert rc == -1
