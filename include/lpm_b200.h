@@ -187,6 +187,24 @@ int lpm_stress_f64(const lpm_lattice* lat, const double* u, const double* Kn, co
 int lpm_energy_f64(const lpm_lattice* lat, const double* u, const double* Kn, const double* Tv, int32_t coef_layout,
                    const lpm_batch* batch, double* w, void* stream);
 
+/* Vector-Jacobian products of the post-processing outputs, for differentiable solves (the autograd passes of
+ * coarse3d/torch_lpm3d.py:85-92 and coarse2d/torch_lpm.py:246-258).  G: upstream gradient of the particle energy
+ * (nsys, n) or of the stress (nsys, n, 6 | 3).  Outputs: du (nsys, n, d) and parameter gradients (nset, n, slots)
+ * summed over the systems of each set (written, or added when accumulate = 1).  scratch: lpm_grad_scratch_bytes. */
+int lpm_energy_vjp_f64(const lpm_lattice* lat, const double* u, const double* G, const double* Kn, const double* Tv,
+                       int32_t coef_layout, const lpm_batch* batch, double* du, double* gKn, double* gTv,
+                       int32_t accumulate, void* scratch, size_t scratch_bytes, void* stream);
+int lpm_stress_vjp_f64(const lpm_lattice* lat, const double* u, const double* Gsig, const double* Kn,
+                       const double* Tv, int32_t coef_layout, const lpm_batch* batch, const double* l0, double V,
+                       double* du, double* gKn, double* gTv, int32_t accumulate, void* scratch, size_t scratch_bytes,
+                       void* stream);
+/* VJP of f = K u on the SC lattice (the autograd pass of coarse3d/torch_lpm3d.py:81-83): du = K^T G for upstream G
+ * (nsys, n, 3), exact also for bond parameters that are not symmetric, and the parameter gradients of sum G . K u.
+ * The square lattice's exact Hessian is symmetric (use lpm_kmv_sq_* and lpm_bond_grad_sq): LPM_ERR_UNSUPPORTED. */
+int lpm_kmv_vjp_f64(const lpm_lattice* lat, const double* u, const double* G, const double* Kn, const double* Tv,
+                    int32_t coef_layout, const lpm_batch* batch, double* du, double* gKn, double* gTv,
+                    int32_t accumulate, void* scratch, size_t scratch_bytes, void* stream);
+
 /* ------------------------------------------------------------------------------------------------ geometry */
 /* Neighbour table of a (possibly masked) box, identical to LatticeGeom.nbr / Lattice2D.nbr
  * (coarse3d/geom3d.py:38-65, coarse2d/lin2d.py:32-74): site_of (nx*ny*nz) int64 = particle id or -1,

@@ -66,6 +66,12 @@ _SIGS = {
                        ctypes.c_int),
     "lpm_energy_f64": ([_P(Lattice), _c_p, _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p], ctypes.c_int),
     "lpm_build_nbr": ([_c_i32, _c_i32, _c_i32, _c_i32, _c_i64, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
+    "lpm_energy_vjp_f64": ([_P(Lattice), _c_p, _c_p, _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p, _c_p, _c_i32, _c_p,
+                            _c_sz, _c_p], ctypes.c_int),
+    "lpm_stress_vjp_f64": ([_P(Lattice), _c_p, _c_p, _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_d, _c_p, _c_p, _c_p,
+                            _c_i32, _c_p, _c_sz, _c_p], ctypes.c_int),
+    "lpm_kmv_vjp_f64": ([_P(Lattice), _c_p, _c_p, _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p, _c_p, _c_i32, _c_p,
+                         _c_sz, _c_p], ctypes.c_int),
     "lpm_kmv_f64_static": ([_P(Lattice), _c_p, _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p], ctypes.c_int),
 }
 

@@ -207,16 +207,18 @@ def cg(dl, Kn, Tv, b, x=None, Minv=None, free=None, tol=1e-10, maxit=20000, chec
        layout=L.LAYOUT_REF, rhs_per_set=None, prof=None):
     """Batched (P)CG on the free DOFs.  b (..., N, d) zero on fixed DOFs; x start (zero if None), returned updated.
 
-    dtype of b decides the precision (float64 or float32); Kn/Tv/Minv must match it.  Returns (x, SolveInfo).
+    dtype of b decides the precision (float64 or float32); Kn/Tv/Minv must match it.  With rhs_per_set given, Kn/Tv
+    are the coefficient sets themselves ((nset, N, NN) for the reference layout, packed for SoA), systems
+    s*rhs_per_set .. (s+1)*rhs_per_set-1 using set s.  Returns (x, SolveInfo).
     """
     lead = b.shape[:-2]
     bf = _flat_vec(b, dl)
     nsys = bf.shape[0]
     dt = bf.dtype
-    if layout == L.LAYOUT_REF:
+    if layout == L.LAYOUT_REF and rhs_per_set is None:
         Kc, rps = coef_sets(Kn, dl, lead)
         Tc, _ = coef_sets(Tv, dl, lead)
-    else:
+    else:                                   # coefficient sets given explicitly, rhs_per_set systems each
         Kc, Tc = Kn.contiguous(), Tv.contiguous()
         rps = rhs_per_set or nsys // Kc.shape[0]
     if Kc.dtype != dt or Tc.dtype != dt:
@@ -336,6 +338,37 @@ def energy(dl, u, Kn, Tv):
     L.check(L.load().lpm_energy_f64(dl.ref, L.ptr(uf), L.ptr(Kc), L.ptr(Tc), L.LAYOUT_REF, ctypes.byref(b_),
                                     L.ptr(out), L.stream_ptr(uf.device)), "lpm_energy_f64")
     return out.reshape(tuple(lead) + (dl.N,))
+
+
+def post_vjp(dl, which, u, G, Kn, Tv):
+    """VJP of the particle energy (which="energy", G (..., N)), the stress (which="stress", G (..., N, 6|3)) or, on the
+    SC lattice, of K u (which="apply", G (..., N, 3): du = K^T G, exact for non-symmetric bond parameters).
+
+    Returns (du shaped like u, gKn, gTv (nset, N, NN) summed over the systems of each coefficient set)."""
+    lead = u.shape[:-2]
+    uf = _flat_vec(u.to(_F64), dl)
+    nsys = uf.shape[0]
+    Kc, rps = coef_sets(Kn.to(_F64), dl, lead)
+    Tc, _ = coef_sets(Tv.to(_F64), dl, lead)
+    Gf = G.to(_F64).reshape((nsys, dl.N) if which == "energy" else (nsys, dl.N, -1)).contiguous()
+    du = torch.empty_like(uf)
+    gK = torch.empty_like(Kc)
+    gT = torch.empty_like(Tc)
+    lib = L.load()
+    scr = _scratch(lib.lpm_grad_scratch_bytes(dl.ref, nsys), uf.device)
+    b_ = _batch(nsys, rps)
+    if which == "apply":
+        rc = lib.lpm_kmv_vjp_f64(dl.ref, L.ptr(uf), L.ptr(Gf), L.ptr(Kc), L.ptr(Tc), L.LAYOUT_REF, ctypes.byref(b_),
+                                 L.ptr(du), L.ptr(gK), L.ptr(gT), 0, L.ptr(scr), scr.numel(), L.stream_ptr(uf.device))
+    elif which == "energy":
+        rc = lib.lpm_energy_vjp_f64(dl.ref, L.ptr(uf), L.ptr(Gf), L.ptr(Kc), L.ptr(Tc), L.LAYOUT_REF, ctypes.byref(b_),
+                                    L.ptr(du), L.ptr(gK), L.ptr(gT), 0, L.ptr(scr), scr.numel(), L.stream_ptr(uf.device))
+    else:
+        rc = lib.lpm_stress_vjp_f64(dl.ref, L.ptr(uf), L.ptr(Gf), L.ptr(Kc), L.ptr(Tc), L.LAYOUT_REF, ctypes.byref(b_),
+                                    L.ptr(dl.l0), dl.V, L.ptr(du), L.ptr(gK), L.ptr(gT), 0, L.ptr(scr), scr.numel(),
+                                    L.stream_ptr(uf.device))
+    L.check(rc, "lpm_%s_vjp_f64" % which)
+    return du.reshape(u.shape), gK, gT
 
 
 def build_nbr(lat, device="cuda"):

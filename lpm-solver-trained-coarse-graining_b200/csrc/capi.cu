@@ -326,6 +326,48 @@ int lpm_energy_f64(const lpm_lattice* lat, const double* u, const double* Kn, co
     return ret(launch_energy(L, u, Kn, Tv, cl, bt, w, S(stream)));
 }
 
+static int vjp_impl(int which, const lpm_lattice* lat, const double* u, const double* G, const double* Kn,
+                    const double* Tv, int32_t layout, const lpm_batch* batch, const double* l0, double V, double* du,
+                    double* gKn, double* gTv, int32_t accumulate, void* scratch, size_t scratch_bytes, void* stream)
+{
+    Lattice L;
+    Batch bt;
+    CoefLayout cl;
+    int rc = to_lattice(lat, L);
+    if (rc || (rc = to_batch(batch, bt)) || (rc = to_layout(layout, L, cl))) return rc;
+    if (!u || !G || !Kn || !Tv || !du || !gKn || !gTv) return LPM_ERR_ARG;
+    if (which == 1 && (!l0 || !(V > 0.0))) return LPM_ERR_ARG;
+    double* st = aligned<double>(scratch, scratch_bytes, 2 * (size_t)bt.nsys * L.N * 4 * sizeof(double), rc);
+    if (rc) return rc;
+    return ret(launch_post_vjp(L, which, u, G, Kn, Tv, cl, bt, l0, V, du, gKn, gTv, st, accumulate, S(stream)));
+}
+
+int lpm_energy_vjp_f64(const lpm_lattice* lat, const double* u, const double* G, const double* Kn, const double* Tv,
+                       int32_t coef_layout, const lpm_batch* batch, double* du, double* gKn, double* gTv,
+                       int32_t accumulate, void* scratch, size_t scratch_bytes, void* stream)
+{
+    return vjp_impl(0, lat, u, G, Kn, Tv, coef_layout, batch, nullptr, 1.0, du, gKn, gTv, accumulate, scratch,
+                    scratch_bytes, stream);
+}
+
+int lpm_stress_vjp_f64(const lpm_lattice* lat, const double* u, const double* Gsig, const double* Kn,
+                       const double* Tv, int32_t coef_layout, const lpm_batch* batch, const double* l0, double V,
+                       double* du, double* gKn, double* gTv, int32_t accumulate, void* scratch, size_t scratch_bytes,
+                       void* stream)
+{
+    return vjp_impl(1, lat, u, Gsig, Kn, Tv, coef_layout, batch, l0, V, du, gKn, gTv, accumulate, scratch,
+                    scratch_bytes, stream);
+}
+
+int lpm_kmv_vjp_f64(const lpm_lattice* lat, const double* u, const double* G, const double* Kn, const double* Tv,
+                    int32_t coef_layout, const lpm_batch* batch, double* du, double* gKn, double* gTv,
+                    int32_t accumulate, void* scratch, size_t scratch_bytes, void* stream)
+{
+    if (lat && lat->dim != 3) return LPM_ERR_UNSUPPORTED;
+    return vjp_impl(2, lat, u, G, Kn, Tv, coef_layout, batch, nullptr, 1.0, du, gKn, gTv, accumulate, scratch,
+                    scratch_bytes, stream);
+}
+
 int lpm_build_nbr(int32_t dim, int32_t nx, int32_t ny, int32_t nz, int64_t n, const int64_t* site_of,
                   const int64_t* sites, int64_t* nbr, void* stream)
 {

@@ -63,6 +63,12 @@ cudaError_t launch_stress(const Lattice& L, const double* u, const double* Kn, c
 cudaError_t launch_energy(const Lattice& L, const double* u, const double* Kn, const double* Tv, const CoefLayout& cl,
                           const Batch& bt, double* w, cudaStream_t st);
 
+// VJPs of the particle energy (which = 0, G (nsys, N)) or stress (which = 1, G (nsys, N, 6 or 3)): du (nsys, N, d)
+// and parameter gradients (nset, N, NN) summed over the systems of each set.  scratch: 2 * nsys * N * 4 doubles.
+cudaError_t launch_post_vjp(const Lattice& L, int which, const double* u, const double* G, const double* Kn,
+                            const double* Tv, const CoefLayout& cl, const Batch& bt, const double* l0, double V,
+                            double* du, double* gK, double* gT, double* scratch, int acc, cudaStream_t st);
+
 // Neighbour table (n, NN) int64 of a masked box, same values as the reference's LatticeGeom.nbr.
 cudaError_t launch_build_nbr(int dim, int nx, int ny, int nz, int64_t n, const int64_t* site_of, const int64_t* sites,
                              int64_t* nbr, cudaStream_t st);

@@ -38,6 +38,7 @@ struct Site {
 template <int DIM>
 struct GridNb {
     static constexpr bool structured = true;
+    static constexpr int dim = DIM;
     int nx, ny, nz;
     __device__ __forceinline__ bool get(const Site& p, int k, int64_t& q) const
     {
@@ -53,6 +54,7 @@ struct GridNb {
 template <int DIM>
 struct TableNb {
     static constexpr bool structured = false;
+    static constexpr int dim = DIM;
     const int32_t* nbr;
     __device__ __forceinline__ bool get(const Site& p, int k, int64_t& q) const
     {

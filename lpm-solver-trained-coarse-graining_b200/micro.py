@@ -124,6 +124,6 @@ def grf3(nx, ny, nz, corr, phi, rng):
     f = rng.standard_normal((nz + 2 * p, ny + 2 * p, nx + 2 * p))
     k2 = (np.fft.fftfreq(f.shape[0])[:, None, None] ** 2 + np.fft.fftfreq(f.shape[1])[None, :, None] ** 2 +
           np.fft.rfftfreq(f.shape[2])[None, None, :] ** 2)
-    f = np.fft.irfftn(np.fft.rfftn(f) * np.exp(-2.0 * (np.pi * corr) ** 2 * k2), s=f.shape)
+    f = np.fft.irfftn(np.fft.rfftn(f) * np.exp(-2.0 * (np.pi * corr) ** 2 * k2), s=f.shape, axes=(0, 1, 2))
     f = f[p:p + nz, p:p + ny, p:p + nx]
     return (f > np.quantile(f, 1.0 - phi)).astype(np.int64).ravel(), dict(kind="grf", corr=corr)

@@ -245,6 +245,25 @@ def part_grad():
     e = (torch.tensor(lam) * op.apply(torch.tensor(u), Kt, Tt)).sum()
     gK, gT = torch.autograd.grad(e, (Kt, Tt))
     out.update(g3n_Kn=Kns, g3n_Tv=Tvs, g3n_gK=gK.numpy(), g3n_gT=gT.numpy())
+    # ---- 3D: autograd of stress / energy / apply (vector-Jacobian products) on a masked-free 5x4x3 box ----
+    latv = G.LatticeGeom(5, 4, 3, 1.0)
+    opv = T3.SCT(latv, "cpu")
+    rv = np.random.default_rng(13)
+    Knv = rv.uniform(0.5, 1.5, (latv.N, 18)) * latv.valid
+    Tvv = rv.uniform(-0.1, 0.1, (latv.N, 18)) * latv.valid
+    uv = rv.standard_normal((2, latv.N, 3))
+    Gs = rv.standard_normal((2, latv.N, 6))
+    Ge = rv.standard_normal((2, latv.N))
+    Gf = rv.standard_normal((2, latv.N, 3))
+    for name, fn, Gw in (("st", opv.stress, Gs), ("en", opv.energy, Ge), ("ap", opv.apply, Gf)):
+        ut = torch.tensor(uv, requires_grad=True)
+        Kt = torch.tensor(Knv, requires_grad=True)
+        Tt = torch.tensor(Tvv, requires_grad=True)
+        e = (fn(ut, Kt, Tt) * torch.tensor(Gw)).sum()
+        du, dK, dT = torch.autograd.grad(e, (ut, Kt, Tt))
+        out.update({"v3%s_du" % name: du.numpy(), "v3%s_dK" % name: dK.numpy(), "v3%s_dT" % name: dT.numpy(),
+                    "v3%s_G" % name: Gw})
+    out.update(v3_Kn=Knv, v3_Tv=Tvv, v3_u=uv)
     # ---- 3D: full differentiable coarse solve (LinSolve through CoarseT.run), 9 loads, tol 1e-13 ----
     cm = T3.CoarseT(nc, s, device="cpu")
     torch.manual_seed(0)
@@ -292,6 +311,24 @@ def part_grad():
     gK, gT = torch.autograd.grad(e, (Kt, Tt))
     out.update(g2_Kn=Kn2, g2_Tv=Tv2, g2_u=u2, g2_lam=l2, g2_gK=gK.numpy(), g2_gT=gT.numpy(),
                g2_Ku=(Kd @ torch.tensor(u2)).detach().numpy())
+    # stress / energy-density VJPs of the 2D model (bond_forces-based, torch_lpm.py:231-258)
+    m7 = T2.CoarseT(7, 5, 1, device="cpu")
+    l7 = m7.lat
+    r7 = np.random.default_rng(17)
+    K7 = r7.uniform(0.3, 0.6, (1, l7.N, 8)) * l7.valid
+    T7 = r7.uniform(-0.05, 0.05, (1, l7.N, 8)) * l7.valid
+    u7 = r7.standard_normal((1, 2 * l7.N))
+    Gs7 = r7.standard_normal((1, l7.N, 3))
+    Ge7 = r7.standard_normal((1, l7.N))
+    for name, fn, Gw in (("st", m7.stress, Gs7), ("en", m7.energy_density, Ge7)):
+        ut = torch.tensor(u7, requires_grad=True)
+        Kt = torch.tensor(K7, requires_grad=True)
+        Tt = torch.tensor(T7, requires_grad=True)
+        e = (fn(ut, Kt, Tt) * torch.tensor(Gw)).sum()
+        du, dK, dT = torch.autograd.grad(e, (ut, Kt, Tt))
+        out.update({"v2%s_du" % name: du.numpy(), "v2%s_dK" % name: dK.numpy(), "v2%s_dT" % name: dT.numpy(),
+                    "v2%s_G" % name: Gw})
+    out.update(v2_Kn=K7, v2_Tv=T7, v2_u=u7)
     # full CoarseT.run + losses gradient (check_gradient.py style; nc = 8, s = 2, B = 2)
     m8 = T2.CoarseT(8, 8, 2, device="cpu")
     lat8 = m8.lat
