@@ -82,6 +82,34 @@ int kmv_impl(int dim, const lpm_lattice* lat, const T* u, const T* Kn, const T* 
     if (L.dim != dim) return LPM_ERR_UNSUPPORTED;
     if ((rc = to_batch(batch, bt)) || (rc = to_layout(layout, L, cl))) return rc;
     if (!u || !Kn || !Tv || !out) return LPM_ERR_ARG;
+    if constexpr (sizeof(T) == 4) {
+        if (dim == 3 && !L.nbr && layout == LPM_LAYOUT_SOA && pair_supported(L.nx) && tma_aligned(u, Kn, Tv)) {
+            // full SC box, packed FP32 coefficients: pair-packed operator on pair-layout copies in the scratch
+            const int npp = (bt.rhs_per_set + 1) / 2, nset = (bt.nsys + bt.rhs_per_set - 1) / bt.rhs_per_set;
+            const size_t nvp = (size_t)nset * npp * L.N * 6;
+            float* up = aligned<float>(scratch, scratch_bytes, 2 * nvp * sizeof(float), rc);
+            if (rc) return rc;
+            if (nset * npp > 65535) return LPM_ERR_UNSUPPORTED;
+            PairArgs a{};
+            a.nx = L.nx;
+            a.ny = L.ny;
+            a.nz = L.nz;
+            a.N = L.N;
+            a.nsys = bt.nsys;
+            a.rhs_per_set = bt.rhs_per_set;
+            a.npp = npp;
+            a.npair = nset * npp;
+            a.zchunk = pair_zchunk(L.nx, L.ny, L.nz, a.npair);
+            a.u = up;
+            a.Kn = Kn;
+            a.Tv = Tv;
+            a.out = up + nvp;
+            cudaError_t e = pair_pack(u, up, L.N, bt.nsys, bt.rhs_per_set, S(stream));
+            if (e == cudaSuccess) e = launch_sc_pair(a, false, S(stream));
+            if (e == cudaSuccess) e = pair_unpack(up + nvp, out, L.N, bt.nsys, bt.rhs_per_set, S(stream));
+            return ret(e);
+        }
+    }
     if (dim == 3 && !L.nbr && layout == LPM_LAYOUT_SOA && tma_supported(L.nx, (int)sizeof(T)) &&
         tma_aligned(u, Kn, Tv)) {
         // full SC box with packed coefficients: TMA-fed single-pass operator (needs no scratch)
@@ -156,7 +184,9 @@ int64_t lpm_kmv_scratch_bytes(const lpm_lattice* lat, int32_t precision, int32_t
     Lattice L;
     if (to_lattice(lat, L) || nsys < 1) return LPM_ERR_ARG;
     const size_t es = precision == LPM_F32 ? 4 : 8;
-    return (int64_t)((size_t)nsys * L.N * 4 * es + 256);
+    // FP32: room for the two pair-layout copies of the pair-packed operator (at most nsys pairs of 6 values)
+    const size_t per = precision == LPM_F32 ? 12 : 4;
+    return (int64_t)((size_t)nsys * L.N * per * es + 256);
 }
 
 int lpm_kmv_sc_f64(const lpm_lattice* lat, const double* u, const double* Kn, const double* Tv, int32_t coef_layout,

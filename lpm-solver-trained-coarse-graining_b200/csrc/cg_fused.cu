@@ -5,8 +5,10 @@
 //              tests convergence every `check` iterations and freezes converged systems
 //   p-update:  x += alpha p;  p = mask(M r) + beta p   (z is recomputed from r instead of being stored)
 // A thread of the vector kernels handles one particle for a group of up to 16 systems of one coefficient set, so
-// the 3x3 preconditioner block is read once per particle and group (Minv repacked to (nset, 9, N)).  Vectors are
-// (nsys, N, 3).  Reductions are deterministic (per-block partials summed in fixed order by a last block).
+// the 3x3 preconditioner block is read once per particle and group (Minv repacked to (nset, 9, N)).  x, r and b are
+// (nsys, N, 3).  In FP32 the operator is the pair-packed kernel (kmv_pair.cu) and p, Ap live in its pair layout
+// (npair, N, 3, 2); its output is unmasked, so the update masks Ap (p stays zero on fixed DOFs, so p.Ap needs no
+// mask).  Reductions are deterministic (per-block partials summed in fixed order by a last block).
 #include <algorithm>
 
 #include "lpm_tma.h"
@@ -32,7 +34,22 @@ struct VecGeom {
     int64_t N;
     int nsys, rps, nmask;
     int ngrp;  // system groups per set = ceil(rps / GRP)
+    int npp;   // pairs per set (pair layout of p and Ap)
 };
+
+// Index of component a of particle i of system s in p / Ap: (nsys, N, 3), or the pair layout (npair, N, 3, 2).
+template <bool PAIRED>
+__device__ __forceinline__ int64_t vix(const VecGeom& G, int s, int64_t i, int a)
+{
+    if constexpr (!PAIRED) {
+        return ((int64_t)s * G.N + i) * 3 + a;
+    } else {
+        const int set = s / G.rps, j = s - set * G.rps;
+        const int64_t pr = (int64_t)set * G.npp + (j >> 1);
+        return ((pr * G.N + i) * 3 + a) * 2 + (j & 1);
+    }
+}
+
 
 struct Group {
     int gid, set, s0, nsg;
@@ -99,7 +116,7 @@ __device__ __forceinline__ void precond(const T* m9, const uint8_t* m, const T* 
 }
 
 // ------------------------------------------------------------------------------------------------------- init
-template <typename T, bool PREC>
+template <typename T, bool PREC, bool PAIRED>
 __global__ void __launch_bounds__(VB) k_fcg_init(VecGeom G, const T* __restrict__ b, const T* __restrict__ Ax,
                                                  const uint8_t* __restrict__ mask, const T* __restrict__ Ms,
                                                  T* __restrict__ r, T* __restrict__ p, FcgScalars sc, double* part,
@@ -127,7 +144,7 @@ __global__ void __launch_bounds__(VB) k_fcg_init(VecGeom G, const T* __restrict_
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const T bv = b[o + a];
-            T w = Ax ? bv - Ax[o + a] : bv;
+            T w = Ax ? bv - Ax[vix<PAIRED>(G, s, i, a)] : bv;
             if (m && !m[a]) w = T(0);
             rv[a] = w;
             vals[j][0] += (double)bv * (double)bv;
@@ -136,7 +153,7 @@ __global__ void __launch_bounds__(VB) k_fcg_init(VecGeom G, const T* __restrict_
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             r[o + a] = rv[a];
-            p[o + a] = zv[a];
+            p[vix<PAIRED>(G, s, i, a)] = zv[a];
             vals[j][1] += (double)rv[a] * (double)zv[a];
             vals[j][2] += (double)rv[a] * (double)rv[a];
         }
@@ -169,7 +186,7 @@ __global__ void __launch_bounds__(VB) k_fcg_init(VecGeom G, const T* __restrict_
 }
 
 // ----------------------------------------------------------------------------------------------------- update
-template <typename T, bool PREC>
+template <typename T, bool PREC, bool PAIRED>
 __global__ void __launch_bounds__(VB) k_fcg_update(VecGeom G, int it, int check, int maxit, double tol,
                                                    const uint8_t* __restrict__ mask, const T* __restrict__ Ms,
                                                    T* __restrict__ r, const T* __restrict__ Ap, FcgScalars sc,
@@ -196,13 +213,15 @@ __global__ void __launch_bounds__(VB) k_fcg_update(VecGeom G, int it, int check,
         if (!sc.act[s]) continue;
         const int64_t o = ((int64_t)s * N + i) * 3;
         const T al = (T)sc.alpha[s];
+        const uint8_t* m = mask ? mask + ((int64_t)(s % G.nmask) * N + i) * 3 : nullptr;
         T rv[3], zv[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            rv[a] = r[o + a] - al * Ap[o + a];
+            const T ap = (m && !m[a]) ? T(0) : Ap[vix<PAIRED>(G, s, i, a)];
+            rv[a] = r[o + a] - al * ap;
             r[o + a] = rv[a];
         }
-        precond<T, PREC>(m9, mask ? mask + ((int64_t)(s % G.nmask) * N + i) * 3 : nullptr, rv, zv);
+        precond<T, PREC>(m9, m, rv, zv);
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             vals[j][0] += (double)rv[a] * (double)zv[a];
@@ -244,7 +263,7 @@ __global__ void __launch_bounds__(VB) k_fcg_update(VecGeom G, int it, int check,
 }
 
 // --------------------------------------------------------------------------------------------------- p-update
-template <typename T, bool PREC>
+template <typename T, bool PREC, bool PAIRED>
 __global__ void __launch_bounds__(VB) k_fcg_pupdate(VecGeom G, const uint8_t* __restrict__ mask,
                                                     const T* __restrict__ Ms, T* __restrict__ x,
                                                     const T* __restrict__ r, T* __restrict__ p, FcgScalars sc)
@@ -265,7 +284,7 @@ __global__ void __launch_bounds__(VB) k_fcg_pupdate(VecGeom G, const uint8_t* __
         const int64_t o = ((int64_t)s * N + i) * 3;
         T pv[3];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) pv[a] = p[o + a];
+        for (int a = 0; a < 3; ++a) pv[a] = p[vix<PAIRED>(G, s, i, a)];
         if (alpha != 0.0) {
             const T al = (T)alpha;
 #pragma unroll
@@ -283,7 +302,7 @@ __global__ void __launch_bounds__(VB) k_fcg_pupdate(VecGeom G, const uint8_t* __
         precond<T, PREC>(m9, mask ? mask + ((int64_t)(s % G.nmask) * N + i) * 3 : nullptr, rv, zv);
         const T be = (T)sc.beta[s];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) p[o + a] = zv[a] + be * pv[a];
+        for (int a = 0; a < 3; ++a) p[vix<PAIRED>(G, s, i, a)] = zv[a] + be * pv[a];
     }
 }
 
@@ -310,15 +329,27 @@ struct FWork {
     int* err;
 };
 
+// FP32 boxes run the pair-packed operator (p and Ap in the pair layout); FP64 the TMA operator.
+template <typename T>
+bool use_pairs(const Lattice& L)
+{
+    return sizeof(T) == 4 && pair_supported(L.nx);
+}
+
 template <typename T>
 void carve(Carve& c, const Lattice& L, int nsys, int rps, bool precond, FWork<T>& w)
 {
-    const size_t nv = (size_t)nsys * L.N * 3;
     const int nset = (nsys + rps - 1) / rps;
+    const int npp = (rps + 1) / 2;
+    const bool paired = use_pairs<T>(L);
+    const size_t nv = (size_t)nsys * L.N * 3;
+    const size_t nvp = paired ? (size_t)nset * npp * L.N * 6 : nv;
     const int nb = (int)((L.N + VB - 1) / VB);
+    const int dots = paired ? pair_dot_blocks_max(L.nx, L.ny, L.nz)
+                            : tma_dot_blocks_max(L.nx, L.ny, L.nz, (int)sizeof(T));
     w.r = c.take<T>(nv);
-    w.p = c.take<T>(nv);
-    w.Ap = c.take<T>(nv);
+    w.p = c.take<T>(nvp);
+    w.Ap = c.take<T>(nvp);
     w.Ms = precond ? c.take<T>((size_t)nset * 9 * L.N) : nullptr;
     w.sc.nsys = nsys;
     w.sc.bn = c.take<double>(nsys);
@@ -331,9 +362,62 @@ void carve(Carve& c, const Lattice& L, int nsys, int rps, bool precond, FWork<T>
     w.sc.nconv = c.take<unsigned>(1);
     w.vpart = c.take<double>((size_t)3 * nsys * nb);
     w.vcnt = c.take<unsigned>((size_t)nset * ((rps + GRP - 1) / GRP) + 1);
-    w.mpart = c.take<double>((size_t)nsys * tma_dot_blocks_max(L.nx, L.ny, L.nz, (int)sizeof(T)));
+    w.mpart = c.take<double>((size_t)nsys * dots);
     w.mcnt = c.take<unsigned>(nsys);
     w.err = c.take<int>(1);
+}
+
+// One operator launch: out = K u, with the alpha-step epilogue when epi.
+template <typename T>
+struct Operator {
+    bool paired;
+    TmaArgs<T> ta;
+    PairArgs pa;
+    cudaError_t run(const T* u, T* out, bool epi, int it, cudaStream_t st)
+    {
+        if constexpr (sizeof(T) == 4) {
+            if (paired) {
+                PairArgs a = pa;
+                a.u = u;
+                a.out = out;
+                a.it = it;
+                if (!epi) {
+                    a.act = nullptr;
+                    a.part = nullptr;
+                    a.has_sc = 0;
+                }
+                return launch_sc_pair(a, epi, st);
+            }
+        }
+        TmaArgs<T> a = ta;
+        a.u = u;
+        a.out = out;
+        a.it = it;
+        if (!epi) {
+            a.mask = nullptr;
+            a.act = nullptr;
+            a.part = nullptr;
+            a.has_sc = 0;
+        }
+        return launch_sc_tma<T>(a, epi, st);
+    }
+};
+
+template <typename T, bool PREC, bool PAIRED>
+void launch_vec_init(dim3 vg, cudaStream_t st, const VecGeom& G, const T* b, const T* Ax, const uint8_t* mask,
+                     FWork<T>& w, double tol, int precheck)
+{
+    k_fcg_init<T, PREC, PAIRED><<<vg, VB, 0, st>>>(G, b, Ax, mask, w.Ms, w.r, w.p, w.sc, w.vpart, w.vcnt, tol,
+                                                    precheck);
+}
+
+template <typename T, bool PREC, bool PAIRED>
+void launch_vec_iter(dim3 vg, cudaStream_t st, const VecGeom& G, int it, const lpm_cg_opts& o, const uint8_t* mask,
+                     T* x, FWork<T>& w)
+{
+    k_fcg_update<T, PREC, PAIRED><<<vg, VB, 0, st>>>(G, it, o.check, o.maxit, o.tol, mask, w.Ms, w.r, w.Ap, w.sc,
+                                                      w.vpart, w.vcnt);
+    k_fcg_pupdate<T, PREC, PAIRED><<<vg, VB, 0, st>>>(G, mask, w.Ms, x, w.r, w.p, w.sc);
 }
 
 }  // namespace
@@ -370,71 +454,97 @@ int cg_solve_fused(const Lattice& L, const T* Kn, const T* Tv, const Batch& bt, 
     const int64_t N = L.N;
     const int nset = (bt.nsys + bt.rhs_per_set - 1) / bt.rhs_per_set;
     const int vgrp = (bt.rhs_per_set + GRP - 1) / GRP;
-    const VecGeom G{N, bt.nsys, bt.rhs_per_set, bt.nmask, vgrp};
+    const int npp = (bt.rhs_per_set + 1) / 2;
+    const bool paired = use_pairs<T>(L);
+    const VecGeom G{N, bt.nsys, bt.rhs_per_set, bt.nmask, vgrp, npp};
     const int nb = (int)((N + VB - 1) / VB);
     cudaError_t e = cudaMemsetAsync(w.vcnt, 0, sizeof(unsigned) * (nset * vgrp + 1), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.mcnt, 0, sizeof(unsigned) * bt.nsys, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.sc.nconv, 0, sizeof(unsigned), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.err, 0, sizeof(int), st);
+    if (e == cudaSuccess && paired)  // dummy lanes of the pair layout stay zero
+        e = cudaMemsetAsync(w.p, 0, sizeof(T) * (size_t)nset * npp * N * 6, st);
     if (e != cudaSuccess) return (int)e;
     if (precond) k_repack_M<T><<<dim3(nb, nset), VB, 0, st>>>(Minv, w.Ms, N);
 
-    TmaArgs<T> ta{};
-    ta.nx = L.nx;
-    ta.ny = L.ny;
-    ta.nz = L.nz;
-    ta.N = N;
-    ta.nsys = bt.nsys;
-    ta.rhs_per_set = bt.rhs_per_set;
-    ta.nmask = bt.nmask;
-    tma_configure(ta);
-    ta.Kn = Kn;
-    ta.Tv = Tv;
-    ta.err = w.err;
+    Operator<T> op{};
+    op.paired = paired;
+    if (paired) {
+        PairArgs& a = op.pa;
+        a.nx = L.nx;
+        a.ny = L.ny;
+        a.nz = L.nz;
+        a.N = N;
+        a.nsys = bt.nsys;
+        a.rhs_per_set = bt.rhs_per_set;
+        a.npp = npp;
+        a.npair = nset * npp;
+        a.zchunk = pair_zchunk(L.nx, L.ny, L.nz, a.npair);
+        a.Kn = reinterpret_cast<const float*>(Kn);
+        a.Tv = reinterpret_cast<const float*>(Tv);
+        a.act = w.sc.act;
+        a.part = w.mpart;
+        a.cnt = w.mcnt;
+        a.scv = w.sc;
+        a.has_sc = 1;
+        a.err = w.err;
+    } else {
+        TmaArgs<T>& a = op.ta;
+        a.nx = L.nx;
+        a.ny = L.ny;
+        a.nz = L.nz;
+        a.N = N;
+        a.nsys = bt.nsys;
+        a.rhs_per_set = bt.rhs_per_set;
+        a.nmask = bt.nmask;
+        tma_configure(a);
+        a.Kn = Kn;
+        a.Tv = Tv;
+        a.mask = mask;
+        a.act = w.sc.act;
+        a.part = w.mpart;
+        a.cnt = w.mcnt;
+        a.scv = w.sc;
+        a.has_sc = 1;
+        a.err = w.err;
+    }
     if (!x_is_zero) {
-        TmaArgs<T> a0 = ta;
-        a0.u = x;
-        a0.out = w.Ap;
-        if ((e = launch_sc_tma<T>(a0, false, st)) != cudaSuccess) return (int)e;
+        const T* xin = x;
+        if (paired) {
+            if constexpr (sizeof(T) == 4) {
+                if ((e = pair_pack(x, w.p, N, bt.nsys, bt.rhs_per_set, st)) != cudaSuccess) return (int)e;
+                xin = w.p;
+            }
+        }
+        if ((e = op.run(xin, w.Ap, false, 0, st)) != cudaSuccess) return (int)e;
     }
     const dim3 vg(nb, nset * vgrp);
+    const T* Ax = x_is_zero ? nullptr : w.Ap;
     if (precond)
-        k_fcg_init<T, true><<<vg, VB, 0, st>>>(G, b, x_is_zero ? nullptr : w.Ap, mask, w.Ms, w.r, w.p, w.sc, w.vpart,
-                                               w.vcnt, o.tol, o.precheck);
+        paired ? launch_vec_init<T, true, true>(vg, st, G, b, Ax, mask, w, o.tol, o.precheck)
+               : launch_vec_init<T, true, false>(vg, st, G, b, Ax, mask, w, o.tol, o.precheck);
     else
-        k_fcg_init<T, false><<<vg, VB, 0, st>>>(G, b, x_is_zero ? nullptr : w.Ap, mask, w.Ms, w.r, w.p, w.sc, w.vpart,
-                                                w.vcnt, o.tol, o.precheck);
+        paired ? launch_vec_init<T, false, true>(vg, st, G, b, Ax, mask, w, o.tol, o.precheck)
+               : launch_vec_init<T, false, false>(vg, st, G, b, Ax, mask, w, o.tol, o.precheck);
     if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
     unsigned nconv = 0;
     e = cudaMemcpyAsync(&nconv, w.sc.nconv, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return (int)e;
 
-    ta.u = w.p;
-    ta.out = w.Ap;
-    ta.mask = mask;
-    ta.act = w.sc.act;
-    ta.part = w.mpart;
-    ta.cnt = w.mcnt;
-    ta.scv = w.sc;
-    ta.has_sc = 1;
     KmvTimer timer(o.prof, st);
     int rc = LPM_OK;
     for (int it = 1; it <= o.maxit && nconv < (unsigned)bt.nsys; ++it) {
-        ta.it = it;
         timer.begin(nconv == 0);
-        e = launch_sc_tma<T>(ta, true, st);
+        e = op.run(w.p, w.Ap, true, it, st);
         timer.end();
         if (e != cudaSuccess) return (int)e;
-        if (precond) {
-            k_fcg_update<T, true><<<vg, VB, 0, st>>>(G, it, o.check, o.maxit, o.tol, mask, w.Ms, w.r, w.Ap, w.sc,
-                                                     w.vpart, w.vcnt);
-            k_fcg_pupdate<T, true><<<vg, VB, 0, st>>>(G, mask, w.Ms, x, w.r, w.p, w.sc);
-        } else {
-            k_fcg_update<T, false><<<vg, VB, 0, st>>>(G, it, o.check, o.maxit, o.tol, mask, w.Ms, w.r, w.Ap, w.sc,
-                                                      w.vpart, w.vcnt);
-            k_fcg_pupdate<T, false><<<vg, VB, 0, st>>>(G, mask, w.Ms, x, w.r, w.p, w.sc);
-        }
+        if (precond)
+            paired ? launch_vec_iter<T, true, true>(vg, st, G, it, o, mask, x, w)
+                   : launch_vec_iter<T, true, false>(vg, st, G, it, o, mask, x, w);
+        else
+            paired ? launch_vec_iter<T, false, true>(vg, st, G, it, o, mask, x, w)
+                   : launch_vec_iter<T, false, false>(vg, st, G, it, o, mask, x, w);
         if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
         if (it % o.poll == 0 || it == o.maxit) {
             e = cudaMemcpyAsync(&nconv, w.sc.nconv, sizeof(unsigned), cudaMemcpyDeviceToHost, st);

@@ -1,0 +1,634 @@
+// Pair-packed TMA-fed SC operator for the FP32 CG engine: out = K u for the two systems of a pair at once.
+//
+// Same decomposition as the TMA operator (code-force form of coarse3d/lin3d.py:126-149):
+//   f_i   = own_i + sum_k n_k (A_q^c + Tv_ik B_q^c),   A = TS/2, B = S/2 (shell-1 values pre-scaled by 1/sqrt2)
+//   own_i = sum_k 2 Kn_ik dL_ik n_k + sum_c (A_i^c s_i^c + B_i^c T_i^c)
+// but the two systems of a pair travel together in one 64-bit register and are processed by the packed FP32x2
+// instructions of sm_100a (add/sub/mul/fma .rn.f32x2): every shared-memory load of u and every add or FMA on a
+// displacement-dependent quantity serves both systems, and the bond coefficients (shared by the pair) are loaded
+// once.
+//
+// Vector layout ("pair layout"): (npair, N, 3, 2) FP32, element (pair, i, a, lane), pair = set * npp + j / 2 and
+// lane = j % 2 for system j of a coefficient set (npp = ceil(rhs_per_set / 2)).  The second lane of the last pair of
+// a set with an odd number of systems is a dummy the caller keeps at zero.
+//
+// The output is not masked: the CG engine keeps p zero on fixed DOFs (so p.Ap needs no mask) and masks Ap where it
+// updates r.
+//
+// Tile: 16 x 16 sites, 256 threads; a warp covers rows ty and ty + 2 of 16 columns (the two half-warps then read
+// Tv rows 48 floats apart: no shared-memory bank conflicts).  The CTA marches in z over a chunk of planes; step z
+// computes the shell sums of plane z+1 (tile + 1-site ring) with the own terms of the tile (phase 1), then the
+// neighbour terms and the output of plane z (phase 2).  Shared memory, 187 KB (one CTA per SM):
+//   u      : 4 planes x 20 rows x 120 floats (sites x0-2 .. x0+17, pair layout)
+//   Tv     : 2 planes x 18 slots x 18 rows x 24 sites (x0-4 .. x0+19)
+//   Kn     : 2 planes x 18 slots x 16 rows x 24 sites (x0 .. x0+23)
+//   (B, A) : 3 planes x 2 shells x 18 x 18 sites x float4 {B lane 0, B lane 1, A lane 0, A lane 1}
+// All global inputs arrive by TMA (no multicast), issued by one thread a plane ahead into rings guarded by
+// mbarriers.  Bonds that leave the box: in warps where every lane's site has all 18 bonds no masking is done;
+// otherwise dL of missing bonds is zeroed by selection, so whatever the coefficients of missing bonds hold is
+// multiplied by zero, as in the reference.  (B, A) of sites outside the box is zero.  Every mbarrier wait is bounded;
+// on expiry the kernel records an error code, waits (bounded) for the copies it issued, and stops computing.
+//
+// Epilogue (EPI): per-system u.out partials in FP32 per thread, reduced in FP64 deterministically; the last block of
+// a system runs the CG alpha step.
+#include <cudaTypedefs.h>
+
+#include <type_traits>
+
+#include "lpm_fused.h"
+#include "lpm_ptx.cuh"
+#include "lpm_tma.h"
+
+namespace lpm {
+
+namespace {
+
+using namespace ptx;
+
+constexpr int PX = 16, PY = 16, PNT = PX * PY;
+constexpr int PUW = 6 * (PX + 4);  // floats per u row: sites x0-2 .. x0+17, 3 components x 2 lanes
+constexpr int PUH = PY + 4;        // u rows y0-2 .. y0+17
+constexpr int PSW = PX + 2, PSH = PY + 2, PSPL = PSW * PSH;  // tile + 1-site ring
+constexpr int PTVW = 24;           // Tv sites per row (x0-4 .. x0+19)
+constexpr int PKNW = 24;           // Kn sites per row (x0 .. x0+23)
+constexpr int PNRING = PSPL - PNT;
+constexpr unsigned FULL18 = 0x3FFFFu;
+
+constexpr size_t PU_SLOT = (size_t)PUH * PUW * 4;
+constexpr size_t PTV_SLOT = (size_t)18 * PSH * PTVW * 4;
+constexpr size_t PKN_SLOT = (size_t)18 * PY * PKNW * 4;
+constexpr size_t PBA_SLOT = (size_t)2 * PSPL * 16;
+constexpr size_t POFF_TV = 4 * PU_SLOT;
+constexpr size_t POFF_KN = POFF_TV + 2 * PTV_SLOT;
+constexpr size_t POFF_BA = POFF_KN + 2 * PKN_SLOT;
+constexpr size_t PBYTES = POFF_BA + 3 * PBA_SLOT;
+static_assert(PU_SLOT % 128 == 0 && PTV_SLOT % 128 == 0 && PKN_SLOT % 128 == 0 && PBA_SLOT % 128 == 0,
+              "TMA destinations must stay 128-byte aligned");
+static_assert(PBYTES <= 227 * 1024, "shared memory budget");
+
+__host__ __device__ constexpr unsigned dir_bits(int axis, int sgn)
+{
+    unsigned m = 0;
+    for (int k = 0; k < 18; ++k) {
+        const int d = axis == 0 ? sc_dx(k) : axis == 1 ? sc_dy(k) : sc_dz(k);
+        if (d == sgn) m |= 1u << k;
+    }
+    return m;
+}
+
+// Slot geometry: for axis slots (shell 0) the component a and sign sa; for diagonal slots (shell 1) the two
+// components a < b, their signs and the plane index of the pair (0: xy, 1: xz, 2: yz).
+struct SlotGeo {
+    int a, b, sa, sb, plane;
+};
+__host__ __device__ constexpr SlotGeo slot_geo(int k)
+{
+    const int o[3] = {sc_dx(k), sc_dy(k), sc_dz(k)};
+    SlotGeo g{-1, -1, 0, 0, -1};
+    for (int c = 0; c < 3; ++c) {
+        if (o[c] == 0) continue;
+        if (g.a < 0) {
+            g.a = c;
+            g.sa = o[c];
+        } else {
+            g.b = c;
+            g.sb = o[c];
+        }
+    }
+    if (g.b >= 0) g.plane = g.a == 0 ? (g.b == 1 ? 0 : 1) : 2;
+    return g;
+}
+
+__device__ __forceinline__ pair_t ld2(const float* p) { return *reinterpret_cast<const pair_t*>(p); }
+
+template <bool EPI>
+__global__ void __launch_bounds__(PNT, 1)
+    k_sc_pair(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ CUtensorMap tm_tv,
+              const __grid_constant__ CUtensorMap tm_kn, PairArgs P)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bars[8];  // u: 0..3, Tv: 4..5, Kn: 6..7
+    __shared__ double red[32];
+    __shared__ int abort_flag;
+    __shared__ bool last_flag;
+
+    float* su = reinterpret_cast<float*>(smem);
+    float* stv = reinterpret_cast<float*>(smem + POFF_TV);
+    float* skn = reinterpret_cast<float*>(smem + POFF_KN);
+    float4* sba = reinterpret_cast<float4*>(smem + POFF_BA);
+
+    const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31;
+    const int tx = lane & 15, ty = ((wid >> 1) << 2) + (wid & 1) + ((lane >> 4) << 1);
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const int ntx = (nx + PX - 1) / PX, nty = (ny + PY - 1) / PY;
+    const int tile = blockIdx.x % (ntx * nty), zc = blockIdx.x / (ntx * nty);
+    const int x0 = (tile % ntx) * PX, y0 = (tile / ntx) * PY;
+    const int pr = blockIdx.y + P.pair0;
+    const int set = pr / P.npp, jp = pr % P.npp;
+    const int sbase = set * P.rhs_per_set + 2 * jp;
+    int nr = P.rhs_per_set - 2 * jp;
+    nr = nr < 2 ? nr : 2;
+    if (sbase + nr > P.nsys) nr = P.nsys - sbase;
+    const int zbeg = zc * P.zchunk;
+    const int zend = min(nz, zbeg + P.zchunk);
+    const bool on0 = nr > 0 && (!P.act || P.act[sbase]);
+    const bool on1 = nr > 1 && (!P.act || P.act[sbase + 1]);
+    bool any_on = on0 || on1;
+
+    if (tid == 0) {
+        for (int b = 0; b < 8; ++b) mbar_init(&bars[b], 1);
+        fence_mbar_init();
+        abort_flag = 0;
+        if (saddr(smem) & 127u) {  // TMA destinations must be 128-byte aligned: refuse to run and report
+            abort_flag = 1;
+            if (P.err) atomicExch(P.err, 2);
+        }
+    }
+    {
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int e = tid; e < 3 * 2 * PSPL; e += PNT) sba[e] = z4;
+        // u slots standing for planes below 0 are never loaded; keep them finite
+        const int nneg = zbeg - 2 < 0 ? 2 - zbeg : 0;
+        for (int e = tid; e < nneg * (int)(PU_SLOT / 4); e += PNT) su[e] = 0.f;
+    }
+    __syncthreads();
+    if (abort_flag) any_on = false;
+
+    // ------------------------------------------------------------------------------------------ producer side
+    // Fill n of a stream lands in slot n % nslots with mbarrier parity (n / nslots) & 1.  Thread 0 issues and keeps
+    // the outstanding fills of each barrier in `pend` (bit b) / `ppar` (parity), for the drain on abort.
+    const int u0 = zbeg - 2, tv0 = zbeg - 1, kn0 = zbeg;
+    unsigned pend = 0, ppar = 0;
+    auto note = [&](int b, int parity) {
+        pend |= 1u << b;
+        ppar = (ppar & ~(1u << b)) | ((unsigned)parity << b);
+    };
+    auto issue_u = [&](int p) {
+        const int n = p - u0;
+        uint64_t* bar = &bars[n & 3];
+        if (p < 0 || p >= nz) {
+            mbar_arrive(bar);
+            return;
+        }
+        mbar_expect_arrive(bar, (uint32_t)PU_SLOT);
+        tma_load4(su + (size_t)(n & 3) * (PU_SLOT / 4), &tm_u, bar, 6 * (x0 - 2), y0 - 2, p, pr);
+        note(n & 3, (n >> 2) & 1);
+    };
+    auto issue_tv = [&](int p) {
+        const int n = p - tv0;
+        uint64_t* bar = &bars[4 + (n & 1)];
+        if (p < 0 || p >= nz) {
+            mbar_arrive(bar);
+            return;
+        }
+        mbar_expect_arrive(bar, (uint32_t)PTV_SLOT);
+        tma_load4(stv + (size_t)(n & 1) * (PTV_SLOT / 4), &tm_tv, bar, x0 - 4, y0 - 1, p, 18 * set);
+        note(4 + (n & 1), (n >> 1) & 1);
+    };
+    auto issue_kn = [&](int p) {
+        const int n = p - kn0;
+        uint64_t* bar = &bars[6 + (n & 1)];
+        if (p < 0 || p >= nz) {
+            mbar_arrive(bar);
+            return;
+        }
+        mbar_expect_arrive(bar, (uint32_t)PKN_SLOT);
+        tma_load4(skn + (size_t)(n & 1) * (PKN_SLOT / 4), &tm_kn, bar, x0, y0, p, 18 * set);
+        note(6 + (n & 1), (n >> 1) & 1);
+    };
+    // Every thread waits (bounded) for the in-range fills it is about to read; an expired wait raises the abort
+    // flag, which all threads test after the next block barrier.
+    auto wait_fill = [&](int b, int parity) {
+        if (!mbar_wait(&bars[b], (uint32_t)parity)) {
+            abort_flag = 1;
+            if (P.err) atomicExch(P.err, 1);
+        } else if (tid == 0) {
+            pend &= ~(1u << b);
+        }
+    };
+    auto wait_planes = [&](int pu, int ptv, int pkn) {
+        if (pu >= 0 && pu < nz && pu >= u0) wait_fill((pu - u0) & 3, ((pu - u0) >> 2) & 1);
+        if (ptv >= 0 && ptv < nz && ptv >= tv0) wait_fill(4 + ((ptv - tv0) & 1), ((ptv - tv0) >> 1) & 1);
+        if (pkn >= 0 && pkn < nz && pkn >= kn0 && pkn < zend) wait_fill(6 + ((pkn - kn0) & 1), ((pkn - kn0) >> 1) & 1);
+    };
+
+    auto u_slot = [&](int p) { return su + (size_t)((p - u0) & 3) * (PU_SLOT / 4); };
+    auto tv_slot = [&](int p) { return stv + (size_t)((p - tv0) & 1) * (PTV_SLOT / 4); };
+    auto kn_slot = [&](int p) { return skn + (size_t)((p - kn0) & 1) * (PKN_SLOT / 4); };
+    auto ba_slot = [&](int p) { return sba + (size_t)(((p % 3) + 3) % 3) * (PBA_SLOT / 16); };
+    auto zero_ba = [&](int p) {
+        float4* d = ba_slot(p);
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int e = tid; e < 2 * PSPL; e += PNT) d[e] = z4;
+    };
+
+    // ---------------------------------------------------------------------------------------------- phase 1
+    // Shell sums of the site (qx, qy) (ring coordinates, 0 = x0-1 / y0-1) of plane zp for both lanes, stored as
+    // (B, A); with OWN also the own terms.  Slot loop fully unrolled; signs are compile-time, so every accumulation is
+    // an add or FMA into a "plus" or "minus" accumulator.  Diagonal slots use d' = o.(u_q - u_i) unscaled.
+    pair_t own_next[3] = {0ull, 0ull, 0ull};
+    float tv_next[18];
+#pragma unroll
+    for (int k = 0; k < 18; ++k) tv_next[k] = 0.f;
+
+    auto site = [&](auto own_tag, auto mask_tag, int qx, int qy, int zp, unsigned vm, const float* tvs,
+                    const float* kns) {
+        constexpr bool OWN = decltype(own_tag)::value;
+        constexpr bool MASKED = decltype(mask_tag)::value;
+        const float* pm = u_slot(zp - 1);
+        const float* p0 = u_slot(zp);
+        const float* pp = u_slot(zp + 1);
+        const int ci = (qy + 1) * PUW + 6 * (qx + 1);
+        const pair_t ui[3] = {ld2(p0 + ci), ld2(p0 + ci + 2), ld2(p0 + ci + 4)};
+        const pair_t cpl[3] = {add2(ui[0], ui[1]), add2(ui[0], ui[2]), add2(ui[1], ui[2])};
+        const pair_t cmi[3] = {sub2(ui[0], ui[1]), sub2(ui[0], ui[2]), sub2(ui[1], ui[2])};
+        pair_t Sp0 = 0ull, Sm0 = 0ull, Sp1 = 0ull, Sm1 = 0ull, Tp0 = 0ull, Tm0 = 0ull, Tp1 = 0ull, Tm1 = 0ull;
+        pair_t fp[3] = {0ull, 0ull, 0ull}, fm[3] = {0ull, 0ull, 0ull};
+        float s0[3] = {0.f, 0.f, 0.f}, s1[3] = {0.f, 0.f, 0.f}, T0[3] = {0.f, 0.f, 0.f}, T1[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int k = 0; k < 18; ++k) {
+            const SlotGeo g = slot_geo(k);
+            const float* pl = sc_dz(k) < 0 ? pm : (sc_dz(k) > 0 ? pp : p0);
+            const int qo = ci + sc_dy(k) * PUW + 6 * sc_dx(k);
+            const float tv = tvs[k * PSH * PTVW];
+            const bool vb = !MASKED || ((vm >> k) & 1u);
+            if (sc_shell(k) == 0) {
+                pair_t t = sub2(ld2(pl + qo + 2 * g.a), ui[g.a]);  // u_q,a - u_i,a ; dL = sa t
+                if (MASKED && !vb) t = 0ull;
+                if (g.sa > 0) {
+                    Sp0 = add2(Sp0, t);
+                    Tp0 = fma2(dup(tv), t, Tp0);
+                } else {
+                    Sm0 = add2(Sm0, t);
+                    Tm0 = fma2(dup(tv), t, Tm0);
+                }
+                if constexpr (OWN) {
+                    const float kn = kns[k * PY * PKNW];
+                    fm[g.a] = fma2(dup(2.f * kn), t, fm[g.a]);  // f_a -= 2 Kn t
+                    if (vb) {
+                        s0[g.a] -= (float)g.sa;
+                        T0[g.a] -= (float)g.sa * tv;
+                    }
+                }
+            } else {
+                const pair_t qa = ld2(pl + qo + 2 * g.a), qb = ld2(pl + qo + 2 * g.b);
+                // d' = sa t with t = (u_q,a +- u_q,b) - (u_i,a +- u_i,b)
+                pair_t t = g.sa == g.sb ? sub2(add2(qa, qb), cpl[g.plane]) : sub2(sub2(qa, qb), cmi[g.plane]);
+                if (MASKED && !vb) t = 0ull;
+                if (g.sa > 0) {
+                    Sp1 = add2(Sp1, t);
+                    Tp1 = fma2(dup(tv), t, Tp1);
+                } else {
+                    Sm1 = add2(Sm1, t);
+                    Tm1 = fma2(dup(tv), t, Tm1);
+                }
+                if constexpr (OWN) {
+                    const float kn = kns[k * PY * PKNW];
+                    const pair_t kn2 = dup(kn);
+                    fm[g.a] = fma2(kn2, t, fm[g.a]);  // f_a -= sa Kn d' = Kn t
+                    if (g.sa == g.sb)
+                        fm[g.b] = fma2(kn2, t, fm[g.b]);
+                    else
+                        fp[g.b] = fma2(kn2, t, fp[g.b]);
+                    if (vb) {
+                        s1[g.a] -= (float)g.sa;
+                        s1[g.b] -= (float)g.sb;
+                        T1[g.a] -= (float)g.sa * tv;
+                        T1[g.b] -= (float)g.sb * tv;
+                    }
+                }
+            }
+            if constexpr (OWN) tv_next[k] = tv;
+        }
+        // B0 = S0/2, A0 = TS0/2; shell 1 pre-scaled by 1/sqrt2: B1w = S1'/4, A1w = TS1'/4
+        const pair_t h = dup(0.5f), q = dup(0.25f);
+        const pair_t B0 = mul2(h, sub2(Sp0, Sm0)), A0 = mul2(h, sub2(Tp0, Tm0));
+        const pair_t B1 = mul2(q, sub2(Sp1, Sm1)), A1 = mul2(q, sub2(Tp1, Tm1));
+        float4* dst = ba_slot(zp) + qy * PSW + qx;
+        float b0l, b0h, a0l, a0h, b1l, b1h, a1l, a1h;
+        unpk(B0, b0l, b0h);
+        unpk(A0, a0l, a0h);
+        unpk(B1, b1l, b1h);
+        unpk(A1, a1l, a1h);
+        dst[0] = make_float4(b0l, b0h, a0l, a0h);
+        dst[PSPL] = make_float4(b1l, b1h, a1l, a1h);
+        if constexpr (OWN) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                pair_t o = sub2(fp[a], fm[a]);
+                o = fma2(B0, dup(T0[a]), o);
+                o = fma2(B1, dup(T1[a]), o);
+                if constexpr (MASKED) {  // s_c vanishes for a site with all bonds
+                    o = fma2(A0, dup(s0[a]), o);
+                    o = fma2(A1, dup(s1[a]), o);
+                }
+                own_next[a] = o;
+            }
+        }
+    };
+
+    constexpr unsigned XN = dir_bits(0, -1), XP = dir_bits(0, 1), YN = dir_bits(1, -1), YP = dir_bits(1, 1),
+                       ZN = dir_bits(2, -1), ZP = dir_bits(2, 1);
+    auto xy_mask = [&](int X, int Y) {
+        unsigned m = FULL18;
+        if (X == 0) m &= ~XN;
+        if (X == nx - 1) m &= ~XP;
+        if (Y == 0) m &= ~YN;
+        if (Y == ny - 1) m &= ~YP;
+        return m;
+    };
+    auto z_mask = [&](int z) {
+        unsigned m = FULL18;
+        if (z == 0) m &= ~ZN;
+        if (z == nz - 1) m &= ~ZP;
+        return m;
+    };
+
+    const int gx = x0 + tx, gy = y0 + ty;
+    const bool own_xy = gx < nx && gy < ny;
+    const unsigned own_mxy = xy_mask(gx, gy);
+    const bool has_item = tid < PNRING;
+    int rqx = 0, rqy = 0;
+    if (tid < PSW) {
+        rqx = tid;
+        rqy = 0;
+    } else if (tid < 2 * PSW) {
+        rqx = tid - PSW;
+        rqy = PSH - 1;
+    } else if (tid < 2 * PSW + PY) {
+        rqx = 0;
+        rqy = tid - 2 * PSW + 1;
+    } else {
+        rqx = PSW - 1;
+        rqy = tid - 2 * PSW - PY + 1;
+    }
+    const int rX = x0 - 1 + rqx, rY = y0 - 1 + rqy;
+    const bool ring_in = has_item && rX >= 0 && rX < nx && rY >= 0 && rY < ny;
+    const unsigned ring_mxy = xy_mask(rX, rY);
+
+    using T_ = std::true_type;
+    using F_ = std::false_type;
+    auto phase1 = [&](int zp, bool own) {
+        if (zp < 0 || zp >= nz) {
+            zero_ba(zp);
+            return;
+        }
+        const unsigned zm = z_mask(zp);
+        const unsigned vm = own_mxy & zm;
+        const bool uni = __all_sync(0xffffffffu, !own_xy || vm == FULL18);
+        if (own_xy) {
+            const float* tvs = tv_slot(zp) + (ty + 1) * PTVW + tx + 4;
+            if (own) {
+                const float* kns = kn_slot(zp) + ty * PKNW + tx;
+                if (uni)
+                    site(T_{}, F_{}, tx + 1, ty + 1, zp, vm, tvs, kns);
+                else
+                    site(T_{}, T_{}, tx + 1, ty + 1, zp, vm, tvs, kns);
+            } else {
+                if (uni)
+                    site(F_{}, F_{}, tx + 1, ty + 1, zp, vm, tvs, nullptr);
+                else
+                    site(F_{}, T_{}, tx + 1, ty + 1, zp, vm, tvs, nullptr);
+            }
+        }
+        const unsigned rvm = ring_mxy & zm;
+        const bool runi = __all_sync(0xffffffffu, !ring_in || rvm == FULL18);
+        if (ring_in) {
+            const float* tvs = tv_slot(zp) + rqy * PTVW + rqx + 3;
+            if (runi)
+                site(F_{}, F_{}, rqx, rqy, zp, rvm, tvs, nullptr);
+            else
+                site(F_{}, T_{}, rqx, rqy, zp, rvm, tvs, nullptr);
+        }
+    };
+
+    // ---------------------------------------------------------------------------------------------- phase 2
+    pair_t own_cur[3] = {0ull, 0ull, 0ull};
+    float tv_cur[18];
+    pair_t dotp = 0ull;
+    auto phase2 = [&](int z) {
+        if (!own_xy) return;
+        const int64_t i = ((int64_t)z * ny + gy) * nx + gx;
+        const float4* bm = ba_slot(z - 1);
+        const float4* b0 = ba_slot(z);
+        const float4* bp = ba_slot(z + 1);
+        const int c0 = (ty + 1) * PSW + (tx + 1);
+        pair_t f[3] = {own_cur[0], own_cur[1], own_cur[2]};
+#pragma unroll
+        for (int k = 0; k < 18; ++k) {
+            const SlotGeo g = slot_geo(k);
+            const float4* pl = sc_dz(k) < 0 ? bm : (sc_dz(k) > 0 ? bp : b0);
+            const float4 v = pl[sc_shell(k) * PSPL + c0 + sc_dy(k) * PSW + sc_dx(k)];
+            const pair_t gw = fma2(dup(tv_cur[k]), pk(v.x, v.y), pk(v.z, v.w));  // zero for bonds leaving the box
+            f[g.a] = g.sa > 0 ? sub2(f[g.a], gw) : add2(f[g.a], gw);
+            if (sc_shell(k) == 1) f[g.b] = g.sb > 0 ? sub2(f[g.b], gw) : add2(f[g.b], gw);
+        }
+        pair_t* o = reinterpret_cast<pair_t*>(P.out + (((int64_t)pr * P.N + i) * 3) * 2);
+        o[0] = f[0];
+        o[1] = f[1];
+        o[2] = f[2];
+        if constexpr (EPI) {
+            const float* pu = u_slot(z) + (ty + 2) * PUW + 6 * (tx + 2);
+            dotp = fma2(ld2(pu), f[0], dotp);
+            dotp = fma2(ld2(pu + 2), f[1], dotp);
+            dotp = fma2(ld2(pu + 4), f[2], dotp);
+        }
+    };
+
+    bool ok = true;
+    if (any_on) {
+        if (tid == 0) {
+            for (int p = zbeg - 2; p <= zbeg + 1; ++p) issue_u(p);
+            issue_tv(zbeg - 1);
+            issue_tv(zbeg);
+            issue_kn(zbeg);
+            if (zbeg + 1 < zend) issue_kn(zbeg + 1);
+        }
+        wait_planes(zbeg - 2, -1, -1);
+        wait_planes(zbeg - 1, zbeg - 1, -1);
+        wait_planes(zbeg, -1, -1);
+        phase1(zbeg - 1, false);
+        __syncthreads();
+        ok = !abort_flag;
+        if (ok) {
+            if (tid == 0) {
+                fence_proxy_async();
+                if (zbeg + 2 <= zend + 1) issue_u(zbeg + 2);
+                if (zbeg + 1 <= zend) issue_tv(zbeg + 1);
+            }
+            wait_planes(zbeg + 1, zbeg, zbeg);
+            phase1(zbeg, true);
+            __syncthreads();
+            ok = !abort_flag;
+        }
+        if (ok) {
+            for (int z = zbeg; z < zend; ++z) {
+#pragma unroll
+                for (int a = 0; a < 3; ++a) own_cur[a] = own_next[a];
+#pragma unroll
+                for (int k = 0; k < 18; ++k) tv_cur[k] = tv_next[k];
+                if (tid == 0) {
+                    fence_proxy_async();
+                    if (z + 3 <= zend + 1) issue_u(z + 3);
+                    if (z + 2 <= zend) issue_tv(z + 2);
+                    if (z + 2 < zend) issue_kn(z + 2);
+                }
+                wait_planes(z + 2, z + 1, z + 1);
+                phase1(z + 1, z + 1 < zend);
+                __syncthreads();
+                if (abort_flag) {
+                    ok = false;
+                    break;
+                }
+                phase2(z);
+                __syncthreads();
+            }
+        }
+        if (!ok && tid == 0) {  // let the copies in flight land before the block's shared memory is released
+            for (int b = 0; b < 8; ++b)
+                if ((pend >> b) & 1u) mbar_wait(&bars[b], (ppar >> b) & 1u);
+        }
+    }
+
+    if constexpr (EPI) {
+        if (!P.part) return;
+        float d0, d1;
+        unpk(dotp, d0, d1);
+        const int nblk = gridDim.x;
+        for (int j = 0; j < nr; ++j) {
+            const int s = sbase + j;
+            const double v = block_sum(ok ? (double)(j == 0 ? d0 : d1) : 0.0, red);
+            if (tid == 0) {
+                P.part[(int64_t)s * nblk + blockIdx.x] = v;
+                __threadfence();
+                last_flag = atomicAdd(P.cnt + s, 1u) == (unsigned)(nblk - 1);
+            }
+            __syncthreads();
+            if (last_flag) {
+                double acc = 0.0;
+                for (int b = tid; b < nblk; b += PNT) acc += __ldcg(P.part + (int64_t)s * nblk + b);
+                acc = block_sum(acc, red);
+                if (tid == 0) {
+                    P.cnt[s] = 0u;
+                    if (P.has_sc) cg_alpha_step(P.scv, s, acc, P.it);
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+template <bool EPI>
+cudaError_t launch_pair(const PairArgs& a, cudaStream_t st)
+{
+    const int nset = (a.nsys + a.rhs_per_set - 1) / a.rhs_per_set;
+    CUtensorMap mu, mtv, mkn;
+    {
+        const uint64_t dims[4] = {(uint64_t)6 * a.nx, (uint64_t)a.ny, (uint64_t)a.nz, (uint64_t)a.npair};
+        const uint64_t str[3] = {(uint64_t)6 * a.nx * 4, (uint64_t)6 * a.nx * a.ny * 4,
+                                 (uint64_t)6 * a.nx * a.ny * a.nz * 4};
+        const uint32_t box[4] = {(uint32_t)PUW, (uint32_t)PUH, 1, 1};
+        if (!make_tensor_map4(&mu, 4, a.u, dims, str, box)) return cudaErrorInvalidValue;
+    }
+    {
+        const uint64_t dims[4] = {(uint64_t)a.nx, (uint64_t)a.ny, (uint64_t)a.nz, (uint64_t)18 * nset};
+        const uint64_t str[3] = {(uint64_t)a.nx * 4, (uint64_t)a.nx * a.ny * 4, (uint64_t)a.nx * a.ny * a.nz * 4};
+        const uint32_t btv[4] = {(uint32_t)PTVW, (uint32_t)PSH, 1, 18};
+        const uint32_t bkn[4] = {(uint32_t)PKNW, (uint32_t)PY, 1, 18};
+        if (!make_tensor_map4(&mtv, 4, a.Tv, dims, str, btv)) return cudaErrorInvalidValue;
+        if (!make_tensor_map4(&mkn, 4, a.Kn, dims, str, bkn)) return cudaErrorInvalidValue;
+    }
+    static unsigned long long attr_set = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!((attr_set >> dev) & 1ull)) {
+        cudaError_t e = cudaFuncSetAttribute(k_sc_pair<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PBYTES);
+        if (e != cudaSuccess) return e;
+        attr_set |= 1ull << dev;
+    }
+    const int ntile = ((a.nx + PX - 1) / PX) * ((a.ny + PY - 1) / PY);
+    const int nzc = (a.nz + a.zchunk - 1) / a.zchunk;
+    for (int g0 = 0; g0 < a.npair; g0 += 65535) {
+        PairArgs b = a;
+        b.pair0 = g0;
+        const int ng = a.npair - g0 < 65535 ? a.npair - g0 : 65535;
+        k_sc_pair<EPI><<<dim3(ntile * nzc, ng), PNT, PBYTES, st>>>(mu, mtv, mkn, b);
+    }
+    return cudaGetLastError();
+}
+
+// (nsys, N, 3) <-> pair layout, one thread per (particle, pair); dummy lanes are written as zero by the packer
+__global__ void k_pair_pack(const float* __restrict__ x, float* __restrict__ xp, int64_t N, int nsys, int rps, int npp)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int pr = blockIdx.y, set = pr / npp, jp = pr % npp;
+    const int s0 = set * rps + 2 * jp;
+    const bool has1 = 2 * jp + 1 < rps && s0 + 1 < nsys;
+    const float* a0 = x + ((int64_t)s0 * N + i) * 3;
+    const float* a1 = x + ((int64_t)(s0 + 1) * N + i) * 3;
+    pair_t* o = reinterpret_cast<pair_t*>(xp + ((int64_t)pr * N + i) * 6);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) o[a] = pk(a0[a], has1 ? a1[a] : 0.f);
+}
+
+__global__ void k_pair_unpack(const float* __restrict__ xp, float* __restrict__ x, int64_t N, int nsys, int rps,
+                              int npp)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int pr = blockIdx.y, set = pr / npp, jp = pr % npp;
+    const int s0 = set * rps + 2 * jp;
+    const bool has1 = 2 * jp + 1 < rps && s0 + 1 < nsys;
+    const pair_t* v = reinterpret_cast<const pair_t*>(xp + ((int64_t)pr * N + i) * 6);
+    float* a0 = x + ((int64_t)s0 * N + i) * 3;
+    float* a1 = x + ((int64_t)(s0 + 1) * N + i) * 3;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float l, h;
+        unpk(v[a], l, h);
+        a0[a] = l;
+        if (has1) a1[a] = h;
+    }
+}
+
+}  // namespace
+
+cudaError_t pair_pack(const float* x, float* xp, int64_t N, int nsys, int rps, cudaStream_t st)
+{
+    const int npp = (rps + 1) / 2, nset = (nsys + rps - 1) / rps;
+    const int npair = nset * npp;
+    if (npair > 65535) return cudaErrorInvalidValue;
+    k_pair_pack<<<dim3((unsigned)((N + 255) / 256), npair), 256, 0, st>>>(x, xp, N, nsys, rps, npp);
+    return cudaGetLastError();
+}
+
+cudaError_t pair_unpack(const float* xp, float* x, int64_t N, int nsys, int rps, cudaStream_t st)
+{
+    const int npp = (rps + 1) / 2, nset = (nsys + rps - 1) / rps;
+    const int npair = nset * npp;
+    if (npair > 65535) return cudaErrorInvalidValue;
+    k_pair_unpack<<<dim3((unsigned)((N + 255) / 256), npair), 256, 0, st>>>(xp, x, N, nsys, rps, npp);
+    return cudaGetLastError();
+}
+
+bool pair_supported(int nx) { return nx % 4 == 0 && tma_supported(nx, 4); }
+
+int pair_zchunk(int nx, int ny, int nz, int npair)
+{
+    const long long base = (long long)((nx + PX - 1) / PX) * ((ny + PY - 1) / PY) * npair;
+    int nzc = 1;
+    while (base * nzc < 2 * 148 && nz / (nzc + 1) >= 8) ++nzc;
+    return (nz + nzc - 1) / nzc;
+}
+
+int pair_dot_blocks_max(int nx, int ny, int nz) { return ((nx + PX - 1) / PX) * ((ny + PY - 1) / PY) * (nz / 8 + 1); }
+
+cudaError_t launch_sc_pair(const PairArgs& a, bool epi, cudaStream_t st)
+{
+    if (a.npair < 1 || a.npp < 1 || a.zchunk < 1) return cudaErrorInvalidValue;
+    return epi ? launch_pair<true>(a, st) : launch_pair<false>(a, st);
+}
+
+}  // namespace lpm

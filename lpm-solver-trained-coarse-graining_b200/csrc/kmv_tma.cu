@@ -27,66 +27,18 @@
 #include <type_traits>
 
 #include "lpm_fused.h"
+#include "lpm_ptx.cuh"
 #include "lpm_tma.h"
 
 namespace lpm {
 
 namespace {
 
+using namespace ptx;
+
 constexpr int TX = 32;
 constexpr int UXW = 112;  // values per u row in the window (16-byte aligned start 3*x0 - 8)
 constexpr int TVW = 40;   // sites per Tv row (start x0 - 4)
-constexpr unsigned kWaitLimit = 1u << 22;  // try_wait polls before a wait is declared expired
-
-// ------------------------------------------------------------------------------------------------- PTX helpers
-__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_arrive(uint64_t* bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(bar)) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(saddr(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait for the phase of `bar` with the given parity; false on expiry.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
-{
-    for (unsigned n = 0; n < kWaitLimit; ++n)
-        if (mbar_test(bar, parity)) return true;
-    return false;
-}
-
-__device__ __forceinline__ void tma_load4(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2,
-                                          int c3)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
-        "%5}], [%6];" ::"r"(saddr(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(saddr(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
 template <typename T>
 struct T2;
@@ -113,18 +65,6 @@ __host__ __device__ constexpr unsigned dir_mask(int axis, int sgn)
         const int d = axis == 0 ? sc_dx(k) : axis == 1 ? sc_dy(k) : sc_dz(k);
         if (d == sgn) m |= 1u << k;
     }
-    return m;
-}
-
-__device__ __forceinline__ unsigned valid_mask(int x, int y, int z, int nx, int ny, int nz)
-{
-    unsigned m = 0x3FFFFu;
-    if (x == 0) m &= ~dir_mask(0, -1);
-    if (x == nx - 1) m &= ~dir_mask(0, 1);
-    if (y == 0) m &= ~dir_mask(1, -1);
-    if (y == ny - 1) m &= ~dir_mask(1, 1);
-    if (z == 0) m &= ~dir_mask(2, -1);
-    if (z == nz - 1) m &= ~dir_mask(2, 1);
     return m;
 }
 
@@ -573,32 +513,11 @@ __global__ void __launch_bounds__(TX* TY, 1)
 }
 
 // ------------------------------------------------------------------------------------------------ host side
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
-{
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    });
-    return fn;
-}
-
 template <typename T>
 bool make_map(CUtensorMap* m, const void* base, const uint64_t dims[4], const uint64_t strides_bytes[3],
               const uint32_t box[4])
 {
-    auto fn = encode_fn();
-    if (!fn) return false;
-    const uint32_t es[4] = {1, 1, 1, 1};
-    const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
-    const CUresult r = fn(m, dt, 4, const_cast<void*>(base), dims, strides_bytes, box, es,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS;
+    return make_tensor_map4(m, (int)sizeof(T), base, dims, strides_bytes, box);
 }
 
 template <typename T, int NR, int TY, bool EPI>
@@ -644,6 +563,33 @@ cudaError_t launch_one(const TmaArgs<T>& a, int ngt, int nzc, cudaStream_t st)
 }
 
 }  // namespace
+
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+bool make_tensor_map4(CUtensorMap* m, int elem_bytes, const void* base, const uint64_t dims[4],
+                      const uint64_t strides_bytes[3], const uint32_t box[4])
+{
+    auto fn = encode_fn();
+    if (!fn) return false;
+    const uint32_t es[4] = {1, 1, 1, 1};
+    const CUtensorMapDataType dt = elem_bytes == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    const CUresult r = fn(m, dt, 4, const_cast<void*>(base), dims, strides_bytes, box, es,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
 
 bool tma_aligned(const void* a, const void* b, const void* c)
 {

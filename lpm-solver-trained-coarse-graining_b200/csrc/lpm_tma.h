@@ -1,5 +1,7 @@
 // TMA-fed fused SC operator: launch arguments and configuration helpers.
 #pragma once
+#include <cuda.h>
+
 #include "lpm_fused.h"
 
 namespace lpm {
@@ -27,6 +29,10 @@ struct TmaArgs {
     int* err;             // set to 1 if an mbarrier wait expired
 };
 
+// Tiled 4D tensor map over FP32 (elem_bytes 4) or FP64 data, no swizzle, zero fill out of bounds; false when the
+// driver entry point is missing or the encoding is rejected.
+bool make_tensor_map4(CUtensorMap* m, int elem_bytes, const void* base, const uint64_t dims[4],
+                      const uint64_t strides_bytes[3], const uint32_t box[4]);
 bool tma_supported(int nx, int elem_bytes);
 bool tma_aligned(const void* a, const void* b, const void* c);  // 16-byte aligned global bases
 int tma_group_size(int rhs_per_set, int elem_bytes);
@@ -36,6 +42,37 @@ int tma_dot_blocks_max(int nx, int ny, int nz, int elem_bytes);
 
 template <typename T>
 cudaError_t launch_sc_tma(const TmaArgs<T>& a, bool epi, cudaStream_t st);
+
+// Pair-packed FP32 operator (kmv_pair.cu): vectors in the pair layout (npair, N, 3, 2), pair = set * npp + j / 2,
+// lane = j % 2 for system j of a set; unmasked output; epilogue as above.
+struct PairArgs {
+    int nx, ny, nz;
+    int64_t N;
+    int nsys, rhs_per_set;
+    int npp;     // pairs per coefficient set = ceil(rhs_per_set / 2)
+    int npair;   // pairs in the batch = nset * npp
+    int pair0;   // first pair of this launch (grid.y chunking)
+    int zchunk;  // z planes per CTA
+    const float* u;   // pair layout
+    const float* Kn;  // (nset, 18, N)
+    const float* Tv;
+    float* out;       // pair layout
+    const int* act;
+    double* part;
+    unsigned* cnt;
+    FcgScalars scv;
+    int has_sc;
+    int it;
+    int* err;
+};
+
+bool pair_supported(int nx);
+int pair_zchunk(int nx, int ny, int nz, int npair);
+int pair_dot_blocks_max(int nx, int ny, int nz);
+cudaError_t launch_sc_pair(const PairArgs& a, bool epi, cudaStream_t st);
+// (nsys, N, 3) FP32 -> pair layout (dummy lanes written as zero) and back (real systems only); npair <= 65535.
+cudaError_t pair_pack(const float* x, float* xp, int64_t N, int nsys, int rps, cudaStream_t st);
+cudaError_t pair_unpack(const float* xp, float* x, int64_t N, int nsys, int rps, cudaStream_t st);
 
 // Fills the configuration fields of a TmaArgs for a batch (nr, ngrp, zchunk).
 template <typename T>
