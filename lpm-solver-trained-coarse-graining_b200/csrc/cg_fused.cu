@@ -34,22 +34,8 @@ struct VecGeom {
     int64_t N;
     int nsys, rps, nmask;
     int ngrp;  // system groups per set = ceil(rps / GRP)
-    int npp;   // pairs per set (pair layout of p and Ap)
+    int npp;   // pairs per set (pair layout)
 };
-
-// Index of component a of particle i of system s in p / Ap: (nsys, N, 3), or the pair layout (npair, N, 3, 2).
-template <bool PAIRED>
-__device__ __forceinline__ int64_t vix(const VecGeom& G, int s, int64_t i, int a)
-{
-    if constexpr (!PAIRED) {
-        return ((int64_t)s * G.N + i) * 3 + a;
-    } else {
-        const int set = s / G.rps, j = s - set * G.rps;
-        const int64_t pr = (int64_t)set * G.npp + (j >> 1);
-        return ((pr * G.N + i) * 3 + a) * 2 + (j & 1);
-    }
-}
-
 
 struct Group {
     int gid, set, s0, nsg;
@@ -67,17 +53,17 @@ __device__ __forceinline__ Group group_of(const VecGeom& G)
 
 // Warp-shuffle reduction of NV values per system, one barrier, per-block partials part[(v*nsys + s)*nblk + b];
 // returns true in the last block of this system group (one counter per group).
-template <int NV>
-__device__ __forceinline__ bool group_reduce(double (*vals)[NV], int nsg, int s0, int nsys, double* part,
-                                             unsigned* cnt, int gid, double* sh, bool* last)
+template <int NV, int GS = GRP, typename A = double>
+__device__ __forceinline__ bool group_reduce(A (*vals)[NV], int nsg, int s0, int nsys, double* part, unsigned* cnt,
+                                             int gid, double* sh, bool* last)
 {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
-    for (int j = 0; j < GRP; ++j) {
+    for (int j = 0; j < GS; ++j) {
         if (j >= nsg) break;
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            const double t = warp_sum(vals[j][v]);
+            const double t = warp_sum((double)vals[j][v]);
             if (lane == 0) sh[(j * NV + v) * 8 + w] = t;
         }
     }
@@ -116,7 +102,7 @@ __device__ __forceinline__ void precond(const T* m9, const uint8_t* m, const T* 
 }
 
 // ------------------------------------------------------------------------------------------------------- init
-template <typename T, bool PREC, bool PAIRED>
+template <typename T, bool PREC>
 __global__ void __launch_bounds__(VB) k_fcg_init(VecGeom G, const T* __restrict__ b, const T* __restrict__ Ax,
                                                  const uint8_t* __restrict__ mask, const T* __restrict__ Ms,
                                                  T* __restrict__ r, T* __restrict__ p, FcgScalars sc, double* part,
@@ -144,7 +130,7 @@ __global__ void __launch_bounds__(VB) k_fcg_init(VecGeom G, const T* __restrict_
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const T bv = b[o + a];
-            T w = Ax ? bv - Ax[vix<PAIRED>(G, s, i, a)] : bv;
+            T w = Ax ? bv - Ax[o + a] : bv;
             if (m && !m[a]) w = T(0);
             rv[a] = w;
             vals[j][0] += (double)bv * (double)bv;
@@ -153,7 +139,7 @@ __global__ void __launch_bounds__(VB) k_fcg_init(VecGeom G, const T* __restrict_
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             r[o + a] = rv[a];
-            p[vix<PAIRED>(G, s, i, a)] = zv[a];
+            p[o + a] = zv[a];
             vals[j][1] += (double)rv[a] * (double)zv[a];
             vals[j][2] += (double)rv[a] * (double)rv[a];
         }
@@ -185,50 +171,11 @@ __global__ void __launch_bounds__(VB) k_fcg_init(VecGeom G, const T* __restrict_
     if (threadIdx.x == 0) cnt[gr.gid] = 0u;
 }
 
-// ----------------------------------------------------------------------------------------------------- update
-template <typename T, bool PREC, bool PAIRED>
-__global__ void __launch_bounds__(VB) k_fcg_update(VecGeom G, int it, int check, int maxit, double tol,
-                                                   const uint8_t* __restrict__ mask, const T* __restrict__ Ms,
-                                                   T* __restrict__ r, const T* __restrict__ Ap, FcgScalars sc,
-                                                   double* part, unsigned* cnt)
+// Last block of a system group after the r.z / r.r reduction: beta, convergence test every `check` iterations,
+// freezing of converged or broken-down systems.
+__device__ __forceinline__ void update_tail(const VecGeom& G, const Group& gr, int it, int check, int maxit,
+                                            double tol, FcgScalars& sc, const double* part, unsigned* cnt)
 {
-    __shared__ double sh[GRP * 2 * 8];
-    __shared__ bool last;
-    const Group gr = group_of(G);
-    const int64_t N = G.N;
-    const int64_t i = (int64_t)blockIdx.x * VB + threadIdx.x;
-    double vals[GRP][2];
-    T m9[9];
-    bool any = false;
-    for (int j = 0; j < gr.nsg; ++j) any |= sc.act[gr.s0 + j] != 0;
-    if (PREC && any && i < N) {
-#pragma unroll
-        for (int e = 0; e < 9; ++e) m9[e] = Ms[((int64_t)gr.set * 9 + e) * N + i];
-    }
-#pragma unroll
-    for (int j = 0; j < GRP; ++j) {
-        vals[j][0] = vals[j][1] = 0.0;
-        if (j >= gr.nsg || i >= N) continue;
-        const int s = gr.s0 + j;
-        if (!sc.act[s]) continue;
-        const int64_t o = ((int64_t)s * N + i) * 3;
-        const T al = (T)sc.alpha[s];
-        const uint8_t* m = mask ? mask + ((int64_t)(s % G.nmask) * N + i) * 3 : nullptr;
-        T rv[3], zv[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const T ap = (m && !m[a]) ? T(0) : Ap[vix<PAIRED>(G, s, i, a)];
-            rv[a] = r[o + a] - al * ap;
-            r[o + a] = rv[a];
-        }
-        precond<T, PREC>(m9, m, rv, zv);
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            vals[j][0] += (double)rv[a] * (double)zv[a];
-            vals[j][1] += (double)rv[a] * (double)rv[a];
-        }
-    }
-    if (!group_reduce<2>(vals, gr.nsg, gr.s0, G.nsys, part, cnt, gr.gid, sh, &last)) return;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int cur = (it - 1) & 1, nxt = it & 1;
     for (int j = w; j < gr.nsg; j += VB / 32) {
@@ -262,8 +209,62 @@ __global__ void __launch_bounds__(VB) k_fcg_update(VecGeom G, int it, int check,
     if (threadIdx.x == 0) cnt[gr.gid] = 0u;
 }
 
+// ----------------------------------------------------------------------------------------------------- update
+template <typename T, bool PREC>
+__global__ void __launch_bounds__(VB) k_fcg_update(VecGeom G, int it, int check, int maxit, double tol,
+                                                   const uint8_t* __restrict__ mask, const T* __restrict__ Ms,
+                                                   T* __restrict__ r, const T* __restrict__ Ap, FcgScalars sc,
+                                                   double* part, unsigned* cnt)
+{
+    __shared__ double sh[GRP * 2 * 8];
+    __shared__ bool last;
+    const Group gr = group_of(G);
+    const int64_t N = G.N;
+    const int64_t i = (int64_t)blockIdx.x * VB + threadIdx.x;
+    double vals[GRP][2];
+    T m9[9];
+    bool any = false;
+    for (int j = 0; j < gr.nsg; ++j) any |= sc.act[gr.s0 + j] != 0;
+    if (PREC && any && i < N) {
+#pragma unroll
+        for (int e = 0; e < 9; ++e) m9[e] = Ms[((int64_t)gr.set * 9 + e) * N + i];
+    }
+    // one system: r -= alpha mask(Ap); z = mask(M r); accumulate r.z, r.r
+    auto one = [&](int s, const T* ap, int stride, double* v) {
+        const int64_t o = ((int64_t)s * N + i) * 3;
+        const T al = (T)sc.alpha[s];
+        const uint8_t* m = mask ? mask + ((int64_t)(s % G.nmask) * N + i) * 3 : nullptr;
+        T rv[3], zv[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const T apv = (m && !m[a]) ? T(0) : ap[a * stride];
+            rv[a] = r[o + a] - al * apv;
+            r[o + a] = rv[a];
+        }
+        precond<T, PREC>(m9, m, rv, zv);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            v[0] += (double)rv[a] * (double)zv[a];
+            v[1] += (double)rv[a] * (double)rv[a];
+        }
+    };
+#pragma unroll
+    for (int j = 0; j < GRP; ++j) vals[j][0] = vals[j][1] = 0.0;
+    if (i < N) {
+#pragma unroll
+        for (int j = 0; j < GRP; ++j) {
+            if (j >= gr.nsg) break;
+            const int s = gr.s0 + j;
+            if (!sc.act[s]) continue;
+            one(s, Ap + ((int64_t)s * N + i) * 3, 1, vals[j]);
+        }
+    }
+    if (!group_reduce<2>(vals, gr.nsg, gr.s0, G.nsys, part, cnt, gr.gid, sh, &last)) return;
+    update_tail(G, gr, it, check, maxit, tol, sc, part, cnt);
+}
+
 // --------------------------------------------------------------------------------------------------- p-update
-template <typename T, bool PREC, bool PAIRED>
+template <typename T, bool PREC>
 __global__ void __launch_bounds__(VB) k_fcg_pupdate(VecGeom G, const uint8_t* __restrict__ mask,
                                                     const T* __restrict__ Ms, T* __restrict__ x,
                                                     const T* __restrict__ r, T* __restrict__ p, FcgScalars sc)
@@ -274,23 +275,18 @@ __global__ void __launch_bounds__(VB) k_fcg_pupdate(VecGeom G, const uint8_t* __
     if (i >= N) return;
     T m9[9];
     bool loaded = false;
-#pragma unroll
-    for (int j = 0; j < GRP; ++j) {
-        if (j >= gr.nsg) break;
-        const int s = gr.s0 + j;
+    // one system: x += alpha p; p = mask(M r) + beta p (active systems); p values at pv[a * stride]
+    auto one = [&](int s, T* pv, int stride) -> bool {
         const double alpha = sc.alpha[s];
         const int act = sc.act[s];
-        if (alpha == 0.0 && !act) continue;
+        if (alpha == 0.0 && !act) return false;
         const int64_t o = ((int64_t)s * N + i) * 3;
-        T pv[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) pv[a] = p[vix<PAIRED>(G, s, i, a)];
         if (alpha != 0.0) {
             const T al = (T)alpha;
 #pragma unroll
-            for (int a = 0; a < 3; ++a) x[o + a] += al * pv[a];
+            for (int a = 0; a < 3; ++a) x[o + a] += al * pv[a * stride];
         }
-        if (!act) continue;
+        if (!act) return false;
         if (PREC && !loaded) {
 #pragma unroll
             for (int e = 0; e < 9; ++e) m9[e] = Ms[((int64_t)gr.set * 9 + e) * N + i];
@@ -302,7 +298,250 @@ __global__ void __launch_bounds__(VB) k_fcg_pupdate(VecGeom G, const uint8_t* __
         precond<T, PREC>(m9, mask ? mask + ((int64_t)(s % G.nmask) * N + i) * 3 : nullptr, rv, zv);
         const T be = (T)sc.beta[s];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) p[vix<PAIRED>(G, s, i, a)] = zv[a] + be * pv[a];
+        for (int a = 0; a < 3; ++a) pv[a * stride] = zv[a] + be * pv[a * stride];
+        return true;
+    };
+#pragma unroll
+    for (int j = 0; j < GRP; ++j) {
+        if (j >= gr.nsg) break;
+        const int s = gr.s0 + j;
+        if (sc.alpha[s] == 0.0 && !sc.act[s]) continue;
+        T* pp = p + ((int64_t)s * N + i) * 3;
+        T pv[3] = {pp[0], pp[1], pp[2]};
+        if (one(s, pv, 1)) {
+            pp[0] = pv[0];
+            pp[1] = pv[1];
+            pp[2] = pv[2];
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------- FP32 pair-layout kernels
+// In FP32 every vector of the engine (r, x, p, Ap) lives in the pair layout; a thread handles one particle of one
+// pair (both systems: 24 contiguous bytes per vector), a block row one pair.  The 3x3 preconditioner blocks of a set
+// are read by the blocks of its pairs at about the same time (adjacent grid rows), so they come from L2 after the
+// first.  b and x cross the solve boundary in the (nsys, N, 3) layout.
+struct PairSys {
+    int pr, set, s0, nl;  // pair, set, first system, real lanes (1 or 2)
+};
+
+__device__ __forceinline__ PairSys pair_of(const VecGeom& G)
+{
+    PairSys q;
+    q.pr = blockIdx.y;
+    q.set = q.pr / G.npp;
+    const int jp = q.pr - q.set * G.npp;
+    q.s0 = q.set * G.rps + 2 * jp;
+    q.nl = min(2, min(G.rps - 2 * jp, G.nsys - q.s0));
+    return q;
+}
+
+__device__ __forceinline__ unsigned mask_bits(const uint8_t* mask, const VecGeom& G, int s, int64_t i)
+{
+    if (!mask) return 7u;
+    const uint8_t* m = mask + ((int64_t)(s % G.nmask) * G.N + i) * 3;
+    return (m[0] ? 1u : 0u) | (m[1] ? 2u : 0u) | (m[2] ? 4u : 0u);
+}
+
+template <bool PREC>
+__device__ __forceinline__ void precond_bits(const float* m9, unsigned mb, const float* rv, float* zv)
+{
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float z = PREC ? m9[3 * a] * rv[0] + m9[3 * a + 1] * rv[1] + m9[3 * a + 2] * rv[2] : rv[a];
+        zv[a] = ((mb >> a) & 1u) ? z : 0.f;
+    }
+}
+
+// v[l][a] <-> 6 contiguous floats (a, lane)
+__device__ __forceinline__ void ld_pair(const float* src, float (*v)[3])
+{
+    const float2* q = reinterpret_cast<const float2*>(src);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float2 t = q[a];
+        v[0][a] = t.x;
+        v[1][a] = t.y;
+    }
+}
+__device__ __forceinline__ void st_pair(float* dst, const float (*v)[3])
+{
+    float2* q = reinterpret_cast<float2*>(dst);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) q[a] = make_float2(v[0][a], v[1][a]);
+}
+
+// r = mask(b - Ax), p = z = mask(M r); b.b, r.z, r.r per system; dummy lanes written as zero.
+template <bool PREC>
+__global__ void __launch_bounds__(VB) k_pair_init(VecGeom G, const float* __restrict__ b, const float* __restrict__ Ax,
+                                                  const uint8_t* __restrict__ mask, const float* __restrict__ Ms,
+                                                  float* __restrict__ r, float* __restrict__ p, FcgScalars sc,
+                                                  double* part, unsigned* cnt, double tol, int precheck)
+{
+    __shared__ double sh[2 * 3 * 8];
+    __shared__ bool last;
+    const PairSys q = pair_of(G);
+    const int64_t N = G.N;
+    const int64_t i = (int64_t)blockIdx.x * VB + threadIdx.x;
+    float vals[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+    if (i < N) {
+        const int64_t po = ((int64_t)q.pr * N + i) * 6;
+        float ax[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}}, rv[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}},
+              zv[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}}, m9[9];
+        if (Ax) ld_pair(Ax + po, ax);
+        if (PREC) {
+#pragma unroll
+            for (int e = 0; e < 9; ++e) m9[e] = Ms[((int64_t)q.set * 9 + e) * N + i];
+        }
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+            if (l >= q.nl) break;
+            const int s = q.s0 + l;
+            const unsigned mb = mask_bits(mask, G, s, i);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const float bv = b[((int64_t)s * N + i) * 3 + a];
+                rv[l][a] = ((mb >> a) & 1u) ? bv - ax[l][a] : 0.f;
+                vals[l][0] += bv * bv;
+            }
+            precond_bits<PREC>(m9, mb, rv[l], zv[l]);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                vals[l][1] += rv[l][a] * zv[l][a];
+                vals[l][2] += rv[l][a] * rv[l][a];
+            }
+        }
+        st_pair(r + po, rv);
+        st_pair(p + po, zv);
+    }
+    if (!group_reduce<3, 2, float>(vals, q.nl, q.s0, G.nsys, part, cnt, q.pr, sh, &last)) return;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int j = w; j < q.nl; j += VB / 32) {
+        const int s = q.s0 + j;
+        const double bb = row_total(part, 0, s, G.nsys, gridDim.x);
+        const double rz = row_total(part, 1, s, G.nsys, gridDim.x);
+        const double rr = row_total(part, 2, s, G.nsys, gridDim.x);
+        if (lane != 0) continue;
+        const double bn = sqrt(bb);
+        const double rel = bn > 0.0 ? sqrt(rr) / bn : 0.0;
+        const bool finite = isfinite(bn) && isfinite(rz) && isfinite(rr);
+        int act = bn > 0.0 && finite;
+        if (act && precheck && rel <= tol) act = 0;
+        sc.bn[s] = bn;
+        sc.rz[s] = rz;
+        sc.rr[s] = rr;
+        sc.alpha[s] = 0.0;
+        sc.beta[s] = 0.0;
+        sc.act[s] = act;
+        sc.iters[s] = 0;
+        sc.relres[s] = rel;
+        sc.status[s] = finite ? LPM_STATUS_OK : LPM_STATUS_BREAKDOWN;
+        if (!act) atomicAdd(sc.nconv, 1u);
+    }
+    if (threadIdx.x == 0) cnt[q.pr] = 0u;
+}
+
+// r -= alpha mask(Ap); z = mask(M r); r.z, r.r; the last block of the pair forms beta and tests convergence.
+template <bool PREC>
+__global__ void __launch_bounds__(VB) k_pair_update(VecGeom G, int it, int check, int maxit, double tol,
+                                                    const uint8_t* __restrict__ mask, const float* __restrict__ Ms,
+                                                    float* __restrict__ r, const float* __restrict__ Ap,
+                                                    FcgScalars sc, double* part, unsigned* cnt)
+{
+    __shared__ double sh[2 * 2 * 8];
+    __shared__ bool last;
+    const PairSys q = pair_of(G);
+    const int64_t N = G.N;
+    const bool act0 = sc.act[q.s0] != 0, act1 = q.nl > 1 && sc.act[q.s0 + 1] != 0;
+    float vals[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+    // grid-stride over particles: few blocks per pair, so the reduction epilogue (fence, counter) is amortised
+    for (int64_t i = (int64_t)blockIdx.x * VB + threadIdx.x; i < N && (act0 || act1); i += (int64_t)gridDim.x * VB) {
+        const int64_t po = ((int64_t)q.pr * N + i) * 6;
+        float ap[2][3], rv[2][3], m9[9];
+        ld_pair(Ap + po, ap);
+        ld_pair(r + po, rv);
+        if (PREC) {
+#pragma unroll
+            for (int e = 0; e < 9; ++e) m9[e] = Ms[((int64_t)q.set * 9 + e) * N + i];
+        }
+        const unsigned mb0 = act0 ? mask_bits(mask, G, q.s0, i) : 0u;
+        const unsigned mb1 = act1 ? mask_bits(mask, G, q.s0 + 1, i) : 0u;
+        const float al0 = (float)sc.alpha[q.s0], al1 = act1 ? (float)sc.alpha[q.s0 + 1] : 0.f;
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+            const bool on = l ? act1 : act0;
+            if (!on) continue;
+            const unsigned mb = l ? mb1 : mb0;
+            const float al = l ? al1 : al0;
+            float zv[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) rv[l][a] -= ((mb >> a) & 1u) ? al * ap[l][a] : 0.f;
+            precond_bits<PREC>(m9, mb, rv[l], zv);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                vals[l][0] += rv[l][a] * zv[a];
+                vals[l][1] += rv[l][a] * rv[l][a];
+            }
+        }
+        st_pair(r + po, rv);
+    }
+    Group gr;
+    gr.gid = q.pr;
+    gr.set = q.set;
+    gr.s0 = q.s0;
+    gr.nsg = q.nl;
+    if (!group_reduce<2, 2, float>(vals, q.nl, q.s0, G.nsys, part, cnt, q.pr, sh, &last)) return;
+    update_tail(G, gr, it, check, maxit, tol, sc, part, cnt);
+}
+
+// x += alpha p; p = mask(M r) + beta p (active systems).
+template <bool PREC>
+__global__ void __launch_bounds__(VB) k_pair_pupdate(VecGeom G, const uint8_t* __restrict__ mask,
+                                                     const float* __restrict__ Ms, float* __restrict__ x,
+                                                     const float* __restrict__ r, float* __restrict__ p,
+                                                     FcgScalars sc)
+{
+    const PairSys q = pair_of(G);
+    const int64_t N = G.N;
+    const int64_t i = (int64_t)blockIdx.x * VB + threadIdx.x;
+    if (i >= N) return;
+    const bool two = q.nl > 1;
+    const double a0d = sc.alpha[q.s0], a1d = two ? sc.alpha[q.s0 + 1] : 0.0;
+    const bool act0 = sc.act[q.s0] != 0, act1 = two && sc.act[q.s0 + 1] != 0;
+    const bool mov = a0d != 0.0 || a1d != 0.0;
+    if (!mov && !act0 && !act1) return;
+    const int64_t po = ((int64_t)q.pr * N + i) * 6;
+    float pv[2][3], xv[2][3], rv[2][3], m9[9];
+    ld_pair(p + po, pv);
+    if (mov) ld_pair(x + po, xv);
+    if (act0 || act1) {
+        ld_pair(r + po, rv);
+        if (PREC) {
+#pragma unroll
+            for (int e = 0; e < 9; ++e) m9[e] = Ms[((int64_t)q.set * 9 + e) * N + i];
+        }
+    }
+    if (mov) {
+        const float al[2] = {(float)a0d, (float)a1d};
+#pragma unroll
+        for (int l = 0; l < 2; ++l)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) xv[l][a] += al[l] * pv[l][a];
+        st_pair(x + po, xv);
+    }
+    if (act0 || act1) {
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+            const bool on = l ? act1 : act0;
+            if (!on) continue;
+            const int s = q.s0 + l;
+            float zv[3];
+            precond_bits<PREC>(m9, mask_bits(mask, G, s, i), rv[l], zv);
+            const float be = (float)sc.beta[s];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) pv[l][a] = zv[a] + be * pv[l][a];
+        }
+        st_pair(p + po, pv);
     }
 }
 
@@ -322,14 +561,14 @@ struct Carve {
 
 template <typename T>
 struct FWork {
-    T *r, *p, *Ap, *Ms;
+    T *r, *p, *Ap, *Ms, *xp;  // xp: pair-layout x (FP32 path)
     FcgScalars sc;
     double *vpart, *mpart;
     unsigned *vcnt, *mcnt;
     int* err;
 };
 
-// FP32 boxes run the pair-packed operator (p and Ap in the pair layout); FP64 the TMA operator.
+// FP32 boxes run the pair-packed operator with every engine vector in the pair layout; FP64 the TMA operator.
 template <typename T>
 bool use_pairs(const Lattice& L)
 {
@@ -342,14 +581,14 @@ void carve(Carve& c, const Lattice& L, int nsys, int rps, bool precond, FWork<T>
     const int nset = (nsys + rps - 1) / rps;
     const int npp = (rps + 1) / 2;
     const bool paired = use_pairs<T>(L);
-    const size_t nv = (size_t)nsys * L.N * 3;
-    const size_t nvp = paired ? (size_t)nset * npp * L.N * 6 : nv;
+    const size_t nv = paired ? (size_t)nset * npp * L.N * 6 : (size_t)nsys * L.N * 3;
     const int nb = (int)((L.N + VB - 1) / VB);
     const int dots = paired ? pair_dot_blocks_max(L.nx, L.ny, L.nz)
                             : tma_dot_blocks_max(L.nx, L.ny, L.nz, (int)sizeof(T));
     w.r = c.take<T>(nv);
-    w.p = c.take<T>(nvp);
-    w.Ap = c.take<T>(nvp);
+    w.p = c.take<T>(nv);
+    w.Ap = c.take<T>(nv);
+    w.xp = paired ? c.take<T>(nv) : nullptr;
     w.Ms = precond ? c.take<T>((size_t)nset * 9 * L.N) : nullptr;
     w.sc.nsys = nsys;
     w.sc.bn = c.take<double>(nsys);
@@ -361,7 +600,7 @@ void carve(Carve& c, const Lattice& L, int nsys, int rps, bool precond, FWork<T>
     w.sc.act = c.take<int>(nsys);
     w.sc.nconv = c.take<unsigned>(1);
     w.vpart = c.take<double>((size_t)3 * nsys * nb);
-    w.vcnt = c.take<unsigned>((size_t)nset * ((rps + GRP - 1) / GRP) + 1);
+    w.vcnt = c.take<unsigned>((size_t)nset * rps + 1);  // one per group or pair
     w.mpart = c.take<double>((size_t)nsys * dots);
     w.mcnt = c.take<unsigned>(nsys);
     w.err = c.take<int>(1);
@@ -403,21 +642,37 @@ struct Operator {
     }
 };
 
-template <typename T, bool PREC, bool PAIRED>
-void launch_vec_init(dim3 vg, cudaStream_t st, const VecGeom& G, const T* b, const T* Ax, const uint8_t* mask,
-                     FWork<T>& w, double tol, int precheck)
+// Vector kernels of one engine step (init, or update + p-update) in the layout of the path.
+template <typename T, bool PREC>
+void launch_init(bool paired, dim3 vg, dim3 pg, cudaStream_t st, const VecGeom& G, const T* b, const T* Ax,
+                 const uint8_t* mask, FWork<T>& w, double tol, int precheck)
 {
-    k_fcg_init<T, PREC, PAIRED><<<vg, VB, 0, st>>>(G, b, Ax, mask, w.Ms, w.r, w.p, w.sc, w.vpart, w.vcnt, tol,
-                                                    precheck);
+    if constexpr (sizeof(T) == 4) {
+        if (paired) {
+            k_pair_init<PREC><<<pg, VB, 0, st>>>(G, b, Ax, mask, w.Ms, w.r, w.p, w.sc, w.vpart, w.vcnt, tol, precheck);
+            return;
+        }
+    }
+    k_fcg_init<T, PREC><<<vg, VB, 0, st>>>(G, b, Ax, mask, w.Ms, w.r, w.p, w.sc, w.vpart, w.vcnt, tol, precheck);
 }
 
-template <typename T, bool PREC, bool PAIRED>
-void launch_vec_iter(dim3 vg, cudaStream_t st, const VecGeom& G, int it, const lpm_cg_opts& o, const uint8_t* mask,
-                     T* x, FWork<T>& w)
+template <typename T, bool PREC>
+void launch_iter(bool paired, dim3 vg, dim3 pg, cudaStream_t st, const VecGeom& G, int it, const lpm_cg_opts& o,
+                 const uint8_t* mask, T* x, FWork<T>& w)
 {
-    k_fcg_update<T, PREC, PAIRED><<<vg, VB, 0, st>>>(G, it, o.check, o.maxit, o.tol, mask, w.Ms, w.r, w.Ap, w.sc,
-                                                      w.vpart, w.vcnt);
-    k_fcg_pupdate<T, PREC, PAIRED><<<vg, VB, 0, st>>>(G, mask, w.Ms, x, w.r, w.p, w.sc);
+    if constexpr (sizeof(T) == 4) {
+        if (paired) {
+            // about two waves of blocks (4 resident per SM) for the reducing kernel
+            const unsigned gx = std::max(1u, std::min(pg.x, (unsigned)((2 * 4 * 148 + pg.y - 1) / pg.y)));
+            k_pair_update<PREC><<<dim3(gx, pg.y), VB, 0, st>>>(G, it, o.check, o.maxit, o.tol, mask, w.Ms, w.r, w.Ap,
+                                                               w.sc, w.vpart, w.vcnt);
+            k_pair_pupdate<PREC><<<pg, VB, 0, st>>>(G, mask, w.Ms, w.xp, w.r, w.p, w.sc);
+            return;
+        }
+    }
+    k_fcg_update<T, PREC><<<vg, VB, 0, st>>>(G, it, o.check, o.maxit, o.tol, mask, w.Ms, w.r, w.Ap, w.sc, w.vpart,
+                                             w.vcnt);
+    k_fcg_pupdate<T, PREC><<<vg, VB, 0, st>>>(G, mask, w.Ms, x, w.r, w.p, w.sc);
 }
 
 }  // namespace
@@ -456,14 +711,14 @@ int cg_solve_fused(const Lattice& L, const T* Kn, const T* Tv, const Batch& bt, 
     const int vgrp = (bt.rhs_per_set + GRP - 1) / GRP;
     const int npp = (bt.rhs_per_set + 1) / 2;
     const bool paired = use_pairs<T>(L);
+    if (paired && nset * npp > 65535) return LPM_ERR_UNSUPPORTED;
     const VecGeom G{N, bt.nsys, bt.rhs_per_set, bt.nmask, vgrp, npp};
     const int nb = (int)((N + VB - 1) / VB);
-    cudaError_t e = cudaMemsetAsync(w.vcnt, 0, sizeof(unsigned) * (nset * vgrp + 1), st);
+    const size_t nvp = (size_t)nset * npp * N * 6;
+    cudaError_t e = cudaMemsetAsync(w.vcnt, 0, sizeof(unsigned) * ((size_t)nset * bt.rhs_per_set + 1), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.mcnt, 0, sizeof(unsigned) * bt.nsys, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.sc.nconv, 0, sizeof(unsigned), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.err, 0, sizeof(int), st);
-    if (e == cudaSuccess && paired)  // dummy lanes of the pair layout stay zero
-        e = cudaMemsetAsync(w.p, 0, sizeof(T) * (size_t)nset * npp * N * 6, st);
     if (e != cudaSuccess) return (int)e;
     if (precond) k_repack_M<T><<<dim3(nb, nset), VB, 0, st>>>(Minv, w.Ms, N);
 
@@ -508,24 +763,22 @@ int cg_solve_fused(const Lattice& L, const T* Kn, const T* Tv, const Batch& bt, 
         a.has_sc = 1;
         a.err = w.err;
     }
-    if (!x_is_zero) {
-        const T* xin = x;
+    // start vector: x (natural layout), or its pair-layout copy xp that the FP32 engine updates
+    if constexpr (sizeof(T) == 4) {
         if (paired) {
-            if constexpr (sizeof(T) == 4) {
-                if ((e = pair_pack(x, w.p, N, bt.nsys, bt.rhs_per_set, st)) != cudaSuccess) return (int)e;
-                xin = w.p;
-            }
+            e = x_is_zero ? cudaMemsetAsync(w.xp, 0, sizeof(T) * nvp, st)
+                          : pair_pack(x, w.xp, N, bt.nsys, bt.rhs_per_set, st);
+            if (e != cudaSuccess) return (int)e;
         }
-        if ((e = op.run(xin, w.Ap, false, 0, st)) != cudaSuccess) return (int)e;
     }
-    const dim3 vg(nb, nset * vgrp);
+    if (!x_is_zero)
+        if ((e = op.run(paired ? w.xp : x, w.Ap, false, 0, st)) != cudaSuccess) return (int)e;
+    const dim3 vg(nb, nset * vgrp), pg(nb, nset * npp);
     const T* Ax = x_is_zero ? nullptr : w.Ap;
     if (precond)
-        paired ? launch_vec_init<T, true, true>(vg, st, G, b, Ax, mask, w, o.tol, o.precheck)
-               : launch_vec_init<T, true, false>(vg, st, G, b, Ax, mask, w, o.tol, o.precheck);
+        launch_init<T, true>(paired, vg, pg, st, G, b, Ax, mask, w, o.tol, o.precheck);
     else
-        paired ? launch_vec_init<T, false, true>(vg, st, G, b, Ax, mask, w, o.tol, o.precheck)
-               : launch_vec_init<T, false, false>(vg, st, G, b, Ax, mask, w, o.tol, o.precheck);
+        launch_init<T, false>(paired, vg, pg, st, G, b, Ax, mask, w, o.tol, o.precheck);
     if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
     unsigned nconv = 0;
     e = cudaMemcpyAsync(&nconv, w.sc.nconv, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
@@ -540,11 +793,9 @@ int cg_solve_fused(const Lattice& L, const T* Kn, const T* Tv, const Batch& bt, 
         timer.end();
         if (e != cudaSuccess) return (int)e;
         if (precond)
-            paired ? launch_vec_iter<T, true, true>(vg, st, G, it, o, mask, x, w)
-                   : launch_vec_iter<T, true, false>(vg, st, G, it, o, mask, x, w);
+            launch_iter<T, true>(paired, vg, pg, st, G, it, o, mask, x, w);
         else
-            paired ? launch_vec_iter<T, false, true>(vg, st, G, it, o, mask, x, w)
-                   : launch_vec_iter<T, false, false>(vg, st, G, it, o, mask, x, w);
+            launch_iter<T, false>(paired, vg, pg, st, G, it, o, mask, x, w);
         if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
         if (it % o.poll == 0 || it == o.maxit) {
             e = cudaMemcpyAsync(&nconv, w.sc.nconv, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
@@ -554,6 +805,9 @@ int cg_solve_fused(const Lattice& L, const T* Kn, const T* Tv, const Batch& bt, 
         }
     }
     timer.collect();
+    if constexpr (sizeof(T) == 4) {
+        if (paired && (e = pair_unpack(w.xp, x, N, bt.nsys, bt.rhs_per_set, st)) != cudaSuccess) return (int)e;
+    }
     int err = 0;
     e = cudaMemcpyAsync(&err, w.err, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
