@@ -127,6 +127,23 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------------------------ CPU side
+def kmv_traffic(nsys):
+    """DRAM bytes per K.u launch for `nsys` systems of the 48^3 workload (6 per specimen), scaled from the ncu capture
+    of a 4-specimen launch (24 systems) summarised in profiles/: read + write bytes grow with the systems and sets."""
+    path = os.path.join(ROOT, "profiles", "k_sc_pair_48cube_batch4.md")
+    if not os.path.exists(path):
+        return None
+    got = {}
+    for line in open(path):
+        for key in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+            if line.startswith("| `%s`" % key):
+                val, unit = line.split("|")[2].split()
+                got[key] = float(val) * {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}[unit]
+    if len(got) != 2:
+        return None
+    return (got["dram__bytes_read.sum"] + got["dram__bytes_write.sum"]) / 24 * nsys
+
+
 def cpu_solve_sample(lat, Kn, Tv, free, ups, nsolve):
     """FP64 block-Jacobi PCG of the CPU oracle (the reference's lin3d._pcg restated in C, all host threads) on the
     first `nsolve` load cases of specimen 0.  Returns (seconds, solves, threads)."""
@@ -253,16 +270,13 @@ def main():
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
     achieved = alg_bytes / (full_ms / 1e3) / 1e9 if prof[3] > 0 else None
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "kmv_traffic.json")
-    if os.path.exists(tfile):
-        try:
-            traffic = _json.load(open(tfile)).get("bytes_per_launch_bench")
-        except ValueError:
-            traffic = None
+    traffic = kmv_traffic(nsys)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
-                "kernel": "FP32 SC K.u (all %d systems, %d coefficient sets) in the inner PCG" % (nsys, B),
+                "kernel": "k_sc_pair: pair-packed FP32 SC K.u with the p.Ap epilogue (all %d systems, %d coefficient "
+                          "sets) in the inner PCG" % (nsys, B),
+                "traffic_source": "ncu dram bytes of a 4-specimen launch (profiles/k_sc_pair_48cube_batch4.md) scaled "
+                                  "by systems",
                 "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": full_ms, "avg_launch_ms_all": all_ms,
                 "launches_timed": int(prof[1]), "peak_source": peak_src}
 
@@ -298,15 +312,21 @@ def main():
     e2e = {"value": world * nsys * a.steps / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h)}
 
-    # ---- comparator: plain FP64 GPU CG (own kernels) on the same batch, and accuracy vs FP64 PCG to 1e-12
+    # ---- comparator: plain FP64 GPU CG on the same batch with this library's fastest FP64 path (packed
+    # coefficients, TMA-fed fused operator, same engine), packing included; accuracy vs FP64 PCG to 1e-12
+    from lpm_b200 import _lib
     b = -core.kmv(dl, ups, Kn, Tv) * free[None, :, :, None]
     torch.cuda.synchronize(dev)
     ev0.record()
-    x64, i64 = core.cg(dl, Kn, Tv, b, free=free, tol=TOL, maxit=20000, check=1, poll=20)
+    K64, T64 = core.pack(Kn[:, 0], torch.float64), core.pack(Tv[:, 0], torch.float64)
+    x64, i64 = core.cg(dl, K64, T64, b, free=free, tol=TOL, maxit=20000, check=1, poll=20, layout=_lib.LAYOUT_SOA,
+                       rhs_per_set=Lc)
     ev1.record()
     torch.cuda.synchronize(dev)
+    del K64, T64
     fp64_cg = {"solves_per_s": nsys / (ev0.elapsed_time(ev1) / 1e3), "iters_mean": float(i64.iters.mean()),
-               "all_converged": bool((i64.status == 0).all())}
+               "all_converged": bool((i64.status == 0).all()),
+               "path": "FP64 plain CG, packed coefficients, TMA-fed fused operator (k_sc_tma<double>)"}
     M64 = core.block_jacobi(dl, Kn[0:1, 0], Tv[0:1, 0], torch.float64)
     xr, ir_ = core.cg(dl, Kn[0:1], Tv[0:1], b[0:1], Minv=M64, free=free, tol=1e-12, maxit=20000, check=1, poll=20)
     uref = ups[0:1] + xr
@@ -326,13 +346,13 @@ def main():
                "sample": "2 load cases (k_xx, k_yy) of specimen 0, FP64 block-Jacobi PCG to 1e-8 by the C oracle "
                          "(restating coarse3d/lin3d.py:464-532), %.1f s" % secs}
 
-    # kernels of this library launched in the timed region: per inner PCG iteration 4 (K.u shell sums + apply,
-    # update, p-update); per step 2 (b = -K u_p) + 2 (FP32 packing) + 1 (block Jacobi); per refinement step 2 (FP64
-    # K.u) + 1 (residual) + 3 (scale, PCG init, correction); plus the final residual check (3).  Iterations per inner
-    # solve are counted as the slowest system's.
+    # kernels of this library launched in the timed region: per inner PCG iteration 3 (pair-packed K.u with the p.Ap
+    # epilogue, update, p-update); per step 2 (b = -K u_p) + 2 (FP32 packing) + 1 (block Jacobi); per refinement
+    # step 2 (FP64 K.u) + 1 (residual) + 1 (scale) + 3 (preconditioner repack, PCG init, unpack) + 1 (correction);
+    # plus the final residual check (3).  Iterations per inner solve are counted as the slowest system's.
     total_inner = int(sum(int(i.iters.max()) for i in infos))
     outer = sum(int(i.outer) for i in infos)
-    gpu_launches = total_inner * 4 + a.steps * (5 + 3) + outer * 6
+    gpu_launches = total_inner * 3 + a.steps * (5 + 3) + outer * 8
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64", "data": "synthetic (seeded spheres microstructures, shapes of the 48^3 config)",
