@@ -1,13 +1,18 @@
 """Benchmark of the LPM linear solve on B200: mixed-precision batched PCG solves per second.
 
-Workload (one "step" = one batched solve of every system from scratch, inputs resident in HBM):
-  48^3 simple-cubic fine LPM, seeded random non-overlapping spheres (r = 4 voxels, volume fraction 0.25, contrast
-  10, E = 1, nu = 0.2; per-bond Kn/Tv = two-end mean of the particle values), 6 KUBC macro-strain load cases
-  (magnitude 1e-3) as 6 right-hand sides per specimen, a batch of B specimens per GPU.  Each step forms b = -K u_p in
-  FP64, packs FP32 coefficients, builds the 3x3 block-Jacobi preconditioner and runs FP32 PCG inside FP64 iterative
-  refinement until every system's FP64 true residual is <= 1e-8 |b|.  Synthetic data (no dataset is involved).
+Workloads (one "step" = one batched solve of every system from scratch, inputs resident in HBM):
+  spheres48 (default): 48^3 simple-cubic fine LPM, seeded random non-overlapping spheres (r = 4 voxels, volume
+    fraction 0.25, contrast 10, E = 1, nu = 0.2; per-bond Kn/Tv = two-end mean of the particle values), 6 KUBC
+    macro-strain load cases (magnitude 1e-3) as 6 right-hand sides per specimen, a batch of B specimens per GPU.
+  ellipsoids192: 192^3, seeded randomly oriented prolate ellipsoids 3:1:1 (volume of a sphere of radius 4, volume
+    fraction 0.30, contrast 15, nu = 0.2), 9 load cases (6 KUBC strains + uniaxial tension along x, y, z) as 9
+    right-hand sides of one specimen.
+Each step forms b = -K u_p in FP64, packs FP32 coefficients, builds the 3x3 block-Jacobi preconditioner and runs FP32
+PCG inside FP64 iterative refinement until every system's FP64 true residual is <= 1e-8 |b|.  Synthetic data (no
+dataset is involved).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--workload spheres48|ellipsoids192]
+                    [--impl ours|reference]
 
 Under torchrun (N > 1) every rank solves its own B specimens (weak scaling, no data-path collective); the step time
 is the max over ranks.  `--impl reference` times the CPU oracle (the reference's FP64 block-Jacobi PCG restated in C,
@@ -29,55 +34,71 @@ sys.path.insert(0, ROOT)
 
 METRIC = "solves/s at rel.res 1e-8 (mixed FP32/FP64-IR batched PCG)"
 UNIT = "solves/s"
-N_SIDE = 48
 LOADS6 = ["k_xx", "k_yy", "k_zz", "k_yz", "k_xz", "k_xy"]
+WORKLOADS = {
+    "spheres48": dict(n=48, loads=LOADS6, micro="spheres", phi=0.25, contrast=10.0, nu=0.2,
+                      label="SC 48^3 spheres r4 phi0.25 contrast10 nu0.2, 6 KUBC RHS per specimen"),
+    "ellipsoids192": dict(n=192, loads=LOADS6 + ["lr_tx", "fb_ty", "tb_tz"], micro="prolate", phi=0.30,
+                          contrast=15.0, nu=0.2,
+                          label="SC 192^3 prolate ellipsoids 3:1:1 r4 phi0.30 contrast15 nu0.2, 6 KUBC + 3 "
+                                "uniaxial tensions as 9 RHS"),
+}
 TOL = 1e-8
 
 
-def workload_config(batch, n_gpus):
-    return {"workload": "SC 48^3 spheres r4 phi0.25 contrast10 nu0.2, 6 KUBC RHS per specimen",
-            "lattice": [N_SIDE] * 3, "specimens_per_gpu": batch, "rhs_per_specimen": 6,
-            "systems_per_gpu": 6 * batch, "tol": TOL, "precision": "fp32 inner PCG + fp64 refinement",
+def workload_config(w, batch, n_gpus):
+    W = WORKLOADS[w]
+    n, L = W["n"], len(W["loads"])
+    return {"workload": W["label"], "lattice": [n] * 3, "specimens_per_gpu": batch, "rhs_per_specimen": L,
+            "systems_per_gpu": L * batch, "tol": TOL, "precision": "fp32 inner PCG + fp64 refinement",
             "preconditioner": "3x3 block Jacobi", "l2": "inputs larger than L2 (%.0f MB of FP64 coefficients per GPU)"
-            % (batch * N_SIDE ** 3 * 36 * 8 / 1e6), "parallelism": "dp%d (independent specimens per GPU)" % n_gpus}
+            % (batch * n ** 3 * 36 * 8 / 1e6), "parallelism": "dp%d (independent specimens per GPU)" % n_gpus}
 
 
-def make_specimen(seed, geom, micro):
-    lat = geom.LatticeGeom(N_SIDE, N_SIDE, N_SIDE, 1.0)
-    ph, _ = micro.spheres(N_SIDE, N_SIDE, N_SIDE, 0.25, 4.0, np.random.default_rng(seed), rjit=0.0)
-    E = np.where(ph == 1, 10.0, 1.0)
-    C = geom.iso_C(E, 0.2)
+def make_specimen(w, seed, geom, micro):
+    W = WORKLOADS[w]
+    n = W["n"]
+    lat = geom.LatticeGeom(n, n, n, 1.0)
+    rng = np.random.default_rng(seed)
+    if W["micro"] == "spheres":
+        ph, _ = micro.spheres(n, n, n, W["phi"], 4.0, rng, rjit=0.0)
+    else:
+        ph, _ = micro.prolate_ellipsoids(n, n, n, W["phi"], 4.0, rng, aspect=3.0, max_tries=60000)
+    E = np.where(ph == 1, W["contrast"], 1.0)
+    C = geom.iso_C(E, W["nu"])
     Kn, Tv = geom.bond_params_two_end_mean(lat, geom.sc_params_from_C(C, 0.5))
     return lat, Kn, Tv
 
 
-def kubc(lat, geom):
+def load_bcs(w, lat, geom):
+    n = WORKLOADS[w]["n"]
     free, ups = [], []
-    for ld in LOADS6:
-        fixed, up, _ = geom.prescribed(ld, lat.x, lat.ijk, (N_SIDE,) * 3, 1)
+    for ld in WORKLOADS[w]["loads"]:
+        fixed, up, _ = geom.prescribed(ld, lat.x, lat.ijk, (n,) * 3, 1)
         free.append(~fixed)
         ups.append(np.where(fixed[:, None], up, 0.0))
     return np.array(free), np.array(ups)
 
 
-def load_workload(seeds):
+def load_workload(w, seeds):
     from lpm_b200 import geom, micro
+    n = WORKLOADS[w]["n"]
     cache = os.path.join(tempfile.gettempdir(), "lpm_bench_cache")
     os.makedirs(cache, exist_ok=True)
     Kn, Tv = [], []
     lat = None
     for s in seeds:
-        fn = os.path.join(cache, "sc48_spheres_%d.npz" % s)
+        fn = os.path.join(cache, "%s_%d.npz" % (w, s))
         if os.path.exists(fn):
             d = np.load(fn)
             k, t = d["Kn"], d["Tv"]
-            lat = lat or geom.LatticeGeom(N_SIDE, N_SIDE, N_SIDE, 1.0)
+            lat = lat or geom.LatticeGeom(n, n, n, 1.0)
         else:
-            lat, k, t = make_specimen(s, geom, micro)
+            lat, k, t = make_specimen(w, s, geom, micro)
             np.savez(fn, Kn=k, Tv=t)
         Kn.append(k)
         Tv.append(t)
-    free, ups = kubc(lat, geom)
+    free, ups = load_bcs(w, lat, geom)
     return lat, np.array(Kn), np.array(Tv), free, ups
 
 
@@ -144,37 +165,40 @@ def kmv_traffic(nsys):
     return (got["dram__bytes_read.sum"] + got["dram__bytes_write.sum"]) / 24 * nsys
 
 
-def cpu_solve_sample(lat, Kn, Tv, free, ups, nsolve):
+def cpu_solve_sample(lat, Kn, Tv, free, ups, nsolve, maxit=20000):
     """FP64 block-Jacobi PCG of the CPU oracle (the reference's lin3d._pcg restated in C, all host threads) on the
-    first `nsolve` load cases of specimen 0.  Returns (seconds, solves, threads)."""
+    first `nsolve` load cases of specimen 0, at most `maxit` iterations each.  Returns (seconds, solves, threads,
+    iterations of the last solve)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     O.set_threads(os.cpu_count() or 1)
     t0 = time.perf_counter()
+    it = 0
     for l in range(nsolve):
         fixed = ~free[l]
-        O.solve_pcg(lat, Kn[0], Tv[0], fixed, ups[l], tol=TOL)
-    return time.perf_counter() - t0, nsolve, O.get_threads()
+        _, info = O.solve_pcg(lat, Kn[0], Tv[0], fixed, ups[l], tol=TOL, maxit=maxit)
+        it = info["iters"]
+    return time.perf_counter() - t0, nsolve, O.get_threads(), it
 
 
 def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    lat, Kn, Tv, free, ups = load_workload([0])
+    lat, Kn, Tv, free, ups = load_workload(a.workload, [0])
     nsolve = 1
     for _ in range(a.warmup):
         cpu_solve_sample(lat, Kn, Tv, free, ups, nsolve)
     secs = []
     for _ in range(a.steps):
-        s, n, thr = cpu_solve_sample(lat, Kn, Tv, free, ups, nsolve)
+        s, n, thr, _ = cpu_solve_sample(lat, Kn, Tv, free, ups, nsolve)
         secs.append(s)
     tot = sum(secs)
     value = a.steps * nsolve / tot
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": 1e3 * tot / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(a.batch, a.gpus),
+            "config": workload_config(a.workload, a.batch, a.gpus),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port",
                              "sample": "%d load case(s) per step of specimen 0, FP64 block-Jacobi PCG to 1e-8 "
                                        "(oracle restating coarse3d/lin3d.py:464-532)" % nsolve},
@@ -188,11 +212,15 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--batch", type=int, default=16, help="specimens per GPU (6 systems each)")
+    ap.add_argument("--batch", type=int, default=None, help="specimens per GPU (default 16 for spheres48, 1 else)")
+    ap.add_argument("--workload", default="spheres48", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 CG comparator")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--inner-tol", type=float, default=1e-5)
     a = ap.parse_args()
+    if a.batch is None:
+        a.batch = 16 if a.workload == "spheres48" else 1
     if a.impl == "reference":
         return run_reference(a)
 
@@ -210,9 +238,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
 
     seeds = [rank * a.batch + j for j in range(a.batch)]
-    lat, Kn_h, Tv_h, free_h, ups_h = load_workload(seeds)
+    lat, Kn_h, Tv_h, free_h, ups_h = load_workload(a.workload, seeds)
     B = a.batch
-    Lc = len(LOADS6)
+    Lc = len(WORKLOADS[a.workload]["loads"])
     dl = core.DeviceLattice(lat, dev)
     Kn = torch.as_tensor(Kn_h, device=dev)[:, None]          # (B, 1, N, 18)
     Tv = torch.as_tensor(Tv_h, device=dev)[:, None]
@@ -270,7 +298,7 @@ def main():
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
     achieved = alg_bytes / (full_ms / 1e3) / 1e9 if prof[3] > 0 else None
-    traffic = kmv_traffic(nsys)
+    traffic = kmv_traffic(nsys) if a.workload == "spheres48" else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                 "kernel": "k_sc_pair: pair-packed FP32 SC K.u with the p.Ap epilogue (all %d systems, %d coefficient "
@@ -316,17 +344,19 @@ def main():
     # coefficients, TMA-fed fused operator, same engine), packing included; accuracy vs FP64 PCG to 1e-12
     from lpm_b200 import _lib
     b = -core.kmv(dl, ups, Kn, Tv) * free[None, :, :, None]
-    torch.cuda.synchronize(dev)
-    ev0.record()
-    K64, T64 = core.pack(Kn[:, 0], torch.float64), core.pack(Tv[:, 0], torch.float64)
-    x64, i64 = core.cg(dl, K64, T64, b, free=free, tol=TOL, maxit=20000, check=1, poll=20, layout=_lib.LAYOUT_SOA,
-                       rhs_per_set=Lc)
-    ev1.record()
-    torch.cuda.synchronize(dev)
-    del K64, T64
-    fp64_cg = {"solves_per_s": nsys / (ev0.elapsed_time(ev1) / 1e3), "iters_mean": float(i64.iters.mean()),
-               "all_converged": bool((i64.status == 0).all()),
-               "path": "FP64 plain CG, packed coefficients, TMA-fed fused operator (k_sc_tma<double>)"}
+    fp64_cg = None
+    if not a.no_fp64:
+        torch.cuda.synchronize(dev)
+        ev0.record()
+        K64, T64 = core.pack(Kn[:, 0], torch.float64), core.pack(Tv[:, 0], torch.float64)
+        x64, i64 = core.cg(dl, K64, T64, b, free=free, tol=TOL, maxit=50000, check=1, poll=20,
+                           layout=_lib.LAYOUT_SOA, rhs_per_set=Lc)
+        ev1.record()
+        torch.cuda.synchronize(dev)
+        del K64, T64, x64
+        fp64_cg = {"solves_per_s": nsys / (ev0.elapsed_time(ev1) / 1e3), "iters_mean": float(i64.iters.mean()),
+                   "all_converged": bool((i64.status == 0).all()),
+                   "path": "FP64 plain CG, packed coefficients, TMA-fed fused operator (k_sc_tma<double>)"}
     M64 = core.block_jacobi(dl, Kn[0:1, 0], Tv[0:1, 0], torch.float64)
     xr, ir_ = core.cg(dl, Kn[0:1], Tv[0:1], b[0:1], Minv=M64, free=free, tol=1e-12, maxit=20000, check=1, poll=20)
     uref = ups[0:1] + xr
@@ -341,10 +371,23 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
-        secs, n, thr = cpu_solve_sample(lat, Kn_h, Tv_h, free_h, ups_h, 2)
-        cpu = {"value": n / secs, "unit": UNIT, "cores": thr, "kind": "port",
-               "sample": "2 load cases (k_xx, k_yy) of specimen 0, FP64 block-Jacobi PCG to 1e-8 by the C oracle "
-                         "(restating coarse3d/lin3d.py:464-532), %.1f s" % secs}
+        if a.workload == "spheres48":
+            secs, n, thr, _ = cpu_solve_sample(lat, Kn_h, Tv_h, free_h, ups_h, 2)
+            cpu = {"value": n / secs, "unit": UNIT, "cores": thr, "kind": "port",
+                   "sample": "2 load cases (k_xx, k_yy) of specimen 0, FP64 block-Jacobi PCG to 1e-8 by the C oracle "
+                             "(restating coarse3d/lin3d.py:464-532), %.1f s" % secs}
+        else:
+            # a full CPU solve of this size takes tens of minutes: time 30 PCG iterations of load 0 and scale by the
+            # iteration count the same FP64 PCG needs on the GPU
+            M0 = core.block_jacobi(dl, Kn[0:1, 0], Tv[0:1, 0], torch.float64)
+            _, i0 = core.cg(dl, Kn[0:1, 0], Tv[0:1, 0], b[0:1, 0], Minv=M0, free=free[0:1], tol=TOL, maxit=20000,
+                            check=1, poll=50)
+            need = int(i0.iters[0])
+            secs, n, thr, done = cpu_solve_sample(lat, Kn_h, Tv_h, free_h, ups_h, 1, maxit=30)
+            cpu = {"value": 1.0 / (secs / max(done, 1) * need), "unit": UNIT, "cores": thr, "kind": "port",
+                   "sample": "30 FP64 block-Jacobi PCG iterations of load k_xx by the C oracle (restating "
+                             "coarse3d/lin3d.py:464-532), %.1f s, scaled to the %d iterations the same PCG needs "
+                             "to 1e-8" % (secs, need)}
 
     # kernels of this library launched in the timed region: per inner PCG iteration 3 (pair-packed K.u with the p.Ap
     # epilogue, update, p-update); per step 2 (b = -K u_p) + 2 (FP32 packing) + 1 (block Jacobi); per refinement
@@ -355,11 +398,13 @@ def main():
     gpu_launches = total_inner * 3 + a.steps * (5 + 3) + outer * 8
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32+f64", "data": "synthetic (seeded spheres microstructures, shapes of the 48^3 config)",
-            "config": workload_config(B, world), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "dtype": "f32+f64", "data": "synthetic (seeded %s microstructures, shapes of the %d^3 config)"
+            % ("spheres" if a.workload == "spheres48" else "prolate-ellipsoid", WORKLOADS[a.workload]["n"]),
+            "config": workload_config(a.workload, B, world), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "clocks": clocks, "gpu_launches": gpu_launches, "all_converged": bool(ok),
             "inner_iters_mean": float(iters.mean()), "outer_steps": [i.outer for i in infos][:1],
-            "fp64_gpu_cg": fp64_cg, "speedup_vs_fp64_gpu_cg": value / world / fp64_cg["solves_per_s"],
+            "fp64_gpu_cg": fp64_cg,
+            "speedup_vs_fp64_gpu_cg": value / world / fp64_cg["solves_per_s"] if fp64_cg else None,
             "accuracy": accuracy}
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -108,14 +108,15 @@ def ellipsoids(nx, ny, nz, phi, rmean, rng, aspect=(1.0, 2.0), rjit=0.4):
     return img.astype(np.int64).ravel(), dict(kind="ellipsoids", rmean=rmean, ninc=n, aspect=aspect)
 
 
-def prolate_ellipsoids(nx, ny, nz, phi, r, rng, aspect=3.0):
-    """Randomly oriented prolate ellipsoids a:b:b = aspect:1:1 with the volume of a sphere of radius r."""
+def prolate_ellipsoids(nx, ny, nz, phi, r, rng, aspect=3.0, max_tries=20000):
+    """Randomly oriented prolate ellipsoids a:b:b = aspect:1:1 with the volume of a sphere of radius r (large boxes
+    need more than the default 20000 attempts to reach phi)."""
     axes = r * np.array([aspect ** (2 / 3), aspect ** (-1 / 3), aspect ** (-1 / 3)])
 
     def shape(r_):
         return axes, random_rotation(r_)
 
-    img, n = rsa(nx, ny, nz, phi, rng, shape)
+    img, n = rsa(nx, ny, nz, phi, rng, shape, max_tries=max_tries)
     return img.astype(np.int64).ravel(), dict(kind="prolate", r=r, ninc=n, aspect=aspect)
 
 
