@@ -205,6 +205,15 @@ int lpm_kmv_vjp_f64(const lpm_lattice* lat, const double* u, const double* G, co
                     int32_t coef_layout, const lpm_batch* batch, double* du, double* gKn, double* gTv,
                     int32_t accumulate, void* scratch, size_t scratch_bytes, void* stream);
 
+/* ------------------------------------------------------------------------------------------------- tuning */
+/* Autotuner of the FP32 packed-coefficient SC operator used by the CG engines on full boxes: times the z-chunk
+ * candidates (whole box, 1/2, 1/3, ... of the planes, at least 8 planes per chunk) on zero vectors of the batch's
+ * shape, records the fastest for (nx, ny, nz, pairs) in a process-wide table that later launches of that shape use,
+ * and returns it.  Kn/Tv: packed FP32 coefficients (LPM_LAYOUT_SOA) of the batch's sets.  scratch:
+ * lpm_kmv_scratch_bytes(lat, LPM_F32, nsys).  No reference counterpart (tuning of this library's tiles). */
+int lpm_autotune_kmv(const lpm_lattice* lat, const lpm_batch* batch, const float* Kn, const float* Tv, void* scratch,
+                     size_t scratch_bytes, int32_t* zchunk_out, void* stream);
+
 /* ------------------------------------------------------------------------------------------------ geometry */
 /* Neighbour table of a (possibly masked) box, identical to LatticeGeom.nbr / Lattice2D.nbr
  * (coarse3d/geom3d.py:38-65, coarse2d/lin2d.py:32-74): site_of (nx*ny*nz) int64 = particle id or -1,

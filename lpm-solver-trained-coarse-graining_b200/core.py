@@ -129,6 +129,18 @@ def _scratch(nbytes, device):
     return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device=device)
 
 
+def autotune(dl, K32, T32, nsys, rhs_per_set):
+    """Time the z-chunk candidates of the pair-packed FP32 operator for this batch shape (packed FP32 coefficients
+    K32/T32 (nset, NN, N)); the fastest is recorded in the library for later launches and returned."""
+    lib = L.load()
+    scr = _scratch(lib.lpm_kmv_scratch_bytes(dl.ref, L.LPM_F32, int(nsys)), K32.device)
+    z = ctypes.c_int32(0)
+    b = _batch(nsys, rhs_per_set)
+    L.check(lib.lpm_autotune_kmv(dl.ref, ctypes.byref(b), L.ptr(K32), L.ptr(T32), L.ptr(scr), scr.numel(),
+                                 ctypes.byref(z), L.stream_ptr(K32.device)), "lpm_autotune_kmv")
+    return int(z.value)
+
+
 def pack(K, dtype=_F32):
     """(nset, N, NN) FP64 -> (nset, NN, N) in `dtype` (the packed SoA layout of the solver)."""
     L.require_cuda(K)

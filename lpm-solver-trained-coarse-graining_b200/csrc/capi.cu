@@ -398,6 +398,65 @@ int lpm_kmv_vjp_f64(const lpm_lattice* lat, const double* u, const double* G, co
                     scratch_bytes, stream);
 }
 
+int lpm_autotune_kmv(const lpm_lattice* lat, const lpm_batch* batch, const float* Kn, const float* Tv, void* scratch,
+                     size_t scratch_bytes, int32_t* zchunk_out, void* stream)
+{
+    Lattice L;
+    Batch bt;
+    int rc = to_lattice(lat, L);
+    if (rc || (rc = to_batch(batch, bt))) return rc;
+    if (!Kn || !Tv || !zchunk_out) return LPM_ERR_ARG;
+    if (L.dim != 3 || L.nbr || !pair_supported(L.nx) || !tma_aligned(Kn, Tv, Kn)) return LPM_ERR_UNSUPPORTED;
+    const int npp = (bt.rhs_per_set + 1) / 2, nset = (bt.nsys + bt.rhs_per_set - 1) / bt.rhs_per_set;
+    const size_t nvp = (size_t)nset * npp * L.N * 6;
+    float* up = aligned<float>(scratch, scratch_bytes, 2 * nvp * sizeof(float), rc);
+    if (rc) return rc;
+    cudaStream_t st = S(stream);
+    cudaError_t e = cudaMemsetAsync(up, 0, nvp * sizeof(float), st);
+    PairArgs a{};
+    a.nx = L.nx;
+    a.ny = L.ny;
+    a.nz = L.nz;
+    a.N = L.N;
+    a.nsys = bt.nsys;
+    a.rhs_per_set = bt.rhs_per_set;
+    a.npp = npp;
+    a.npair = nset * npp;
+    a.u = up;
+    a.Kn = Kn;
+    a.Tv = Tv;
+    a.out = up + nvp;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    int best = pair_zchunk_heuristic(L.nx, L.ny, L.nz, a.npair);
+    float best_ms = 0.f;
+    bool have = false;
+    for (int nzc = 1; e == cudaSuccess && nzc <= pair_zchunk_max_chunks(L.nz); ++nzc) {
+        const int zc = (L.nz + nzc - 1) / nzc;
+        if (nzc > 1 && (L.nz + zc - 1) / zc != nzc) continue;  // same chunking as a smaller count
+        a.zchunk = zc;
+        e = launch_sc_pair(a, false, st);  // warm-up
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventRecord(e0, st);
+        for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = launch_sc_pair(a, false, st);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e == cudaSuccess && (!have || ms < best_ms)) {
+            best_ms = ms;
+            best = zc;
+            have = true;
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (e != cudaSuccess) return ret(e);
+    pair_zchunk_record(L.nx, L.ny, L.nz, a.npair, best);
+    *zchunk_out = best;
+    return LPM_OK;
+}
+
 int lpm_build_nbr(int32_t dim, int32_t nx, int32_t ny, int32_t nz, int64_t n, const int64_t* site_of,
                   const int64_t* sites, int64_t* nbr, void* stream)
 {

@@ -10,6 +10,9 @@
 // (npair, N, 3, 2); its output is unmasked, so the update masks Ap (p stays zero on fixed DOFs, so p.Ap needs no
 // mask).  Reductions are deterministic (per-block partials summed in fixed order by a last block).
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "lpm_tma.h"
 
@@ -211,11 +214,12 @@ __device__ __forceinline__ void update_tail(const VecGeom& G, const Group& gr, i
 
 // ----------------------------------------------------------------------------------------------------- update
 template <typename T, bool PREC>
-__global__ void __launch_bounds__(VB) k_fcg_update(VecGeom G, int it, int check, int maxit, double tol,
+__global__ void __launch_bounds__(VB) k_fcg_update(VecGeom G, int it_host, int check, int maxit, double tol,
                                                    const uint8_t* __restrict__ mask, const T* __restrict__ Ms,
                                                    T* __restrict__ r, const T* __restrict__ Ap, FcgScalars sc,
                                                    double* part, unsigned* cnt)
 {
+    const int it = sc.itp ? *sc.itp : it_host;
     __shared__ double sh[GRP * 2 * 8];
     __shared__ bool last;
     const Group gr = group_of(G);
@@ -269,6 +273,7 @@ __global__ void __launch_bounds__(VB) k_fcg_pupdate(VecGeom G, const uint8_t* __
                                                     const T* __restrict__ Ms, T* __restrict__ x,
                                                     const T* __restrict__ r, T* __restrict__ p, FcgScalars sc)
 {
+    if (sc.itp && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) atomicAdd(sc.itp, 1);
     const Group gr = group_of(G);
     const int64_t N = G.N;
     const int64_t i = (int64_t)blockIdx.x * VB + threadIdx.x;
@@ -443,11 +448,12 @@ __global__ void __launch_bounds__(VB) k_pair_init(VecGeom G, const float* __rest
 
 // r -= alpha mask(Ap); z = mask(M r); r.z, r.r; the last block of the pair forms beta and tests convergence.
 template <bool PREC>
-__global__ void __launch_bounds__(VB) k_pair_update(VecGeom G, int it, int check, int maxit, double tol,
+__global__ void __launch_bounds__(VB) k_pair_update(VecGeom G, int it_host, int check, int maxit, double tol,
                                                     const uint8_t* __restrict__ mask, const float* __restrict__ Ms,
                                                     float* __restrict__ r, const float* __restrict__ Ap,
                                                     FcgScalars sc, double* part, unsigned* cnt)
 {
+    const int it = sc.itp ? *sc.itp : it_host;
     __shared__ double sh[2 * 2 * 8];
     __shared__ bool last;
     const PairSys q = pair_of(G);
@@ -501,6 +507,7 @@ __global__ void __launch_bounds__(VB) k_pair_pupdate(VecGeom G, const uint8_t* _
                                                      const float* __restrict__ r, float* __restrict__ p,
                                                      FcgScalars sc)
 {
+    if (sc.itp && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) atomicAdd(sc.itp, 1);
     const PairSys q = pair_of(G);
     const int64_t N = G.N;
     const int64_t i = (int64_t)blockIdx.x * VB + threadIdx.x;
@@ -604,6 +611,63 @@ void carve(Carve& c, const Lattice& L, int nsys, int rps, bool precond, FWork<T>
     w.mpart = c.take<double>((size_t)nsys * dots);
     w.mcnt = c.take<unsigned>(nsys);
     w.err = c.take<int>(1);
+    w.sc.itp = c.take<int>(1);
+}
+
+// ----------------------------------------------------------------------------------------- graph replay
+// A block of `poll` iterations (operator + update + p-update each) depends only on the buffers, sizes and options
+// below, and reads the iteration number from device memory; it is captured once as a CUDA graph and replayed for
+// every later block with the same key (e.g. every inner solve of a refinement loop, every round of a serving bucket).
+struct GraphKey {
+    const void *ws, *Kn, *Tv, *mask, *x;
+    int nsys, rps, nmask, nx, ny, nz, poll, check, maxit, precond, elem;
+    double tol;
+    bool operator<(const GraphKey& o) const
+    {
+        return std::tie(ws, Kn, Tv, mask, x, nsys, rps, nmask, nx, ny, nz, poll, check, maxit, precond, elem, tol) <
+               std::tie(o.ws, o.Kn, o.Tv, o.mask, o.x, o.nsys, o.rps, o.nmask, o.nx, o.ny, o.nz, o.poll, o.check,
+                        o.maxit, o.precond, o.elem, o.tol);
+    }
+};
+
+class GraphCache {
+public:
+    cudaGraphExec_t find(const GraphKey& k)
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        auto it = map_.find(k);
+        return it == map_.end() ? nullptr : it->second;
+    }
+    void put(const GraphKey& k, cudaGraphExec_t e)
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        if (map_.size() >= 64) {  // bounded: drop everything (entries are cheap to re-capture)
+            for (auto& kv : map_) cudaGraphExecDestroy(kv.second);
+            map_.clear();
+        }
+        map_[k] = e;
+    }
+
+private:
+    std::mutex mu_;
+    std::map<GraphKey, cudaGraphExec_t> map_;
+};
+
+// One non-blocking stream per host thread and device for graph capture (never used to run work).
+cudaStream_t capture_stream()
+{
+    thread_local cudaStream_t streams[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    if (!streams[dev] && cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking) != cudaSuccess)
+        streams[dev] = nullptr;
+    return streams[dev];
+}
+
+GraphCache& graph_cache()
+{
+    static GraphCache* c = new GraphCache();  // never destroyed: graphs may outlive static destruction order
+    return *c;
 }
 
 // One operator launch: out = K u, with the alpha-step epilogue when epi.
@@ -787,22 +851,58 @@ int cg_solve_fused(const Lattice& L, const T* Kn, const T* Tv, const Batch& bt, 
 
     KmvTimer timer(o.prof, st);
     int rc = LPM_OK;
-    for (int it = 1; it <= o.maxit && nconv < (unsigned)bt.nsys; ++it) {
+    static const int kOne = 1;
+    if ((e = cudaMemcpyAsync(w.sc.itp, &kOne, sizeof(int), cudaMemcpyHostToDevice, st)) != cudaSuccess) return (int)e;
+    auto one_iter = [&](int it, cudaStream_t s) -> cudaError_t {
         timer.begin(nconv == 0);
-        e = op.run(w.p, w.Ap, true, it, st);
+        cudaError_t ee = op.run(w.p, w.Ap, true, it, s);
         timer.end();
-        if (e != cudaSuccess) return (int)e;
+        if (ee != cudaSuccess) return ee;
         if (precond)
-            launch_iter<T, true>(paired, vg, pg, st, G, it, o, mask, x, w);
+            launch_iter<T, true>(paired, vg, pg, s, G, it, o, mask, x, w);
         else
-            launch_iter<T, false>(paired, vg, pg, st, G, it, o, mask, x, w);
-        if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
-        if (it % o.poll == 0 || it == o.maxit) {
-            e = cudaMemcpyAsync(&nconv, w.sc.nconv, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-            if (e != cudaSuccess) return (int)e;
-            timer.collect();
+            launch_iter<T, false>(paired, vg, pg, s, G, it, o, mask, x, w);
+        return cudaGetLastError();
+    };
+    const GraphKey key{ws, Kn, Tv, mask, x, bt.nsys, bt.rhs_per_set, bt.nmask, L.nx, L.ny, L.nz, o.poll, o.check,
+                       o.maxit, precond ? 1 : 0, (int)sizeof(T), o.tol};
+    int it = 1;
+    while (it <= o.maxit && nconv < (unsigned)bt.nsys) {
+        const int block = std::min(o.poll - (it - 1) % o.poll, o.maxit - it + 1);
+        // full blocks after the first one replay a captured graph (not while per-launch timings are requested)
+        cudaGraphExec_t ge = nullptr;
+        if (!o.prof && it > 1 && block == o.poll) {
+            ge = graph_cache().find(key);
+            if (!ge) {
+                // captured on a private stream (the caller's may be the legacy default stream, which cannot be
+                // captured); the graph is then launched on the caller's stream
+                cudaStream_t cs = capture_stream();
+                if (!cs) return (int)cudaErrorNotReady;
+                cudaGraph_t g = nullptr;
+                if ((e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return (int)e;
+                cudaError_t ce = cudaSuccess;
+                for (int b = 0; b < block && ce == cudaSuccess; ++b) ce = one_iter(it + b, cs);
+                e = cudaStreamEndCapture(cs, &g);
+                if (ce != cudaSuccess) {
+                    if (g) cudaGraphDestroy(g);
+                    return (int)ce;
+                }
+                if (e != cudaSuccess) return (int)e;
+                e = cudaGraphInstantiate(&ge, g, 0);
+                cudaGraphDestroy(g);
+                if (e != cudaSuccess) return (int)e;
+                graph_cache().put(key, ge);
+            }
+            if ((e = cudaGraphLaunch(ge, st)) != cudaSuccess) return (int)e;
+        } else {
+            for (int b = 0; b < block; ++b)
+                if ((e = one_iter(it + b, st)) != cudaSuccess) return (int)e;
         }
+        it += block;
+        e = cudaMemcpyAsync(&nconv, w.sc.nconv, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return (int)e;
+        timer.collect();
     }
     timer.collect();
     if constexpr (sizeof(T) == 4) {

@@ -33,6 +33,9 @@
 // a system runs the CG alpha step.
 #include <cudaTypedefs.h>
 
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <type_traits>
 
 #include "lpm_fused.h"
@@ -615,13 +618,38 @@ cudaError_t pair_unpack(const float* xp, float* x, int64_t N, int nsys, int rps,
 
 bool pair_supported(int nx) { return nx % 4 == 0 && tma_supported(nx, 4); }
 
-int pair_zchunk(int nx, int ny, int nz, int npair)
+// z planes per CTA: an autotuned value for this shape if one was recorded (lpm_autotune_kmv), else enough z chunks
+// for two CTAs per SM of work with at least 8 planes each.
+namespace {
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, int> g_tuned;
+}  // namespace
+
+int pair_zchunk_heuristic(int nx, int ny, int nz, int npair)
 {
     const long long base = (long long)((nx + PX - 1) / PX) * ((ny + PY - 1) / PY) * npair;
     int nzc = 1;
     while (base * nzc < 2 * 148 && nz / (nzc + 1) >= 8) ++nzc;
     return (nz + nzc - 1) / nzc;
 }
+
+int pair_zchunk(int nx, int ny, int nz, int npair)
+{
+    {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        auto it = g_tuned.find(std::make_tuple(nx, ny, nz, npair));
+        if (it != g_tuned.end()) return it->second;
+    }
+    return pair_zchunk_heuristic(nx, ny, nz, npair);
+}
+
+void pair_zchunk_record(int nx, int ny, int nz, int npair, int zchunk)
+{
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tuned[std::make_tuple(nx, ny, nz, npair)] = zchunk;
+}
+
+int pair_zchunk_max_chunks(int nz) { return nz / 8 > 1 ? nz / 8 : 1; }
 
 int pair_dot_blocks_max(int nx, int ny, int nz) { return ((nx + PX - 1) / PX) * ((ny + PY - 1) / PY) * (nz / 8 + 1); }
 

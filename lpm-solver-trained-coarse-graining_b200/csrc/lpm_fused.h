@@ -18,11 +18,14 @@ struct FcgScalars {
     int* iters;
     double* relres;
     int* status;
+    int* itp;  // device copy of the current iteration number (1-based), advanced by the p-update kernel; lets a
+               // captured block of iterations replay without host-side parameters
 };
 
 // alpha step of system s, run by the last block of the operator epilogue once p.Ap is complete.
 __device__ __forceinline__ void cg_alpha_step(const FcgScalars& sc, int s, double pAp, int it)
 {
+    if (sc.itp) it = *sc.itp;
     sc.pAp[s] = pAp;
     if (!sc.act[s]) {
         sc.alpha[s] = 0.0;

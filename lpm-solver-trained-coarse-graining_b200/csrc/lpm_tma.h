@@ -67,7 +67,10 @@ struct PairArgs {
 };
 
 bool pair_supported(int nx);
-int pair_zchunk(int nx, int ny, int nz, int npair);
+int pair_zchunk(int nx, int ny, int nz, int npair);            // autotuned value if recorded, else heuristic
+int pair_zchunk_heuristic(int nx, int ny, int nz, int npair);
+void pair_zchunk_record(int nx, int ny, int nz, int npair, int zchunk);
+int pair_zchunk_max_chunks(int nz);                               // z chunks allowed (>= 8 planes each)
 int pair_dot_blocks_max(int nx, int ny, int nz);
 cudaError_t launch_sc_pair(const PairArgs& a, bool epi, cudaStream_t st);
 // (nsys, N, 3) FP32 -> pair layout (dummy lanes written as zero) and back (real systems only); npair <= 65535.
