@@ -206,6 +206,335 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------------------------- serving stream
+SERVE_2D = [64, 128, 256, 512]
+SERVE_3D = [24, 48, 72, 96]
+
+
+def serve_requests(n_req, seed):
+    """The serving mix: 60% 2D square boxes (n in {64..512}^2, Gaussian random field), 40% 3D SC boxes (n in
+    {24..96}^3, random field or spheres), inclusion fraction U(0.15, 0.40), contrast U(5, 15), 1-6 (2D) or 1-9 (3D)
+    load cases drawn from the load sets.  Returns a list of (dim, shape, Kn, Tv, free (L,N,d), up (L,N,d))."""
+    from lpm_b200 import geom, micro
+    rng = np.random.default_rng(seed)
+    cache = os.path.join(tempfile.gettempdir(), "lpm_bench_cache")
+    os.makedirs(cache, exist_ok=True)
+    out = []
+    for _ in range(n_req):
+        is2d = rng.random() < 0.6
+        phi, contrast = rng.uniform(0.15, 0.40), rng.uniform(5.0, 15.0)
+        mseed = int(rng.integers(1 << 30))
+        if is2d:
+            n = int(rng.choice(SERVE_2D))
+            lat = geom.SquareLattice(n, n, 1.0)
+            ph = micro.grf_two_phase(n, n, 6.0, phi, mseed)
+            C = geom.iso_C2d(np.where(ph == 1, contrast, 1.0), 0.25, plane="stress")
+            Kn, Tv = geom.bond_params_two_end_mean(lat, geom.square_params_from_C(C))
+            loads = list(rng.choice(geom.LOADS2D, size=int(rng.integers(1, 7)), replace=False))
+            free, up = [], []
+            for ld in loads:
+                fixed, u, _ = geom.prescribed2d(ld, lat.x, lat.ij, n, n, 1, 1.0)
+                free.append(np.repeat(~fixed[:, None], 2, 1))
+                up.append(np.where(fixed[:, None], u, 0.0))
+            out.append((2, (n, n), Kn, Tv, np.array(free), np.array(up)))
+        else:
+            n = int(rng.choice(SERVE_3D))
+            lat = geom.LatticeGeom(n, n, n, 1.0)
+            if rng.random() < 0.5:
+                ph, _ = micro.grf3(n, n, n, 4.0, phi, np.random.default_rng(mseed))
+            else:
+                ph, _ = micro.spheres(n, n, n, phi, 4.0, np.random.default_rng(mseed), rjit=0.0)
+            C = geom.iso_C(np.where(ph == 1, contrast, 1.0), 0.2)
+            Kn, Tv = geom.bond_params_two_end_mean(lat, geom.sc_params_from_C(C, 0.5))
+            loads = list(rng.choice(geom.LOADS, size=int(rng.integers(1, 10)), replace=False))
+            free, up = [], []
+            for ld in loads:
+                fixed, u, _ = geom.prescribed(ld, lat.x, lat.ijk, (n,) * 3, 1)
+                free.append(np.repeat(~fixed[:, None], 3, 1))
+                up.append(np.where(fixed[:, None], u, 0.0))
+            out.append((3, (n,) * 3, Kn, Tv, np.array(free), np.array(up)))
+    return out
+
+
+def run_serve(a):
+    """Serving stream: continuous batching vs sequential plain FP64 CG, on one GPU (rank 0 only)."""
+    import threading
+    import torch
+    from lpm_b200 import _lib, core, geom, serve
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    n_req = a.requests
+    specs = serve_requests(n_req, 1234)
+    nsolve = sum(sp[4].shape[0] for sp in specs)
+    srv = serve.Server(device=dev, rmax=9, rmax2d=6, max_slots=8, tol=TOL, inner_tol=a.inner_tol,
+                       idle_release_s=1e9)
+
+    def stream(arrivals):
+        reqs = [serve.Request(*sp) for sp in specs]
+        t0 = time.perf_counter()
+        done = [None]
+
+        def feed():
+            for r, t in zip(reqs, arrivals):
+                dt = t0 + t - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                r.arrival = time.perf_counter()
+                srv.submit(r)
+
+        th = threading.Thread(target=feed)
+        th.start()
+        srv.done.clear()
+        srv.wait_all(n_req, timeout=3600)
+        th.join()
+        t1 = max(r.done for r in reqs)
+        return reqs, t1 - t0
+
+    try:
+        for _ in range(max(a.warmup, 1)):            # warm-up: creates and autotunes the buckets
+            stream([0.0] * n_req)
+        reqs_cap, t_cap = stream([0.0] * n_req)      # capacity: everything at t = 0 (saturated)
+        cap = n_req / t_cap
+        lat_cap = serve.latency_stats(reqs_cap)
+        rate = a.load_factor * cap
+        gaps = np.random.default_rng(7).exponential(1.0 / rate, n_req)
+        arrivals = np.cumsum(gaps) - gaps[0]
+        sampler = ClockSampler(dev.index or 0)
+        sampler.start()
+        for b in srv.buckets.values():
+            b.rounds, b.busy_s, b.admit_s, b.inner_iters = 0, 0.0, 0.0, 0
+        reqs, t_run = stream(list(arrivals))
+        clocks = sampler.stop()
+        bstats = serve.bucket_stats(srv)
+        ok = all(r.status == 0 and (r.relres <= TOL).all() for r in reqs)
+        lat_ms = serve.latency_stats(reqs)
+    finally:
+        srv.close()
+
+    # sequential plain FP64 CG on the same GPU, same requests and arrival times (FIFO, one request at a time)
+    seq_t, seq_by = [], {}
+    for sp in specs:
+        dim, shape, Kn, Tv, free, up = sp
+        lat = geom.LatticeGeom(*shape, 1.0) if dim == 3 else geom.SquareLattice(*shape, 1.0)
+        dl = core.DeviceLattice(lat, dev)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        Kt, Tt = torch.as_tensor(Kn, device=dev), torch.as_tensor(Tv, device=dev)
+        fr = torch.as_tensor(free.astype(np.float64), device=dev)
+        ut = torch.as_tensor(up, device=dev) * (1 - fr)
+        b = -core.kmv(dl, ut, Kt, Tt) * fr
+        if dim == 3:
+            K64, T64 = core.pack(Kt[None], torch.float64), core.pack(Tt[None], torch.float64)
+            x, info = core.cg(dl, K64, T64, b, free=fr, tol=TOL, maxit=100000, check=1, poll=20,
+                              layout=_lib.LAYOUT_SOA, rhs_per_set=b.shape[0])
+        else:
+            x, info = core.cg(dl, Kt, Tt, b, free=fr, tol=TOL, maxit=100000, check=1, poll=20)
+        (ut + x).cpu()
+        seq_t.append(time.perf_counter() - t0)
+        seq_by.setdefault("%dD %d" % (dim, shape[0]), []).append(round(seq_t[-1], 3))
+    end, seq_lat = 0.0, []
+    for t_arr, t_solve in zip(arrivals, seq_t):
+        start = max(t_arr, end)
+        end = start + t_solve
+        seq_lat.append(end - t_arr)
+    seq_lat = np.array(seq_lat)
+    line = {"metric": "serving capacity solves/s at rel.res 1e-8 (continuous batching), p50/p99 latency at 0.7 load",
+            "value": nsolve / t_cap, "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": max(a.warmup, 1),
+            "ms_per_step": t_cap * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic (seeded random-field / sphere microstructures)",
+            "config": {"workload": "serving mix: 60% 2D square n in {64,128,256,512}^2, 40% 3D SC n in {24,48,72,96}^3, "
+                                   "phi U(0.15,0.40), contrast U(5,15), 1-6 / 1-9 load cases",
+                       "requests": n_req, "systems": nsolve, "arrival": "Poisson, rate %.3f req/s = %.2f x measured "
+                       "capacity %.3f req/s" % (rate, a.load_factor, cap), "tol": TOL,
+                       "buckets": "per lattice size, up to 8 specimens x 9 systems, HBM budget 60% of free memory"},
+            "latency_ms": lat_ms, "poisson_run": {"solves_per_s": nsolve / t_run, "seconds": t_run,
+                                                    "requests_per_s": n_req / t_run},
+            "capacity_run": {"requests_per_s": cap, "seconds": t_cap, "latency_ms": lat_cap},
+            "all_converged": bool(ok), "buckets": bstats,
+            "clocks": clocks,
+            "sequential_fp64_cg": {"solves_per_s": nsolve / (sum(seq_t)), "p50_ms": float(np.percentile(seq_lat, 50)
+                                   * 1e3), "p99_ms": float(np.percentile(seq_lat, 99) * 1e3),
+                                   "path": "plain FP64 CG per request (fused FP64 operator in 3D), FIFO",
+                                   "seconds_by_size": seq_by}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------ 2D configurations
+def plain2d_specimens(seeds, n=128):
+    """2D 128^2 square lattice, Gaussian random field (corr 6, phi 0.30), E 1 / 10, nu 0.25 plane stress, two-end
+    mean bonds, uniaxial tension u_x = 1e-3 (n-1) on the right column (left column u_x = 0, corner pinned)."""
+    from lpm_b200 import geom, micro
+    lat = geom.SquareLattice(n, n, 1.0)
+    Kn, Tv = [], []
+    for sd in seeds:
+        ph = micro.grf_two_phase(n, n, 6.0, 0.30, sd)
+        C = geom.iso_C2d(np.where(ph == 1, 10.0, 1.0), 0.25, plane="stress")
+        k, t = geom.bond_params_two_end_mean(lat, geom.square_params_from_C(C))
+        Kn.append(k)
+        Tv.append(t)
+    fixed, up, _ = geom.uniaxial_tension_2d(lat, 1e-3)
+    return lat, np.array(Kn), np.array(Tv), fixed, up
+
+
+def run_plain2d(a):
+    """cfg 1: FP64 unpreconditioned CG to rel. residual 1e-10 on ten 128^2 specimens (one batched solve per step)."""
+    import torch
+    from lpm_b200 import core
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    seeds = list(range(10))
+    lat, Kn_h, Tv_h, fixed, up_h = plain2d_specimens(seeds)
+    dl = core.DeviceLattice(lat, dev)
+    Kn, Tv = torch.as_tensor(Kn_h, device=dev), torch.as_tensor(Tv_h, device=dev)
+    free = torch.as_tensor((~fixed).astype(np.float64), device=dev)
+    up = torch.as_tensor(np.where(fixed, up_h, 0.0), device=dev)
+    B = len(seeds)
+
+    def step(Kn, Tv, free, up):
+        b = -core.kmv(dl, up[None].expand(B, -1, -1), Kn, Tv) * free
+        x, info = core.cg(dl, Kn, Tv, b, free=free, tol=1e-10, maxit=200000, check=1, poll=50, precheck=True)
+        return up + x, info
+
+    for _ in range(max(a.warmup, 3)):
+        u, info = step(Kn, Tv, free, up)
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(dev.index or 0)
+    sampler.start()
+    ev0.record()
+    for _ in range(a.steps):
+        u, info = step(Kn, Tv, free, up)
+    ev1.record()
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    # end to end: host arrays in, host solution out
+    Kp, Tp = torch.as_tensor(Kn_h).pin_memory(), torch.as_tensor(Tv_h).pin_memory()
+    out = torch.empty((B, lat.N, 2), dtype=torch.float64).pin_memory()
+    torch.cuda.synchronize(dev)
+    ev0.record()
+    for _ in range(a.steps):
+        uu, _ = step(Kp.to(dev, non_blocking=True), Tp.to(dev, non_blocking=True), free, up)
+        out.copy_(uu, non_blocking=True)
+    ev1.record()
+    torch.cuda.synchronize(dev)
+    ms_e2e = ev0.elapsed_time(ev1)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.set_threads(os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    _, cinfo = O.sq_solve_cg(lat, Kn_h[0], Tv_h[0], fixed, up_h, tol=1e-10)
+    cpu_s = time.perf_counter() - t0
+    its = info.iters
+    bytes_per_it = B * lat.N * (128 + 32)            # FP64 2D K.u: Kn+Tv (2*8*8 B) + u, f (2*2*8 B) per particle
+    line = {"metric": "solves/s at rel.res 1e-10 (plain FP64 CG, 2D 128^2)", "value": B * a.steps / (ms / 1e3),
+            "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": max(a.warmup, 3), "ms_per_step": ms / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Gaussian random fields, shapes of the 128^2 config)",
+            "config": {"workload": "2D square 128^2 GRF corr6 phi0.30 contrast10 nu0.25 plane stress, uniaxial "
+                                   "tension, FP64 plain CG to 1e-10 (cg2plain semantics)", "specimens": B,
+                       "l2": "L2-resident (%.1f MB of FP64 coefficients)" % (Kn_h.nbytes * 2 / 1e6)},
+            "iters_mean": float(its.mean()), "all_converged": bool((info.status == 0).all()),
+            "kmv_effective_gbs": None,
+            "e2e": {"value": B * a.steps / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(Kp.numel() * 16),
+                    "d2h_bytes_per_step": int(out.numel() * 8)},
+            "cpu_baseline": {"value": 1.0 / cpu_s, "unit": UNIT, "cores": O.get_threads(), "kind": "port",
+                             "sample": "specimen 0 by the C oracle's plain CG (timing/t2d/cg2plain.py:11-68), "
+                                       "%d iterations, %.2f s" % (cinfo["iters"], cpu_s)},
+            "clocks": clocks}
+    line["kmv_effective_gbs"] = bytes_per_it * float(its.max()) / (ms / a.steps / 1e3) / 1e9
+    print(json.dumps(line), flush=True)
+
+
+def run_coarse2d(a):
+    """cfg 3: differentiable coarse 2D solve (128^2 coarse from 256^2 fine at s = 2), 3 loads, MSE loss against a
+    seeded target; forward + backward time, gradient vs central finite differences on 64 random bonds (FP64)."""
+    import torch
+    from lpm_b200 import geom, micro
+    from lpm_b200 import torch_lpm as T2
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    nf, s = 256, 2
+    nc = nf // s
+    ph = micro.grf_two_phase(nf, nf, 6.0, 0.30, 3)
+    Cpix = geom.iso_C2d(np.where(ph == 1, 10.0, 1.0), 0.25, plane="stress")
+    model = T2.CoarseT(nc, nc, s, 1.0, device=dev, loads=["lr_tx", "tb_ty", "tb_sx"])
+    lat = model.lat
+    cp = geom.cell_params_from_C6(geom.voigt_cells2d(Cpix, nf, nf, s))
+    K0, T0 = geom.bond_params_from_cells2d(lat, cp)
+    rng = np.random.default_rng(11)
+    q = np.where(lat.valid, lat.nbr, 0)
+    opp = np.repeat(lat.opp[None, :], lat.N, 0)
+
+    def lognormal_sym(rg):
+        z = rg.standard_normal((lat.N, 8))
+        z = np.where(np.arange(8)[None, :] % 2 == 0, z, z[q, opp])      # one factor per undirected bond
+        return np.exp(0.2 * z)
+    f0 = lognormal_sym(rng).astype(np.float32).astype(np.float64)
+    target = model.run(torch.as_tensor(K0 * lognormal_sym(rng), device=dev)[None],
+                       torch.as_tensor(T0, device=dev)[None])
+    tgt = {ld: v["u"].detach() for ld, v in target.items()}
+    Kb = torch.as_tensor(K0 * f0, device=dev)[None]
+    Tb = torch.as_tensor(T0, device=dev)[None]
+    qt, ot = torch.as_tensor(q, device=dev), torch.as_tensor(opp, device=dev)
+    valid = torch.as_tensor(lat.valid, device=dev, dtype=torch.float64)
+
+    def loss_of(th):
+        Kn = Kb * torch.exp(0.5 * (th + th[:, qt, ot])) * valid
+        out = model.run(Kn, Tb)
+        return sum(((out[ld]["u"] - tgt[ld]) ** 2).mean() for ld in tgt)
+
+    th = torch.zeros((1, lat.N, 8), dtype=torch.float64, device=dev, requires_grad=True)
+    for _ in range(max(a.warmup, 3)):
+        th.grad = None
+        loss_of(th).backward()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        th.grad = None
+        L = loss_of(th)
+        L.backward()
+    torch.cuda.synchronize(dev)
+    fb_ms = (time.perf_counter() - t0) / a.steps * 1e3
+    # gradient check at a tighter solve tolerance, so that the differences of two solves resolve h = 1e-6
+    model.tol = 1e-14
+    th.grad = None
+    loss_of(th).backward()
+    g = th.grad.detach().clone()
+    # central differences on 64 random undirected bonds (perturbing theta of the (i, k) slot, k even)
+    ii = rng.choice(np.flatnonzero(lat.valid[:, 0]), 64, replace=False)
+    kk = rng.choice(np.arange(0, 8, 2), 64)
+    h = 1e-6
+    errs = []
+    with torch.no_grad():
+        for i, k in zip(ii, kk):
+            e = torch.zeros_like(th)
+            e[0, i, k] = h
+            fd = (float(loss_of(th + e)) - float(loss_of(th - e))) / (2 * h)
+            ad = float(g[0, i, k])
+            errs.append(abs(fd - ad) / max(abs(fd), abs(ad), 1e-300))
+    errs = np.array(errs)
+    line = {"metric": "forward+backward ms (differentiable 2D coarse solve, 128^2, 3 loads)", "value": fb_ms,
+            "unit": "ms", "n_gpus": 1, "steps": a.steps, "warmup": max(a.warmup, 3), "ms_per_step": fb_ms,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded GRF 256^2 fine, Voigt cells s = 2, lognormal(0.2) per undirected bond, "
+                    "parameters rounded to FP32)",
+            "config": {"workload": "2D coarse 128^2 from 256^2 at s = 2, loads lr_tx tb_ty tb_sx, MSE loss vs "
+                                   "seeded target displacements, adjoint gradient w.r.t. log bond stiffness",
+                       "solve_tol": 1e-12, "gradient_check_solve_tol": 1e-14},
+            "gradient_check": {"bonds": 64, "h": h, "rel_err_max": float(errs.max()),
+                               "rel_err_median": float(np.median(errs))},
+            "loss": float(L.detach())}
+    print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------------------------------------- GPU side
 def main():
     ap = argparse.ArgumentParser()
@@ -213,7 +542,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--batch", type=int, default=None, help="specimens per GPU (default 16 for spheres48, 1 else)")
-    ap.add_argument("--workload", default="spheres48", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="spheres48", choices=sorted(WORKLOADS) + ["serve", "plain2d", "coarse2d"])
+    ap.add_argument("--requests", type=int, default=40, help="serving stream: number of requests")
+    ap.add_argument("--load-factor", type=float, default=0.7, help="serving stream: arrival rate / capacity")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 CG comparator")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
@@ -221,6 +552,12 @@ def main():
     a = ap.parse_args()
     if a.batch is None:
         a.batch = 16 if a.workload == "spheres48" else 1
+    if a.workload == "serve":
+        return run_serve(a)
+    if a.workload == "plain2d":
+        return run_plain2d(a)
+    if a.workload == "coarse2d":
+        return run_coarse2d(a)
     if a.impl == "reference":
         return run_reference(a)
 

@@ -122,6 +122,9 @@ class Bucket:
         self.slots = [None] * S
         self.queue = collections.deque()
         self.rounds = 0
+        self.busy_s = 0.0
+        self.admit_s = 0.0
+        self.inner_iters = 0
         self.idle_since = time.perf_counter()
 
     # ------------------------------------------------------------------------------------------------ state
@@ -145,6 +148,7 @@ class Bucket:
                                                                                       self.R))
         R, d, N = self.R, self.d, self.N
         sl = slice(s * R, (s + 1) * R)
+        t_adm = time.perf_counter()
         with torch.cuda.stream(self.stream):
             dv = self.device
             self.K64[s].copy_(torch.as_tensor(req.Kn), non_blocking=False)
@@ -165,12 +169,14 @@ class Bucket:
             self.x[sl] = 0.0
         self.slots[s] = req
         req.admitted = time.perf_counter()
+        self.admit_s += req.admitted - t_adm
 
     def round(self):
         """One refinement step over the bucket.  Returns the per-system (relres, status) on the host."""
         lib = L.load()
         opts = L.IrOpts(float(self.tol), float(self.inner_tol), int(self.maxit), 1, 1, 10, None)
         outer = ctypes.c_int32(0)
+        t0 = time.perf_counter()
         with torch.cuda.stream(self.stream):
             L.check(lib.lpm_ir_batched(self.dl.ref, L.ptr(self.K64), L.ptr(self.T64), L.LAYOUT_REF, L.ptr(self.K32),
                                        L.ptr(self.T32), L.ptr(self.M32), ctypes.byref(self._batch), L.ptr(self.mask),
@@ -181,6 +187,8 @@ class Bucket:
             st = self.st.cpu().numpy()
             its = self.it.cpu().numpy()
         self.rounds += 1
+        self.busy_s += time.perf_counter() - t0
+        self.inner_iters += int(its.max())
         return rel, st, its
 
     def retire(self, s, status):
@@ -208,13 +216,14 @@ class Server:
     released.  `bucket_factory(key, slots, rmax)` builds buckets (the CUDA `Bucket` by default)."""
 
     def __init__(self, device="cuda", budget_bytes=None, rmax=9, max_slots=8, tol=1e-8, inner_tol=1e-5,
-                 max_rounds=40, idle_release_s=0.5, bucket_factory=None, bytes_fn=bucket_bytes):
+                 max_rounds=40, idle_release_s=0.5, bucket_factory=None, bytes_fn=bucket_bytes, rmax2d=None):
         self.device = torch.device(device)
         if budget_bytes is None:
             free, _ = torch.cuda.mem_get_info(self.device)
             budget_bytes = int(0.6 * free)
         self.budget = int(budget_bytes)
         self.rmax, self.max_slots = rmax, max_slots
+        self.rmax2d = rmax if rmax2d is None else rmax2d   # system slots per specimen of 2D buckets
         self.tol, self.inner_tol, self.max_rounds = tol, inner_tol, max_rounds
         self.idle_release_s = idle_release_s
         self.bytes_fn = bytes_fn
@@ -233,11 +242,14 @@ class Server:
     def used_bytes(self):
         return sum(self.reserved.values())
 
+    def _rmax(self, key):
+        return self.rmax2d if key[0] == 2 else self.rmax
+
     def _slots_for(self, key):
         """Largest slot count (<= max_slots) whose bucket fits in the remaining budget; 0 if none fits."""
         left = self.budget - self.used_bytes()
         for s in range(self.max_slots, 0, -1):
-            if self.bytes_fn(key, s, self.rmax) <= left:
+            if self.bytes_fn(key, s, self._rmax(key)) <= left:
                 return s
         return 0
 
@@ -262,10 +274,10 @@ class Server:
                 slots = self._slots_for(req.key)
             if slots == 0:
                 return False
-            b = self.factory(req.key, slots, self.rmax)
+            b = self.factory(req.key, slots, self._rmax(req.key))
             b.retired = False
             self.buckets[req.key] = b
-            self.reserved[req.key] = self.bytes_fn(req.key, slots, self.rmax)
+            self.reserved[req.key] = self.bytes_fn(req.key, slots, self._rmax(req.key))
             t = threading.Thread(target=self._worker, args=(req.key, b), daemon=True)
             self.threads[req.key] = t
             t.start()
@@ -274,8 +286,8 @@ class Server:
         return True
 
     def submit(self, req):
-        if req.nloads < 1 or req.nloads > self.rmax:
-            raise ValueError("a request brings 1..%d load cases (got %d)" % (self.rmax, req.nloads))
+        if req.nloads < 1 or req.nloads > self._rmax(req.key):
+            raise ValueError("a request brings 1..%d load cases (got %d)" % (self._rmax(req.key), req.nloads))
         if req.arrival is None:
             req.arrival = time.perf_counter()
         with self.lock:
@@ -353,6 +365,17 @@ class Server:
             self.lock.notify_all()
         for t in self.threads.values():
             t.join(timeout=30)
+
+
+def bucket_stats(server):
+    """Per-bucket activity of a server: rounds, GPU-side busy seconds of the rounds, admission seconds, inner PCG
+    iterations (slowest system per round, summed), capacity."""
+    out = {}
+    for key, b in list(server.buckets.items()):
+        out["%dD %s" % (key[0], "x".join(str(v) for v in key[1:1 + key[0]]))] = {
+            "slots": b.S, "rounds": b.rounds, "busy_s": round(getattr(b, "busy_s", 0.0), 3),
+            "admit_s": round(getattr(b, "admit_s", 0.0), 3), "inner_iters": getattr(b, "inner_iters", 0)}
+    return out
 
 
 def latency_stats(reqs):
