@@ -15,9 +15,11 @@
 // stopping test is on the FP64 true residual.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "lpm_cg.h"
+#include "lpm_graph.h"
 #include "lpm_tma.h"
 
 namespace lpm {
@@ -129,13 +131,14 @@ __global__ void __launch_bounds__(VB) k_cg_init(int64_t N, int sys0, Batch bt, c
 
 // ----------------------------------------------------------------------------------------------------- update
 template <typename T, int DIM, bool PREC>
-__global__ void __launch_bounds__(VB) k_cg_update(int64_t N, int sys0, Batch bt, int it, int check, int maxit,
-                                                  double tol, const uint8_t* __restrict__ mask,
+__global__ void __launch_bounds__(VB) k_cg_update(int64_t N, int sys0, Batch bt, int it_host, int check,
+                                                  int maxit, double tol, const uint8_t* __restrict__ mask,
                                                   const T* __restrict__ Minv, T* __restrict__ x, T* __restrict__ r,
                                                   T* __restrict__ z, const T* __restrict__ p,
                                                   const T* __restrict__ Ap, CgScalars sc)
 {
     __shared__ double sh[32];
+    const int it = sc.itp ? *sc.itp : it_host;
     const int s = sys0 + blockIdx.y;
     const int cur = (it - 1) & 1, nxt = it & 1;
     const int act = sc.act[s];
@@ -205,6 +208,7 @@ template <typename T, int DIM>
 __global__ void __launch_bounds__(VB) k_cg_pupdate(int64_t N, int sys0, const T* __restrict__ z, T* __restrict__ p,
                                                    CgScalars sc)
 {
+    if (sc.itp && sys0 == 0 && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) atomicAdd(sc.itp, 1);
     const int s = sys0 + blockIdx.y;
     if (!sc.act[s]) return;
     const int64_t i = (int64_t)blockIdx.x * VB + threadIdx.x;
@@ -329,6 +333,7 @@ void carve_cg(Carver& cv, const Lattice& L, int nsys, bool precond, CgWork<T>& w
     w.mv_part = cv.take<double>((size_t)nsys * kmv_dot_blocks(L));
     w.mv_cnt = cv.take<unsigned>(nsys);
     w.mv_final = w.sc.pAp;
+    w.sc.itp = cv.take<int>(1);
 }
 
 template <typename T>
@@ -467,26 +472,39 @@ int cg_solve(const Lattice& L, const T* Kn, const T* Tv, const CoefLayout& cl, c
     e = cudaMemcpyAsync(&nconv, w.sc.nconv, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return (int)e;
-    for (int it = 1; it <= o.maxit && nconv < (unsigned)bt.nsys; ++it) {
+    static const int kOne = 1;
+    if ((e = cudaMemcpyAsync(w.sc.itp, &kOne, sizeof(int), cudaMemcpyHostToDevice, st)) != cudaSuccess) return (int)e;
+    auto one_iter = [&](int it, cudaStream_t s) -> cudaError_t {
         timer.begin(nconv == 0);
-        e = launch_kmv<T>(L, w.p, Kn, Tv, cl, bt, w.Ap, w.st, &ep, st);
+        cudaError_t ee = launch_kmv<T>(L, w.p, Kn, Tv, cl, bt, w.Ap, w.st, &ep, s);
         timer.end();
-        if (e != cudaSuccess) return (int)e;
+        if (ee != cudaSuccess) return ee;
         for (int s0 = 0; s0 < bt.nsys; s0 += 65535) {
             const int ns = bt.nsys - s0 < 65535 ? bt.nsys - s0 : 65535;
             const dim3 g(nb, ns);
             if (L.dim == 3)
-                launch_update<T, 3>(g, st, precond, bt, N, s0, it, o, mask, Minv, x, w);
+                launch_update<T, 3>(g, s, precond, bt, N, s0, it, o, mask, Minv, x, w);
             else
-                launch_update<T, 2>(g, st, precond, bt, N, s0, it, o, mask, Minv, x, w);
+                launch_update<T, 2>(g, s, precond, bt, N, s0, it, o, mask, Minv, x, w);
         }
-        if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
-        if (it % o.poll == 0 || it == o.maxit) {
-            e = cudaMemcpyAsync(&nconv, w.sc.nconv, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-            if (e != cudaSuccess) return (int)e;
-            timer.collect();
-        }
+        return cudaGetLastError();
+    };
+    GraphKey key;
+    key.ptr = {ws, Kn, Tv, mask, x, Minv, L.nbr, nullptr, nullptr, nullptr};
+    key.val = {2, bt.nsys, bt.rhs_per_set, bt.nmask, L.nx, L.ny, L.nz, o.poll, o.check, o.maxit, precond ? 1 : 0,
+               (long long)sizeof(T), cl.set_stride, cl.slot_stride * 1000003LL + cl.site_stride, L.dim, 0};
+    double tolv = o.tol;
+    std::memcpy(&key.val[15], &tolv, sizeof(double));
+    int it = 1;
+    while (it <= o.maxit && nconv < (unsigned)bt.nsys) {
+        const int block = std::min(o.poll - (it - 1) % o.poll, o.maxit - it + 1);
+        const bool use_graph = !o.prof && it > 1 && block == o.poll;
+        if ((e = run_iteration_block(use_graph, key, it, block, st, one_iter)) != cudaSuccess) return (int)e;
+        it += block;
+        e = cudaMemcpyAsync(&nconv, w.sc.nconv, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return (int)e;
+        timer.collect();
     }
     timer.collect();
     return LPM_OK;

@@ -10,10 +10,11 @@
 // (npair, N, 3, 2); its output is unmasked, so the update masks Ap (p stays zero on fixed DOFs, so p.Ap needs no
 // mask).  Reductions are deterministic (per-block partials summed in fixed order by a last block).
 #include <algorithm>
+#include <cstring>
 #include <map>
 #include <mutex>
-#include <tuple>
 
+#include "lpm_graph.h"
 #include "lpm_tma.h"
 
 namespace lpm {
@@ -614,62 +615,6 @@ void carve(Carve& c, const Lattice& L, int nsys, int rps, bool precond, FWork<T>
     w.sc.itp = c.take<int>(1);
 }
 
-// ----------------------------------------------------------------------------------------- graph replay
-// A block of `poll` iterations (operator + update + p-update each) depends only on the buffers, sizes and options
-// below, and reads the iteration number from device memory; it is captured once as a CUDA graph and replayed for
-// every later block with the same key (e.g. every inner solve of a refinement loop, every round of a serving bucket).
-struct GraphKey {
-    const void *ws, *Kn, *Tv, *mask, *x;
-    int nsys, rps, nmask, nx, ny, nz, poll, check, maxit, precond, elem;
-    double tol;
-    bool operator<(const GraphKey& o) const
-    {
-        return std::tie(ws, Kn, Tv, mask, x, nsys, rps, nmask, nx, ny, nz, poll, check, maxit, precond, elem, tol) <
-               std::tie(o.ws, o.Kn, o.Tv, o.mask, o.x, o.nsys, o.rps, o.nmask, o.nx, o.ny, o.nz, o.poll, o.check,
-                        o.maxit, o.precond, o.elem, o.tol);
-    }
-};
-
-class GraphCache {
-public:
-    cudaGraphExec_t find(const GraphKey& k)
-    {
-        std::lock_guard<std::mutex> g(mu_);
-        auto it = map_.find(k);
-        return it == map_.end() ? nullptr : it->second;
-    }
-    void put(const GraphKey& k, cudaGraphExec_t e)
-    {
-        std::lock_guard<std::mutex> g(mu_);
-        if (map_.size() >= 64) {  // bounded: drop everything (entries are cheap to re-capture)
-            for (auto& kv : map_) cudaGraphExecDestroy(kv.second);
-            map_.clear();
-        }
-        map_[k] = e;
-    }
-
-private:
-    std::mutex mu_;
-    std::map<GraphKey, cudaGraphExec_t> map_;
-};
-
-// One non-blocking stream per host thread and device for graph capture (never used to run work).
-cudaStream_t capture_stream()
-{
-    thread_local cudaStream_t streams[64] = {};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-    if (!streams[dev] && cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking) != cudaSuccess)
-        streams[dev] = nullptr;
-    return streams[dev];
-}
-
-GraphCache& graph_cache()
-{
-    static GraphCache* c = new GraphCache();  // never destroyed: graphs may outlive static destruction order
-    return *c;
-}
-
 // One operator launch: out = K u, with the alpha-step epilogue when epi.
 template <typename T>
 struct Operator {
@@ -864,40 +809,18 @@ int cg_solve_fused(const Lattice& L, const T* Kn, const T* Tv, const Batch& bt, 
             launch_iter<T, false>(paired, vg, pg, s, G, it, o, mask, x, w);
         return cudaGetLastError();
     };
-    const GraphKey key{ws, Kn, Tv, mask, x, bt.nsys, bt.rhs_per_set, bt.nmask, L.nx, L.ny, L.nz, o.poll, o.check,
-                       o.maxit, precond ? 1 : 0, (int)sizeof(T), o.tol};
+    GraphKey key;
+    key.ptr = {ws, Kn, Tv, mask, x, nullptr, nullptr, nullptr, nullptr, nullptr};
+    key.val = {1, bt.nsys, bt.rhs_per_set, bt.nmask, L.nx, L.ny, L.nz, o.poll, o.check, o.maxit, precond ? 1 : 0,
+               (long long)sizeof(T), 0, 0, 0, 0};
+    double tolv = o.tol;
+    std::memcpy(&key.val[12], &tolv, sizeof(double));
     int it = 1;
     while (it <= o.maxit && nconv < (unsigned)bt.nsys) {
         const int block = std::min(o.poll - (it - 1) % o.poll, o.maxit - it + 1);
         // full blocks after the first one replay a captured graph (not while per-launch timings are requested)
-        cudaGraphExec_t ge = nullptr;
-        if (!o.prof && it > 1 && block == o.poll) {
-            ge = graph_cache().find(key);
-            if (!ge) {
-                // captured on a private stream (the caller's may be the legacy default stream, which cannot be
-                // captured); the graph is then launched on the caller's stream
-                cudaStream_t cs = capture_stream();
-                if (!cs) return (int)cudaErrorNotReady;
-                cudaGraph_t g = nullptr;
-                if ((e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return (int)e;
-                cudaError_t ce = cudaSuccess;
-                for (int b = 0; b < block && ce == cudaSuccess; ++b) ce = one_iter(it + b, cs);
-                e = cudaStreamEndCapture(cs, &g);
-                if (ce != cudaSuccess) {
-                    if (g) cudaGraphDestroy(g);
-                    return (int)ce;
-                }
-                if (e != cudaSuccess) return (int)e;
-                e = cudaGraphInstantiate(&ge, g, 0);
-                cudaGraphDestroy(g);
-                if (e != cudaSuccess) return (int)e;
-                graph_cache().put(key, ge);
-            }
-            if ((e = cudaGraphLaunch(ge, st)) != cudaSuccess) return (int)e;
-        } else {
-            for (int b = 0; b < block; ++b)
-                if ((e = one_iter(it + b, st)) != cudaSuccess) return (int)e;
-        }
+        const bool use_graph = !o.prof && it > 1 && block == o.poll;
+        if ((e = run_iteration_block(use_graph, key, it, block, st, one_iter)) != cudaSuccess) return (int)e;
         it += block;
         e = cudaMemcpyAsync(&nconv, w.sc.nconv, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -914,6 +837,39 @@ int cg_solve_fused(const Lattice& L, const T* Kn, const T* Tv, const Batch& bt, 
     if (e != cudaSuccess) return (int)e;
     if (err) rc = LPM_ERR_TIMEOUT;
     return rc;
+}
+
+// ----------------------------------------------------------------------------------------- graph cache
+namespace {
+std::mutex g_graph_mu;
+std::map<GraphKey, cudaGraphExec_t>* g_graphs = new std::map<GraphKey, cudaGraphExec_t>();  // never destroyed
+}  // namespace
+
+cudaGraphExec_t graph_find(const GraphKey& k)
+{
+    std::lock_guard<std::mutex> g(g_graph_mu);
+    auto it = g_graphs->find(k);
+    return it == g_graphs->end() ? nullptr : it->second;
+}
+
+void graph_put(const GraphKey& k, cudaGraphExec_t e)
+{
+    std::lock_guard<std::mutex> g(g_graph_mu);
+    if (g_graphs->size() >= 64) {  // bounded: drop everything (entries are cheap to capture again)
+        for (auto& kv : *g_graphs) cudaGraphExecDestroy(kv.second);
+        g_graphs->clear();
+    }
+    (*g_graphs)[k] = e;
+}
+
+cudaStream_t graph_capture_stream()
+{
+    thread_local cudaStream_t streams[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    if (!streams[dev] && cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking) != cudaSuccess)
+        streams[dev] = nullptr;
+    return streams[dev];
 }
 
 template int cg_solve_fused<float>(const Lattice&, const float*, const float*, const Batch&, const float*,

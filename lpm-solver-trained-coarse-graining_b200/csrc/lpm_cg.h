@@ -22,6 +22,7 @@ struct CgScalars {
     double* relres;    // caller output
     int* status;       // caller output
     int nblk;          // partial blocks per system of the vector kernels
+    int* itp;          // device copy of the current iteration number, advanced by the p-update kernel
 };
 
 // Optional CUDA-event timing of the operator launches of a solve (prof != nullptr).  prof[0] += ms and prof[1] += count
