@@ -147,6 +147,28 @@ class ClockSampler:
         return out
 
 
+# ------------------------------------------------------------------------------------------------ ranks
+def shard_seeds(rank, batch):
+    """Specimen seeds of a rank: every rank solves its own `batch` specimens (weak scaling, no shared data)."""
+    return [rank * batch + j for j in range(batch)]
+
+
+def max_over_ranks(ms, world, device):
+    """Step time of the job: the slowest rank's (NCCL on GPUs, gloo in the CPU tests)."""
+    if world <= 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world, systems_per_rank, steps, ms):
+    """Whole-job solves/s: the systems all ranks solved over the max-over-ranks time."""
+    return world * systems_per_rank * steps / (ms / 1e3)
+
+
 # ------------------------------------------------------------------------------------------------ CPU side
 def kmv_traffic(nsys):
     """DRAM bytes per K.u launch for `nsys` systems of the 48^3 workload (6 per specimen), scaled from the ncu capture
@@ -574,7 +596,7 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
 
-    seeds = [rank * a.batch + j for j in range(a.batch)]
+    seeds = shard_seeds(rank, a.batch)
     lat, Kn_h, Tv_h, free_h, ups_h = load_workload(a.workload, seeds)
     B = a.batch
     Lc = len(WORKLOADS[a.workload]["loads"])
@@ -615,12 +637,8 @@ def main():
     ev1.record()
     barrier()
     clocks = sampler.stop()
-    ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * nsys * a.steps / (ms / 1e3)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world, dev)
+    value = job_throughput(world, nsys, a.steps, ms)
     ok = all((i.status == 0).all() and (i.relres <= TOL).all() for i in infos)
     iters = np.concatenate([i.iters for i in infos])
 
@@ -672,12 +690,8 @@ def main():
         e2e_step()
     ev1.record()
     barrier()
-    ms_e2e = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms_e2e], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-    e2e = {"value": world * nsys * a.steps / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+    ms_e2e = max_over_ranks(ev0.elapsed_time(ev1), world, dev)
+    e2e = {"value": job_throughput(world, nsys, a.steps, ms_e2e), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h)}
 
     # ---- comparator: plain FP64 GPU CG on the same batch with this library's fastest FP64 path (packed
