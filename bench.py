@@ -570,7 +570,7 @@ def main():
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 CG comparator")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--inner-tol", type=float, default=1e-5)
+    ap.add_argument("--inner-tol", type=float, default=1e-3)
     a = ap.parse_args()
     if a.batch is None:
         a.batch = 16 if a.workload == "spheres48" else 1

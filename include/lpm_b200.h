@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define LPM_ABI_VERSION 1
+#define LPM_ABI_VERSION 2
 
 /* return codes */
 #define LPM_OK 0
@@ -69,6 +69,7 @@ typedef struct lpm_cg_opts {
     int32_t poll;     /* host reads the converged count every `poll` iterations */
     int32_t precheck; /* 1: test the initial residual before iterating (cg2plain.cg_mf / solver2d.pcg_mf) */
     double* prof;     /* optional HOST array of 4: K.u ms / launches, and the same for full-batch launches */
+    const double* tol_sys; /* optional DEVICE array (nsys): per-system tolerance used instead of tol */
 } lpm_cg_opts;
 
 typedef struct lpm_ir_opts {
@@ -153,8 +154,10 @@ int64_t lpm_ir_workspace_bytes(const lpm_lattice* lat, const lpm_batch* batch, i
 /* FP32 inner PCG + FP64 iterative refinement to |b - K x| <= tol |b| on the FP64 operator.
  * Kn64/Tv64: FP64 coefficients (coef_layout64); Kn32/Tv32: the same packed to FP32 SoA (lpm_pack_coef_f32);
  * Minv32: FP32 block-Jacobi inverse or NULL.  x (FP64) updated in place, zero on fixed DOFs on entry.
- * Outputs: total inner iterations, final FP64 relative residual, status per system (device arrays); outer_steps is a
- * HOST pointer (may be NULL) that receives the number of refinement steps. */
+ * Each refinement step solves K d = r/|r| of system s by FP32 PCG to the relative tolerance
+ * max(inner_tol, tol / (4 rel_s)), rel_s its FP64 relative residual (inexact refinement: the last step reduces only
+ * what is left; a system's iterations never depend on the other systems of the batch).  Outputs: total inner iterations, final FP64 relative residual, status per system (device arrays);
+ * outer_steps is a HOST pointer (may be NULL) that receives the number of refinement steps. */
 int lpm_ir_batched(const lpm_lattice* lat, const double* Kn64, const double* Tv64, int32_t coef_layout64,
                    const float* Kn32, const float* Tv32, const float* Minv32, const lpm_batch* batch,
                    const uint8_t* mask, const double* b, double* x, const lpm_ir_opts* opts, void* workspace,

@@ -29,7 +29,7 @@ class Batch(ctypes.Structure):
 
 class CgOpts(ctypes.Structure):
     _fields_ = [("tol", _c_d), ("maxit", _c_i32), ("check", _c_i32), ("poll", _c_i32), ("precheck", _c_i32),
-                ("prof", _P(_c_d))]
+                ("prof", _P(_c_d)), ("tol_sys", _c_p)]
 
 
 class IrOpts(ctypes.Structure):

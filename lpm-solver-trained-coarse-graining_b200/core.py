@@ -250,7 +250,7 @@ def cg(dl, Kn, Tv, b, x=None, Minv=None, free=None, tol=1e-10, maxit=20000, chec
     rel = torch.zeros(nsys, dtype=_F64, device=bf.device)
     st = torch.zeros(nsys, dtype=torch.int32, device=bf.device)
     opts = L.CgOpts(float(tol), int(maxit), int(check), int(poll or max(check, 10)), int(bool(precheck)),
-                    _prof_ptr(prof))
+                    _prof_ptr(prof), None)
     fn = lib.lpm_cg_batched_f64 if prec == L.LPM_F64 else lib.lpm_cg_batched_f32
     L.check(fn(dl.ref, L.ptr(Kc), L.ptr(Tc), layout, ctypes.byref(b_), L.ptr(Minv), L.ptr(m), L.ptr(bf), L.ptr(xf),
                int(x0_zero), ctypes.byref(opts), L.ptr(ws), ws.numel(), L.ptr(it), L.ptr(rel), L.ptr(st),
@@ -259,7 +259,7 @@ def cg(dl, Kn, Tv, b, x=None, Minv=None, free=None, tol=1e-10, maxit=20000, chec
     return xf.reshape(b.shape), info
 
 
-def ir(dl, Kn64, Tv64, b, x=None, free=None, tol=1e-8, inner_tol=1e-5, maxit=20000, max_outer=20, check=1,
+def ir(dl, Kn64, Tv64, b, x=None, free=None, tol=1e-8, inner_tol=1e-3, maxit=20000, max_outer=20, check=1,
        poll=10, precond=True, packed=None, prof=None):
     """Mixed-precision solve: FP32 inner PCG, FP64 iterative refinement to |b - K x| <= tol |b| (FP64 operator).
 

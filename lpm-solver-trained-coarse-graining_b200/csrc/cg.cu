@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(VB) k_cg_init(int64_t N, int sys0, Batch bt, c
     const double rel = bn > 0.0 ? sqrt(tot[2]) / bn : 0.0;
     const bool finite = isfinite(bn) && isfinite(tot[1]) && isfinite(tot[2]);
     int act = bn > 0.0 && finite;
-    if (act && precheck && rel <= tol) act = 0;
+    if (act && precheck && rel <= (sc.tols ? sc.tols[s] : tol)) act = 0;
     sc.bn[s] = bn;
     sc.rz[s] = tot[1];
     sc.rr[s] = tot[2];
@@ -184,6 +184,7 @@ __global__ void __launch_bounds__(VB) k_cg_update(int64_t N, int sys0, Batch bt,
     sc.rr[s] = rrn;
     sc.beta[s] = rzc != 0.0 ? rzn / rzc : 0.0;
     const double rel = sqrt(rrn) / sc.bn[s];
+    const double tl = sc.tols ? sc.tols[s] : tol;
     if (!isfinite(pAp) || pAp < 0.0 || !isfinite(rrn) || !isfinite(rzn)) {
         sc.act[s] = 0;
         sc.iters[s] = it;
@@ -194,10 +195,10 @@ __global__ void __launch_bounds__(VB) k_cg_update(int64_t N, int sys0, Batch bt,
     }
     if (it % check == 0 || it == maxit) {
         sc.relres[s] = rel;
-        if (rel <= tol || it == maxit) {
+        if (rel <= tl || it == maxit) {
             sc.act[s] = 0;
             sc.iters[s] = it;
-            if (rel > tol) sc.status[s] = LPM_STATUS_NOT_CONVERGED;
+            if (rel > tl) sc.status[s] = LPM_STATUS_NOT_CONVERGED;
             atomicAdd(sc.nconv, 1u);
         }
     }
@@ -343,7 +344,7 @@ struct IrWork {
     unsigned* cnt;
     float *r32, *d32;
     int *it_in, *st_in;
-    double* rel_in;
+    double *rel_in, *itol;
     void* cg_ws;
     size_t cg_bytes;
 };
@@ -363,6 +364,7 @@ void carve_ir(Carver& cv, const Lattice& L, const Batch& bt, bool precond, IrWor
     w.it_in = cv.take<int>(nsys);
     w.st_in = cv.take<int>(nsys);
     w.rel_in = cv.take<double>(nsys);
+    w.itol = cv.take<double>(nsys);
     w.cg_bytes = cg_workspace_bytes(L, bt, LPM_F32, precond);
     w.cg_ws = cv.take<char>(w.cg_bytes);
 }
@@ -445,6 +447,7 @@ int cg_solve(const Lattice& L, const T* Kn, const T* Tv, const CoefLayout& cl, c
     w.sc.iters = iters;
     w.sc.relres = relres;
     w.sc.status = status;
+    w.sc.tols = o.tol_sys;
     const int64_t N = L.N;
     cudaError_t e = cudaMemsetAsync(w.sc.cnt, 0, sizeof(unsigned) * bt.nsys, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.mv_cnt, 0, sizeof(unsigned) * bt.nsys, st);
@@ -490,7 +493,7 @@ int cg_solve(const Lattice& L, const T* Kn, const T* Tv, const CoefLayout& cl, c
         return cudaGetLastError();
     };
     GraphKey key;
-    key.ptr = {ws, Kn, Tv, mask, x, Minv, L.nbr, nullptr, nullptr, nullptr};
+    key.ptr = {ws, Kn, Tv, mask, x, Minv, L.nbr, o.tol_sys, nullptr, nullptr};
     key.val = {2, bt.nsys, bt.rhs_per_set, bt.nmask, L.nx, L.ny, L.nz, o.poll, o.check, o.maxit, precond ? 1 : 0,
                (long long)sizeof(T), cl.set_stride, cl.slot_stride * 1000003LL + cl.site_stride, L.dim, 0};
     double tolv = o.tol;
@@ -534,7 +537,7 @@ int ir_solve(const Lattice& L, const double* Kn64, const double* Tv64, const Coe
     double *rn2 = w.scal, *bn2 = w.scal + ns, *scale = w.scal + 2 * ns, *step = w.scal + 3 * ns;
     std::vector<double> h(2 * (size_t)ns), hs(2 * (size_t)ns);
     std::vector<int> h_it(ns), h_st(ns), tot_it(ns, 0), fin_st(ns, LPM_STATUS_OK);
-    std::vector<double> h_rel(ns, 0.0);
+    std::vector<double> h_rel(ns, 0.0), h_tol(ns, o.inner_tol);
     cudaError_t e = cudaMemsetAsync(w.cnt, 0, sizeof(unsigned) * ns, st);
     if (e != cudaSuccess) return (int)e;
     const int nb = vec_blocks(N);
@@ -581,8 +584,15 @@ int ir_solve(const Lattice& L, const double* Kn64, const double* Tv64, const Coe
                 k_ir_scale<2><<<g, VB, 0, st>>>(N, s0, w.r64, scale, w.r32, w.d32);
         }
         int remaining = 0;
-        for (int s = 0; s < ns; ++s) remaining = std::max(remaining, o.maxit - tot_it[s]);
-        lpm_cg_opts io{o.inner_tol, remaining, o.check, o.poll, 0, o.prof};
+        for (int s = 0; s < ns; ++s) {
+            remaining = std::max(remaining, o.maxit - tot_it[s]);
+            // inexact refinement: an inner solve need not reduce its residual below what is left to reach tol
+            // (factor 4 of margin: the FP32 operator's own error stays well inside), and never below inner_tol
+            h_tol[s] = h_rel[s] > 0.0 ? std::min(0.5, std::max(o.inner_tol, 0.25 * o.tol / h_rel[s])) : o.inner_tol;
+        }
+        e = cudaMemcpyAsync(w.itol, h_tol.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return (int)e;
+        lpm_cg_opts io{o.inner_tol, remaining, o.check, o.poll, 0, o.prof, w.itol};
         rc = cg_solve<float>(L, Kn32, Tv32, cl32, bt, Minv32, mask, w.r32, w.d32, 1, io, w.cg_ws, w.cg_bytes,
                              w.it_in, w.rel_in, w.st_in, st);
         if (rc != LPM_OK) return rc;

@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(VB) k_fcg_init(VecGeom G, const T* __restrict_
         const double rel = bn > 0.0 ? sqrt(rr) / bn : 0.0;
         const bool finite = isfinite(bn) && isfinite(rz) && isfinite(rr);
         int act = bn > 0.0 && finite;
-        if (act && precheck && rel <= tol) act = 0;
+        if (act && precheck && rel <= (sc.tols ? sc.tols[s] : tol)) act = 0;
         sc.bn[s] = bn;
         sc.rz[s] = rz;
         sc.rr[s] = rr;
@@ -192,6 +192,7 @@ __device__ __forceinline__ void update_tail(const VecGeom& G, const Group& gr, i
         sc.rr[s] = rrn;
         sc.beta[s] = rzc != 0.0 ? rzn / rzc : 0.0;
         const double rel = sqrt(rrn) / sc.bn[s];
+        const double tl = sc.tols ? sc.tols[s] : tol;
         if (!isfinite(rrn) || !isfinite(rzn)) {
             sc.act[s] = 0;
             sc.iters[s] = it;
@@ -202,10 +203,10 @@ __device__ __forceinline__ void update_tail(const VecGeom& G, const Group& gr, i
         }
         if (it % check == 0 || it == maxit) {
             sc.relres[s] = rel;
-            if (rel <= tol || it == maxit) {
+            if (rel <= tl || it == maxit) {
                 sc.act[s] = 0;
                 sc.iters[s] = it;
-                if (rel > tol) sc.status[s] = LPM_STATUS_NOT_CONVERGED;
+                if (rel > tl) sc.status[s] = LPM_STATUS_NOT_CONVERGED;
                 atomicAdd(sc.nconv, 1u);
             }
         }
@@ -432,7 +433,7 @@ __global__ void __launch_bounds__(VB) k_pair_init(VecGeom G, const float* __rest
         const double rel = bn > 0.0 ? sqrt(rr) / bn : 0.0;
         const bool finite = isfinite(bn) && isfinite(rz) && isfinite(rr);
         int act = bn > 0.0 && finite;
-        if (act && precheck && rel <= tol) act = 0;
+        if (act && precheck && rel <= (sc.tols ? sc.tols[s] : tol)) act = 0;
         sc.bn[s] = bn;
         sc.rz[s] = rz;
         sc.rr[s] = rr;
@@ -715,6 +716,7 @@ int cg_solve_fused(const Lattice& L, const T* Kn, const T* Tv, const Batch& bt, 
     w.sc.iters = iters;
     w.sc.relres = relres;
     w.sc.status = status;
+    w.sc.tols = o.tol_sys;
     const int64_t N = L.N;
     const int nset = (bt.nsys + bt.rhs_per_set - 1) / bt.rhs_per_set;
     const int vgrp = (bt.rhs_per_set + GRP - 1) / GRP;
@@ -810,7 +812,7 @@ int cg_solve_fused(const Lattice& L, const T* Kn, const T* Tv, const Batch& bt, 
         return cudaGetLastError();
     };
     GraphKey key;
-    key.ptr = {ws, Kn, Tv, mask, x, nullptr, nullptr, nullptr, nullptr, nullptr};
+    key.ptr = {ws, Kn, Tv, mask, x, o.tol_sys, nullptr, nullptr, nullptr, nullptr};
     key.val = {1, bt.nsys, bt.rhs_per_set, bt.nmask, L.nx, L.ny, L.nz, o.poll, o.check, o.maxit, precond ? 1 : 0,
                (long long)sizeof(T), 0, 0, 0, 0};
     double tolv = o.tol;

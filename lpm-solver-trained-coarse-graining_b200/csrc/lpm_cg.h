@@ -23,6 +23,7 @@ struct CgScalars {
     int* status;       // caller output
     int nblk;          // partial blocks per system of the vector kernels
     int* itp;          // device copy of the current iteration number, advanced by the p-update kernel
+    const double* tols;  // optional per-system tolerance (replaces the scalar tol)
 };
 
 // Optional CUDA-event timing of the operator launches of a solve (prof != nullptr).  prof[0] += ms and prof[1] += count

@@ -20,6 +20,7 @@ struct FcgScalars {
     int* status;
     int* itp;  // device copy of the current iteration number (1-based), advanced by the p-update kernel; lets a
                // captured block of iterations replay without host-side parameters
+    const double* tols;  // optional per-system tolerance (replaces the scalar tol)
 };
 
 // alpha step of system s, run by the last block of the operator epilogue once p.Ap is complete.

@@ -72,7 +72,7 @@ def solve_mf(lat, Kn, Tv, fixed_dofs, u_fixed, tol=1e-10, maxit=200000, precond=
                                                status=int(info.status[0]))
 
 
-def solve_mixed(lat, Kn, Tv, fixed_dofs, u_fixed, tol=1e-10, inner_tol=1e-5, maxit=200000, precond=False):
+def solve_mixed(lat, Kn, Tv, fixed_dofs, u_fixed, tol=1e-10, inner_tol=1e-3, maxit=200000, precond=False):
     """The same problem with FP32 (P)CG inside FP64 iterative refinement (FP64 true residual <= tol)."""
     lat, dl, Kt, Tt, free, b, ub = _prep(lat, Kn, Tv, fixed_dofs, u_fixed)
     x, info = core.ir(dl, Kt, Tt, b, free=free, tol=tol, inner_tol=inner_tol, maxit=maxit, precond=precond)

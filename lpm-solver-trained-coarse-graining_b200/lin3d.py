@@ -101,7 +101,7 @@ def solve_cg(lat, Kn, Tv, fixed, u_presc, tol=1e-4, maxit=200000):
     return _solve(lat, Kn, Tv, fixed, u_presc, tol, maxit, False)
 
 
-def solve_mixed(lat, Kn, Tv, fixed, u_presc, tol=1e-8, inner_tol=1e-5, maxit=20000):
+def solve_mixed(lat, Kn, Tv, fixed, u_presc, tol=1e-8, inner_tol=1e-3, maxit=20000):
     """The same problem with FP32 block-Jacobi PCG inside FP64 iterative refinement (FP64 true residual <= tol)."""
     lat = _as_lattice(lat)
     dl = lat.device_lattice

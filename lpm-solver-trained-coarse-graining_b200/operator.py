@@ -180,7 +180,7 @@ class LatticeOperator:
         info.raise_on_breakdown()
         return up + x, int(info.iters.max()), float(info.relres.max())
 
-    def solve_mixed(self, Kn, Tv, up, free, tol=1e-8, inner_tol=1e-5, maxit=20000):
+    def solve_mixed(self, Kn, Tv, up, free, tol=1e-8, inner_tol=1e-3, maxit=20000):
         """FP32 inner PCG with FP64 iterative refinement to |b - K x| <= tol |b| (FP64 true residual)."""
         with torch.no_grad():
             lead = torch.broadcast_shapes(up.shape[:-2], Kn.shape[:-2], free.shape[:-1])

@@ -84,7 +84,7 @@ def bucket_bytes(key, slots, rmax):
 class Bucket:
     """Persistent device batch of one lattice size."""
 
-    def __init__(self, key, slots, rmax, device, tol=1e-8, inner_tol=1e-5, maxit=50000, autotune=True):
+    def __init__(self, key, slots, rmax, device, tol=1e-8, inner_tol=1e-3, maxit=50000, autotune=True):
         self.key, self.S, self.R = key, int(slots), int(rmax)
         self.device = torch.device(device)
         self.tol, self.inner_tol, self.maxit = tol, inner_tol, maxit
@@ -215,7 +215,7 @@ class Server:
     whose bucket cannot be created yet (budget) waits in a pending list and is placed as soon as idle buckets are
     released.  `bucket_factory(key, slots, rmax)` builds buckets (the CUDA `Bucket` by default)."""
 
-    def __init__(self, device="cuda", budget_bytes=None, rmax=9, max_slots=8, tol=1e-8, inner_tol=1e-5,
+    def __init__(self, device="cuda", budget_bytes=None, rmax=9, max_slots=8, tol=1e-8, inner_tol=1e-3,
                  max_rounds=40, idle_release_s=0.5, bucket_factory=None, bytes_fn=bucket_bytes, rmax2d=None):
         self.device = torch.device(device)
         if budget_bytes is None:
