@@ -608,7 +608,8 @@ def main():
     nsys = B * Lc
 
     # tile tuning of the FP32 operator for this batch shape (the library records it for later launches)
-    core.autotune(dl, core.pack(Kn[:, 0], torch.float32), core.pack(Tv[:, 0], torch.float32), nsys, Lc)
+    tiles = core.autotune(dl, core.pack(Kn[:, 0], torch.float32), core.pack(Tv[:, 0], torch.float32), nsys, Lc,
+                          with_variant=True)
 
     def step(Kn, Tv, free, ups, prof=None):
         b = -core.kmv(dl, ups, Kn, Tv) * free[None, :, :, None]
@@ -754,7 +755,9 @@ def main():
             "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64", "data": "synthetic (seeded %s microstructures, shapes of the %d^3 config)"
             % ("spheres" if a.workload == "spheres48" else "prolate-ellipsoid", WORKLOADS[a.workload]["n"]),
-            "config": workload_config(a.workload, B, world), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "config": dict(workload_config(a.workload, B, world),
+                           operator_tiles={"zchunk": tiles[0], "variant": ["staged", "lean"][tiles[1]]}),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "clocks": clocks, "gpu_launches": gpu_launches, "all_converged": bool(ok),
             "inner_iters_mean": float(iters.mean()), "outer_steps": [i.outer for i in infos][:1],
             "fp64_gpu_cg": fp64_cg,

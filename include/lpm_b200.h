@@ -209,13 +209,17 @@ int lpm_kmv_vjp_f64(const lpm_lattice* lat, const double* u, const double* G, co
                     int32_t accumulate, void* scratch, size_t scratch_bytes, void* stream);
 
 /* ------------------------------------------------------------------------------------------------- tuning */
-/* Autotuner of the FP32 packed-coefficient SC operator used by the CG engines on full boxes: times the z-chunk
- * candidates (whole box, 1/2, 1/3, ... of the planes, at least 8 planes per chunk) on zero vectors of the batch's
- * shape, records the fastest for (nx, ny, nz, pairs) in a process-wide table that later launches of that shape use,
- * and returns it.  Kn/Tv: packed FP32 coefficients (LPM_LAYOUT_SOA) of the batch's sets.  scratch:
+/* Autotuner of the FP32 packed-coefficient SC operator used by the CG engines on full boxes: times its two variants
+ * (0: Tv and Kn staged in shared memory, one CTA per SM; 1: lean, two CTAs per SM) with each z-chunk candidate (whole
+ * box, 1/2, 1/3, ... of the planes, at least 8 planes per chunk) on zero vectors of the batch's shape, records the
+ * fastest for (nx, ny, nz, pairs) in a process-wide table that later launches of that shape use, and returns it
+ * (variant_out may be NULL).  Kn/Tv: packed FP32 coefficients (LPM_LAYOUT_SOA) of the batch's sets.  scratch:
  * lpm_kmv_scratch_bytes(lat, LPM_F32, nsys).  No reference counterpart (tuning of this library's tiles). */
 int lpm_autotune_kmv(const lpm_lattice* lat, const lpm_batch* batch, const float* Kn, const float* Tv, void* scratch,
-                     size_t scratch_bytes, int32_t* zchunk_out, void* stream);
+                     size_t scratch_bytes, int32_t* zchunk_out, int32_t* variant_out, void* stream);
+/* Pins the operator's tiles for a batch shape instead of timing them (reproducible runs, tests): z planes per CTA
+ * (1..nz, at most nz/8 chunks) and variant (0 or 1, as above).  No reference counterpart. */
+int lpm_tune_kmv_set(const lpm_lattice* lat, const lpm_batch* batch, int32_t zchunk, int32_t variant);
 
 /* ------------------------------------------------------------------------------------------------ geometry */
 /* Neighbour table of a (possibly masked) box, identical to LatticeGeom.nbr / Lattice2D.nbr

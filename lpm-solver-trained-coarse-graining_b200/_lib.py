@@ -72,7 +72,9 @@ _SIGS = {
                             _c_i32, _c_p, _c_sz, _c_p], ctypes.c_int),
     "lpm_kmv_vjp_f64": ([_P(Lattice), _c_p, _c_p, _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p, _c_p, _c_i32, _c_p,
                          _c_sz, _c_p], ctypes.c_int),
-    "lpm_autotune_kmv": ([_P(Lattice), _P(Batch), _c_p, _c_p, _c_p, _c_sz, _P(_c_i32), _c_p], ctypes.c_int),
+    "lpm_autotune_kmv": ([_P(Lattice), _P(Batch), _c_p, _c_p, _c_p, _c_sz, _P(_c_i32), _P(_c_i32), _c_p],
+                         ctypes.c_int),
+    "lpm_tune_kmv_set": ([_P(Lattice), _P(Batch), _c_i32, _c_i32], ctypes.c_int),
     "lpm_kmv_f64_static": ([_P(Lattice), _c_p, _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p], ctypes.c_int),
 }
 

@@ -129,16 +129,23 @@ def _scratch(nbytes, device):
     return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device=device)
 
 
-def autotune(dl, K32, T32, nsys, rhs_per_set):
-    """Time the z-chunk candidates of the pair-packed FP32 operator for this batch shape (packed FP32 coefficients
-    K32/T32 (nset, NN, N)); the fastest is recorded in the library for later launches and returned."""
+def autotune(dl, K32, T32, nsys, rhs_per_set, with_variant=False):
+    """Time the variants and z-chunk candidates of the pair-packed FP32 operator for this batch shape (packed FP32
+    coefficients K32/T32 (nset, NN, N)); the fastest is recorded in the library for later launches and returned
+    (zchunk, or (zchunk, variant) with with_variant)."""
     lib = L.load()
     scr = _scratch(lib.lpm_kmv_scratch_bytes(dl.ref, L.LPM_F32, int(nsys)), K32.device)
-    z = ctypes.c_int32(0)
+    z, v = ctypes.c_int32(0), ctypes.c_int32(0)
     b = _batch(nsys, rhs_per_set)
     L.check(lib.lpm_autotune_kmv(dl.ref, ctypes.byref(b), L.ptr(K32), L.ptr(T32), L.ptr(scr), scr.numel(),
-                                 ctypes.byref(z), L.stream_ptr(K32.device)), "lpm_autotune_kmv")
-    return int(z.value)
+                                 ctypes.byref(z), ctypes.byref(v), L.stream_ptr(K32.device)), "lpm_autotune_kmv")
+    return (int(z.value), int(v.value)) if with_variant else int(z.value)
+
+
+def tune_set(dl, nsys, rhs_per_set, zchunk, variant):
+    """Pin the pair-packed operator's z-chunk and variant for this batch shape (instead of autotune)."""
+    b = _batch(nsys, rhs_per_set)
+    L.check(L.load().lpm_tune_kmv_set(dl.ref, ctypes.byref(b), int(zchunk), int(variant)), "lpm_tune_kmv_set")
 
 
 def pack(K, dtype=_F32):

@@ -100,6 +100,7 @@ int kmv_impl(int dim, const lpm_lattice* lat, const T* u, const T* Kn, const T* 
             a.npp = npp;
             a.npair = nset * npp;
             a.zchunk = pair_zchunk(L.nx, L.ny, L.nz, a.npair);
+            a.variant = pair_variant(L.nx, L.ny, L.nz, a.npair);
             a.u = up;
             a.Kn = Kn;
             a.Tv = Tv;
@@ -399,7 +400,7 @@ int lpm_kmv_vjp_f64(const lpm_lattice* lat, const double* u, const double* G, co
 }
 
 int lpm_autotune_kmv(const lpm_lattice* lat, const lpm_batch* batch, const float* Kn, const float* Tv, void* scratch,
-                     size_t scratch_bytes, int32_t* zchunk_out, void* stream)
+                     size_t scratch_bytes, int32_t* zchunk_out, int32_t* variant_out, void* stream)
 {
     Lattice L;
     Batch bt;
@@ -429,31 +430,50 @@ int lpm_autotune_kmv(const lpm_lattice* lat, const lpm_batch* batch, const float
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (e == cudaSuccess) e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
-    int best = pair_zchunk_heuristic(L.nx, L.ny, L.nz, a.npair);
+    int best = pair_zchunk_heuristic(L.nx, L.ny, L.nz, a.npair), best_var = kPairDefaultVariant;
     float best_ms = 0.f;
     bool have = false;
-    for (int nzc = 1; e == cudaSuccess && nzc <= pair_zchunk_max_chunks(L.nz); ++nzc) {
-        const int zc = (L.nz + nzc - 1) / nzc;
-        if (nzc > 1 && (L.nz + zc - 1) / zc != nzc) continue;  // same chunking as a smaller count
-        a.zchunk = zc;
-        e = launch_sc_pair(a, false, st);  // warm-up
-        float ms = 0.f;
-        if (e == cudaSuccess) e = cudaEventRecord(e0, st);
-        for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = launch_sc_pair(a, false, st);
-        if (e == cudaSuccess) e = cudaEventRecord(e1, st);
-        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
-        if (e == cudaSuccess && (!have || ms < best_ms)) {
-            best_ms = ms;
-            best = zc;
-            have = true;
+    for (int var = 0; var < 2; ++var) {
+        for (int nzc = 1; e == cudaSuccess && nzc <= pair_zchunk_max_chunks(L.nz); ++nzc) {
+            const int zc = (L.nz + nzc - 1) / nzc;
+            if (nzc > 1 && (L.nz + zc - 1) / zc != nzc) continue;  // same chunking as a smaller count
+            a.zchunk = zc;
+            a.variant = var;
+            e = launch_sc_pair(a, false, st);  // warm-up
+            float ms = 0.f;
+            if (e == cudaSuccess) e = cudaEventRecord(e0, st);
+            for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = launch_sc_pair(a, false, st);
+            if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e == cudaSuccess && (!have || ms < best_ms)) {
+                best_ms = ms;
+                best = zc;
+                best_var = var;
+                have = true;
+            }
         }
     }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (e != cudaSuccess) return ret(e);
-    pair_zchunk_record(L.nx, L.ny, L.nz, a.npair, best);
+    pair_zchunk_record(L.nx, L.ny, L.nz, a.npair, best, best_var);
     *zchunk_out = best;
+    if (variant_out) *variant_out = best_var;
+    return LPM_OK;
+}
+
+int lpm_tune_kmv_set(const lpm_lattice* lat, const lpm_batch* batch, int32_t zchunk, int32_t variant)
+{
+    Lattice L;
+    Batch bt;
+    int rc = to_lattice(lat, L);
+    if (rc || (rc = to_batch(batch, bt))) return rc;
+    if (L.dim != 3 || zchunk < 1 || zchunk > L.nz || (L.nz + zchunk - 1) / zchunk > pair_zchunk_max_chunks(L.nz) ||
+        (variant != 0 && variant != 1))
+        return LPM_ERR_ARG;
+    const int npp = (bt.rhs_per_set + 1) / 2, nset = (bt.nsys + bt.rhs_per_set - 1) / bt.rhs_per_set;
+    pair_zchunk_record(L.nx, L.ny, L.nz, nset * npp, zchunk, variant);
     return LPM_OK;
 }
 

@@ -746,6 +746,7 @@ int cg_solve_fused(const Lattice& L, const T* Kn, const T* Tv, const Batch& bt, 
         a.npp = npp;
         a.npair = nset * npp;
         a.zchunk = pair_zchunk(L.nx, L.ny, L.nz, a.npair);
+        a.variant = pair_variant(L.nx, L.ny, L.nz, a.npair);
         a.Kn = reinterpret_cast<const float*>(Kn);
         a.Tv = reinterpret_cast<const float*>(Tv);
         a.act = w.sc.act;

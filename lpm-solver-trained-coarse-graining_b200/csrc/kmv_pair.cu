@@ -61,13 +61,19 @@ constexpr size_t PU_SLOT = (size_t)PUH * PUW * 4;
 constexpr size_t PTV_SLOT = (size_t)18 * PSH * PTVW * 4;
 constexpr size_t PKN_SLOT = (size_t)18 * PY * PKNW * 4;
 constexpr size_t PBA_SLOT = (size_t)2 * PSPL * 16;
+// Two variants share the kernel.  Staged (LEAN = false): Tv double-buffered and Kn staged by TMA, 187 KB, one CTA
+// per SM.  Lean (LEAN = true): one Tv slot refilled right after phase 1 has read it, Kn of the own sites read from
+// global memory in phase 1 and Tv of the own sites from global memory (L2) in phase 2, 101 KB and at most 128
+// registers: two CTAs (16 warps) per SM.
 constexpr size_t POFF_TV = 4 * PU_SLOT;
-constexpr size_t POFF_KN = POFF_TV + 2 * PTV_SLOT;
-constexpr size_t POFF_BA = POFF_KN + 2 * PKN_SLOT;
-constexpr size_t PBYTES = POFF_BA + 3 * PBA_SLOT;
+__host__ __device__ constexpr int tv_slots(bool lean) { return lean ? 1 : 2; }
+__host__ __device__ constexpr size_t off_kn(bool lean) { return POFF_TV + tv_slots(lean) * PTV_SLOT; }
+__host__ __device__ constexpr size_t off_ba(bool lean) { return off_kn(lean) + (lean ? 0 : 2 * PKN_SLOT); }
+__host__ __device__ constexpr size_t pair_bytes(bool lean) { return off_ba(lean) + 3 * PBA_SLOT; }
 static_assert(PU_SLOT % 128 == 0 && PTV_SLOT % 128 == 0 && PKN_SLOT % 128 == 0 && PBA_SLOT % 128 == 0,
               "TMA destinations must stay 128-byte aligned");
-static_assert(PBYTES <= 227 * 1024, "shared memory budget");
+static_assert(pair_bytes(false) <= 227 * 1024, "shared memory budget");
+static_assert(2 * (pair_bytes(true) + 2048) <= 228 * 1024, "two lean CTAs per SM");
 
 __host__ __device__ constexpr unsigned dir_bits(int axis, int sgn)
 {
@@ -104,8 +110,8 @@ __host__ __device__ constexpr SlotGeo slot_geo(int k)
 
 __device__ __forceinline__ pair_t ld2(const float* p) { return *reinterpret_cast<const pair_t*>(p); }
 
-template <bool EPI>
-__global__ void __launch_bounds__(PNT, 1)
+template <bool EPI, bool LEAN>
+__global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
     k_sc_pair(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ CUtensorMap tm_tv,
               const __grid_constant__ CUtensorMap tm_kn, PairArgs P)
 {
@@ -117,8 +123,8 @@ __global__ void __launch_bounds__(PNT, 1)
 
     float* su = reinterpret_cast<float*>(smem);
     float* stv = reinterpret_cast<float*>(smem + POFF_TV);
-    float* skn = reinterpret_cast<float*>(smem + POFF_KN);
-    float4* sba = reinterpret_cast<float4*>(smem + POFF_BA);
+    float* skn = reinterpret_cast<float*>(smem + off_kn(LEAN));
+    float4* sba = reinterpret_cast<float4*>(smem + off_ba(LEAN));
 
     const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31;
     const int tx = lane & 15, ty = ((wid >> 1) << 2) + (wid & 1) + ((lane >> 4) << 1);
@@ -177,16 +183,18 @@ __global__ void __launch_bounds__(PNT, 1)
         tma_load4(su + (size_t)(n & 3) * (PU_SLOT / 4), &tm_u, bar, 6 * (x0 - 2), y0 - 2, p, pr);
         note(n & 3, (n >> 2) & 1);
     };
+    // Tv fill n: slot n % tv_slots, barrier 4 + slot, parity (n / tv_slots) & 1
+    constexpr int NTV = tv_slots(LEAN);
     auto issue_tv = [&](int p) {
         const int n = p - tv0;
-        uint64_t* bar = &bars[4 + (n & 1)];
+        uint64_t* bar = &bars[4 + n % NTV];
         if (p < 0 || p >= nz) {
             mbar_arrive(bar);
             return;
         }
         mbar_expect_arrive(bar, (uint32_t)PTV_SLOT);
-        tma_load4(stv + (size_t)(n & 1) * (PTV_SLOT / 4), &tm_tv, bar, x0 - 4, y0 - 1, p, 18 * set);
-        note(4 + (n & 1), (n >> 1) & 1);
+        tma_load4(stv + (size_t)(n % NTV) * (PTV_SLOT / 4), &tm_tv, bar, x0 - 4, y0 - 1, p, 18 * set);
+        note(4 + n % NTV, (n / NTV) & 1);
     };
     auto issue_kn = [&](int p) {
         const int n = p - kn0;
@@ -211,12 +219,13 @@ __global__ void __launch_bounds__(PNT, 1)
     };
     auto wait_planes = [&](int pu, int ptv, int pkn) {
         if (pu >= 0 && pu < nz && pu >= u0) wait_fill((pu - u0) & 3, ((pu - u0) >> 2) & 1);
-        if (ptv >= 0 && ptv < nz && ptv >= tv0) wait_fill(4 + ((ptv - tv0) & 1), ((ptv - tv0) >> 1) & 1);
-        if (pkn >= 0 && pkn < nz && pkn >= kn0 && pkn < zend) wait_fill(6 + ((pkn - kn0) & 1), ((pkn - kn0) >> 1) & 1);
+        if (ptv >= 0 && ptv < nz && ptv >= tv0) wait_fill(4 + (ptv - tv0) % NTV, ((ptv - tv0) / NTV) & 1);
+        if (!LEAN && pkn >= 0 && pkn < nz && pkn >= kn0 && pkn < zend)
+            wait_fill(6 + ((pkn - kn0) & 1), ((pkn - kn0) >> 1) & 1);
     };
 
     auto u_slot = [&](int p) { return su + (size_t)((p - u0) & 3) * (PU_SLOT / 4); };
-    auto tv_slot = [&](int p) { return stv + (size_t)((p - tv0) & 1) * (PTV_SLOT / 4); };
+    auto tv_slot = [&](int p) { return stv + (size_t)((p - tv0) % NTV) * (PTV_SLOT / 4); };
     auto kn_slot = [&](int p) { return skn + (size_t)((p - kn0) & 1) * (PKN_SLOT / 4); };
     auto ba_slot = [&](int p) { return sba + (size_t)(((p % 3) + 3) % 3) * (PBA_SLOT / 16); };
     auto zero_ba = [&](int p) {
@@ -235,7 +244,7 @@ __global__ void __launch_bounds__(PNT, 1)
     for (int k = 0; k < 18; ++k) tv_next[k] = 0.f;
 
     auto site = [&](auto own_tag, auto mask_tag, int qx, int qy, int zp, unsigned vm, const float* tvs,
-                    const float* kns) {
+                    const float* kns, int64_t kst) {
         constexpr bool OWN = decltype(own_tag)::value;
         constexpr bool MASKED = decltype(mask_tag)::value;
         const float* pm = u_slot(zp - 1);
@@ -266,7 +275,7 @@ __global__ void __launch_bounds__(PNT, 1)
                     Tm0 = fma2(dup(tv), t, Tm0);
                 }
                 if constexpr (OWN) {
-                    const float kn = kns[k * PY * PKNW];
+                    const float kn = LEAN ? __ldg(kns + k * kst) : kns[k * kst];
                     fm[g.a] = fma2(dup(2.f * kn), t, fm[g.a]);  // f_a -= 2 Kn t
                     if (vb) {
                         s0[g.a] -= (float)g.sa;
@@ -286,7 +295,7 @@ __global__ void __launch_bounds__(PNT, 1)
                     Tm1 = fma2(dup(tv), t, Tm1);
                 }
                 if constexpr (OWN) {
-                    const float kn = kns[k * PY * PKNW];
+                    const float kn = LEAN ? __ldg(kns + k * kst) : kns[k * kst];
                     const pair_t kn2 = dup(kn);
                     fm[g.a] = fma2(kn2, t, fm[g.a]);  // f_a -= sa Kn d' = Kn t
                     if (g.sa == g.sb)
@@ -301,7 +310,7 @@ __global__ void __launch_bounds__(PNT, 1)
                     }
                 }
             }
-            if constexpr (OWN) tv_next[k] = tv;
+            if constexpr (OWN && !LEAN) tv_next[k] = tv;
         }
         // B0 = S0/2, A0 = TS0/2; shell 1 pre-scaled by 1/sqrt2: B1w = S1'/4, A1w = TS1'/4
         const pair_t h = dup(0.5f), q = dup(0.25f);
@@ -382,16 +391,24 @@ __global__ void __launch_bounds__(PNT, 1)
         if (own_xy) {
             const float* tvs = tv_slot(zp) + (ty + 1) * PTVW + tx + 4;
             if (own) {
-                const float* kns = kn_slot(zp) + ty * PKNW + tx;
+                const float* kns;
+                int64_t kst;
+                if constexpr (LEAN) {
+                    kns = P.Kn + (int64_t)18 * set * P.N + ((int64_t)zp * ny + gy) * nx + gx;
+                    kst = P.N;
+                } else {
+                    kns = kn_slot(zp) + ty * PKNW + tx;
+                    kst = PY * PKNW;
+                }
                 if (uni)
-                    site(T_{}, F_{}, tx + 1, ty + 1, zp, vm, tvs, kns);
+                    site(T_{}, F_{}, tx + 1, ty + 1, zp, vm, tvs, kns, kst);
                 else
-                    site(T_{}, T_{}, tx + 1, ty + 1, zp, vm, tvs, kns);
+                    site(T_{}, T_{}, tx + 1, ty + 1, zp, vm, tvs, kns, kst);
             } else {
                 if (uni)
-                    site(F_{}, F_{}, tx + 1, ty + 1, zp, vm, tvs, nullptr);
+                    site(F_{}, F_{}, tx + 1, ty + 1, zp, vm, tvs, nullptr, 0);
                 else
-                    site(F_{}, T_{}, tx + 1, ty + 1, zp, vm, tvs, nullptr);
+                    site(F_{}, T_{}, tx + 1, ty + 1, zp, vm, tvs, nullptr, 0);
             }
         }
         const unsigned rvm = ring_mxy & zm;
@@ -399,9 +416,9 @@ __global__ void __launch_bounds__(PNT, 1)
         if (ring_in) {
             const float* tvs = tv_slot(zp) + rqy * PTVW + rqx + 3;
             if (runi)
-                site(F_{}, F_{}, rqx, rqy, zp, rvm, tvs, nullptr);
+                site(F_{}, F_{}, rqx, rqy, zp, rvm, tvs, nullptr, 0);
             else
-                site(F_{}, T_{}, rqx, rqy, zp, rvm, tvs, nullptr);
+                site(F_{}, T_{}, rqx, rqy, zp, rvm, tvs, nullptr, 0);
         }
     };
 
@@ -417,12 +434,14 @@ __global__ void __launch_bounds__(PNT, 1)
         const float4* bp = ba_slot(z + 1);
         const int c0 = (ty + 1) * PSW + (tx + 1);
         pair_t f[3] = {own_cur[0], own_cur[1], own_cur[2]};
+        const float* tvg = P.Tv + (int64_t)18 * set * P.N + i;
 #pragma unroll
         for (int k = 0; k < 18; ++k) {
             const SlotGeo g = slot_geo(k);
             const float4* pl = sc_dz(k) < 0 ? bm : (sc_dz(k) > 0 ? bp : b0);
             const float4 v = pl[sc_shell(k) * PSPL + c0 + sc_dy(k) * PSW + sc_dx(k)];
-            const pair_t gw = fma2(dup(tv_cur[k]), pk(v.x, v.y), pk(v.z, v.w));  // zero for bonds leaving the box
+            const float tvk = LEAN ? __ldg(tvg + (int64_t)k * P.N) : tv_cur[k];
+            const pair_t gw = fma2(dup(tvk), pk(v.x, v.y), pk(v.z, v.w));  // zero for bonds leaving the box
             f[g.a] = g.sa > 0 ? sub2(f[g.a], gw) : add2(f[g.a], gw);
             if (sc_shell(k) == 1) f[g.b] = g.sb > 0 ? sub2(f[g.b], gw) : add2(f[g.b], gw);
         }
@@ -438,14 +457,18 @@ __global__ void __launch_bounds__(PNT, 1)
         }
     };
 
+    // Tv fills: staged variant a plane ahead at the start of each step; lean variant right after the block barrier
+    // that ends the phase 1 reading its single slot.
     bool ok = true;
     if (any_on) {
         if (tid == 0) {
             for (int p = zbeg - 2; p <= zbeg + 1; ++p) issue_u(p);
             issue_tv(zbeg - 1);
-            issue_tv(zbeg);
-            issue_kn(zbeg);
-            if (zbeg + 1 < zend) issue_kn(zbeg + 1);
+            if constexpr (!LEAN) {
+                issue_tv(zbeg);
+                issue_kn(zbeg);
+                if (zbeg + 1 < zend) issue_kn(zbeg + 1);
+            }
         }
         wait_planes(zbeg - 2, -1, -1);
         wait_planes(zbeg - 1, zbeg - 1, -1);
@@ -457,24 +480,35 @@ __global__ void __launch_bounds__(PNT, 1)
             if (tid == 0) {
                 fence_proxy_async();
                 if (zbeg + 2 <= zend + 1) issue_u(zbeg + 2);
-                if (zbeg + 1 <= zend) issue_tv(zbeg + 1);
+                if constexpr (LEAN)
+                    issue_tv(zbeg);
+                else if (zbeg + 1 <= zend)
+                    issue_tv(zbeg + 1);
             }
             wait_planes(zbeg + 1, zbeg, zbeg);
             phase1(zbeg, true);
             __syncthreads();
             ok = !abort_flag;
+            if (LEAN && ok && tid == 0) {
+                fence_proxy_async();
+                if (zbeg + 1 <= zend) issue_tv(zbeg + 1);
+            }
         }
         if (ok) {
             for (int z = zbeg; z < zend; ++z) {
 #pragma unroll
                 for (int a = 0; a < 3; ++a) own_cur[a] = own_next[a];
+                if constexpr (!LEAN) {
 #pragma unroll
-                for (int k = 0; k < 18; ++k) tv_cur[k] = tv_next[k];
+                    for (int k = 0; k < 18; ++k) tv_cur[k] = tv_next[k];
+                }
                 if (tid == 0) {
                     fence_proxy_async();
                     if (z + 3 <= zend + 1) issue_u(z + 3);
-                    if (z + 2 <= zend) issue_tv(z + 2);
-                    if (z + 2 < zend) issue_kn(z + 2);
+                    if constexpr (!LEAN) {
+                        if (z + 2 <= zend) issue_tv(z + 2);
+                        if (z + 2 < zend) issue_kn(z + 2);
+                    }
                 }
                 wait_planes(z + 2, z + 1, z + 1);
                 phase1(z + 1, z + 1 < zend);
@@ -482,6 +516,10 @@ __global__ void __launch_bounds__(PNT, 1)
                 if (abort_flag) {
                     ok = false;
                     break;
+                }
+                if (LEAN && tid == 0) {  // the Tv slot is free: fill it with the plane of the next phase 1
+                    fence_proxy_async();
+                    if (z + 2 <= zend) issue_tv(z + 2);
                 }
                 phase2(z);
                 __syncthreads();
@@ -521,7 +559,7 @@ __global__ void __launch_bounds__(PNT, 1)
     }
 }
 
-template <bool EPI>
+template <bool EPI, bool LEAN>
 cudaError_t launch_pair(const PairArgs& a, cudaStream_t st)
 {
     const int nset = (a.nsys + a.rhs_per_set - 1) / a.rhs_per_set;
@@ -539,14 +577,18 @@ cudaError_t launch_pair(const PairArgs& a, cudaStream_t st)
         const uint32_t btv[4] = {(uint32_t)PTVW, (uint32_t)PSH, 1, 18};
         const uint32_t bkn[4] = {(uint32_t)PKNW, (uint32_t)PY, 1, 18};
         if (!make_tensor_map4(&mtv, 4, a.Tv, dims, str, btv)) return cudaErrorInvalidValue;
-        if (!make_tensor_map4(&mkn, 4, a.Kn, dims, str, bkn)) return cudaErrorInvalidValue;
+        if (LEAN)
+            mkn = mtv;  // not read by the lean variant
+        else if (!make_tensor_map4(&mkn, 4, a.Kn, dims, str, bkn))
+            return cudaErrorInvalidValue;
     }
     static unsigned long long attr_set = 0;
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if (!((attr_set >> dev) & 1ull)) {
-        cudaError_t e = cudaFuncSetAttribute(k_sc_pair<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PBYTES);
+        cudaError_t e = cudaFuncSetAttribute(k_sc_pair<EPI, LEAN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)pair_bytes(LEAN));
         if (e != cudaSuccess) return e;
         attr_set |= 1ull << dev;
     }
@@ -556,7 +598,7 @@ cudaError_t launch_pair(const PairArgs& a, cudaStream_t st)
         PairArgs b = a;
         b.pair0 = g0;
         const int ng = a.npair - g0 < 65535 ? a.npair - g0 : 65535;
-        k_sc_pair<EPI><<<dim3(ntile * nzc, ng), PNT, PBYTES, st>>>(mu, mtv, mkn, b);
+        k_sc_pair<EPI, LEAN><<<dim3(ntile * nzc, ng), PNT, pair_bytes(LEAN), st>>>(mu, mtv, mkn, b);
     }
     return cudaGetLastError();
 }
@@ -622,7 +664,7 @@ bool pair_supported(int nx) { return nx % 4 == 0 && tma_supported(nx, 4); }
 // for two CTAs per SM of work with at least 8 planes each.
 namespace {
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int>, int> g_tuned;
+std::map<std::tuple<int, int, int, int>, std::pair<int, int>> g_tuned;  // shape -> (zchunk, variant)
 }  // namespace
 
 int pair_zchunk_heuristic(int nx, int ny, int nz, int npair)
@@ -638,15 +680,22 @@ int pair_zchunk(int nx, int ny, int nz, int npair)
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
         auto it = g_tuned.find(std::make_tuple(nx, ny, nz, npair));
-        if (it != g_tuned.end()) return it->second;
+        if (it != g_tuned.end()) return it->second.first;
     }
     return pair_zchunk_heuristic(nx, ny, nz, npair);
 }
 
-void pair_zchunk_record(int nx, int ny, int nz, int npair, int zchunk)
+int pair_variant(int nx, int ny, int nz, int npair)
 {
     std::lock_guard<std::mutex> g(g_tune_mu);
-    g_tuned[std::make_tuple(nx, ny, nz, npair)] = zchunk;
+    auto it = g_tuned.find(std::make_tuple(nx, ny, nz, npair));
+    return it != g_tuned.end() ? it->second.second : kPairDefaultVariant;
+}
+
+void pair_zchunk_record(int nx, int ny, int nz, int npair, int zchunk, int variant)
+{
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tuned[std::make_tuple(nx, ny, nz, npair)] = std::make_pair(zchunk, variant);
 }
 
 int pair_zchunk_max_chunks(int nz) { return nz / 8 > 1 ? nz / 8 : 1; }
@@ -656,7 +705,9 @@ int pair_dot_blocks_max(int nx, int ny, int nz) { return ((nx + PX - 1) / PX) * 
 cudaError_t launch_sc_pair(const PairArgs& a, bool epi, cudaStream_t st)
 {
     if (a.npair < 1 || a.npp < 1 || a.zchunk < 1) return cudaErrorInvalidValue;
-    return epi ? launch_pair<true>(a, st) : launch_pair<false>(a, st);
+    if (a.variant)
+        return epi ? launch_pair<true, true>(a, st) : launch_pair<false, true>(a, st);
+    return epi ? launch_pair<true, false>(a, st) : launch_pair<false, false>(a, st);
 }
 
 }  // namespace lpm

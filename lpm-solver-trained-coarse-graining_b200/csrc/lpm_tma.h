@@ -53,6 +53,7 @@ struct PairArgs {
     int npair;   // pairs in the batch = nset * npp
     int pair0;   // first pair of this launch (grid.y chunking)
     int zchunk;  // z planes per CTA
+    int variant; // 0: staged (Tv, Kn through shared memory, one CTA per SM); 1: lean (two CTAs per SM)
     const float* u;   // pair layout
     const float* Kn;  // (nset, 18, N)
     const float* Tv;
@@ -67,9 +68,11 @@ struct PairArgs {
 };
 
 bool pair_supported(int nx);
+constexpr int kPairDefaultVariant = 0;
 int pair_zchunk(int nx, int ny, int nz, int npair);            // autotuned value if recorded, else heuristic
+int pair_variant(int nx, int ny, int nz, int npair);           // autotuned variant if recorded, else the default
 int pair_zchunk_heuristic(int nx, int ny, int nz, int npair);
-void pair_zchunk_record(int nx, int ny, int nz, int npair, int zchunk);
+void pair_zchunk_record(int nx, int ny, int nz, int npair, int zchunk, int variant);
 int pair_zchunk_max_chunks(int nz);                               // z chunks allowed (>= 8 planes each)
 int pair_dot_blocks_max(int nx, int ny, int nz);
 cudaError_t launch_sc_pair(const PairArgs& a, bool epi, cudaStream_t st);
