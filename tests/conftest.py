@@ -40,3 +40,8 @@ def relmax(a, b):
     a = np.asarray(a, float)
     b = np.asarray(b, float)
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.fixture(scope="session")
+def gamg():
+    return _load("golden_amg.npz")

@@ -363,7 +363,76 @@ def part_grad():
     print("golden_grad.npz:", len(out), "arrays")
 
 
-PARTS = {"sc": part_sc, "sq": part_sq, "grad": part_grad}
+def part_amg():
+    """Aggregation AMG of timing/t3d/amg3d.py with the settings of timing/t3d/problems.py:19 (AMG_CFG) on a 14^3
+    spheres specimen, one hierarchy per BC set (ring, tb, lr) as problems.solve_amg; coarse_max = 100 so that the
+    hierarchy has a W-cycled level 1 above a dense level 2.  Plus the iteration count of the 48^3 spheres workload."""
+    _env()
+    sys.path.insert(0, os.path.join(REF, "coarse3d"))
+    sys.path.insert(0, os.path.join(REF, "timing", "t3d"))
+    _stub("common")
+    import numpy as np
+    import geom3d as G
+    import lin3d as L3
+    import micro3d
+    import amg3d as A3
+
+    out = {}
+
+    def specimen(n, seed, r):
+        ph, _ = micro3d.spheres(n, n, n, 0.25, r, np.random.default_rng(seed), rjit=0.0)
+        lat = L3.Lattice3D(n, n, n, 1.0)
+        C = G.iso_C(np.where(ph == 1, 10.0, 1.0), 0.2)
+        Kn, Tv = G.bond_params_two_end_mean(lat, G.sc_params_from_C(C, 0.5))
+        return lat, Kn, Tv
+
+    n = 14
+    lat, Kn, Tv = specimen(n, 3, 2.5)
+    out.update(a_n=n, a_Kn=Kn, a_Tv=Tv)
+    D = lat.block_diag(Kn, Tv)
+    rho0 = None
+    brng = np.random.default_rng(21)
+    for name, ld in (("ring", "k_xx"), ("tb", "tb_tz"), ("lr", "lr_tx")):
+        fixed, up, _ = G.prescribed(ld, lat.x, lat.ijk, (n,) * 3, 1)
+        geo = A3.AMGGeom(lat, ~fixed, agg=3, coarse_max=100)
+        M = L3.k_block_jacobi(D, ~fixed)
+        h = A3.AMG3D(geo, Kn, Tv, nu=1, gamma=2, power_its=5, Minv0=M, rho0=rho0)
+        rho0 = h.rho0
+        pre = "a_%s_" % name
+        out[pre + "g"] = np.array([geo.l0["g"]] + [L["gc"] for L in geo.levels], np.int64)
+        out[pre + "P"] = geo.l0["P"]
+        out[pre + "agg_of"] = geo.l0["agg_of"]
+        out[pre + "Q1"] = geo.levels[0]["Q"]
+        out[pre + "rho"] = np.array([h.rho0] + list(h.rho))
+        out[pre + "A1"] = h.A[0].astype(np.float32)
+        out[pre + "A2"] = h.A[1]
+        r = brng.standard_normal((lat.N, 3))
+        A3._mask(r, ~fixed)
+        out[pre + "vin"] = r
+        out[pre + "vout"] = h.vcycle(r.copy())
+        b = -L3.k_apply(up, lat.nbr, lat.ndir, Kn, Tv)
+        A3._mask(b, ~fixed)
+        x, it, rel = h.pcg(b, 1e-8)
+        out[pre + "pcg_x"] = up + x
+        out[pre + "pcg_it"] = it
+        out[pre + "pcg_rel"] = rel
+    # 48^3 spheres (r = 4, seed 0, the bench specimen), ring BCs, load k_xx
+    n = 48
+    lat, Kn, Tv = specimen(n, 0, 4.0)
+    fixed, up, _ = G.prescribed("k_xx", lat.x, lat.ijk, (n,) * 3, 1)
+    geo = A3.AMGGeom(lat, ~fixed, agg=3, coarse_max=1000)
+    h = A3.AMG3D(geo, Kn, Tv, nu=1, gamma=2, power_its=5,
+                 Minv0=L3.k_block_jacobi(lat.block_diag(Kn, Tv), ~fixed))
+    b = -L3.k_apply(up, lat.nbr, lat.ndir, Kn, Tv)
+    A3._mask(b, ~fixed)
+    x, it, rel = h.pcg(b, 1e-8)
+    out.update(a48_it=it, a48_rel=rel, a48_rho=np.array([h.rho0] + list(h.rho)),
+               a48_g=np.array([geo.l0["g"]] + [L["gc"] for L in geo.levels], np.int64))
+    np.savez_compressed(os.path.join(HERE, "golden_amg.npz"), **out)
+    print("golden_amg.npz:", len(out), "arrays")
+
+
+PARTS = {"sc": part_sc, "sq": part_sq, "grad": part_grad, "amg": part_amg}
 
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] in PARTS:
