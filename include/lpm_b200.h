@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define LPM_ABI_VERSION 2
+#define LPM_ABI_VERSION 3
 
 /* return codes */
 #define LPM_OK 0
@@ -207,6 +207,67 @@ int lpm_stress_vjp_f64(const lpm_lattice* lat, const double* u, const double* Gs
 int lpm_kmv_vjp_f64(const lpm_lattice* lat, const double* u, const double* G, const double* Kn, const double* Tv,
                     int32_t coef_layout, const lpm_batch* batch, double* du, double* gKn, double* gTv,
                     int32_t accumulate, void* scratch, size_t scratch_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------------- AMG preconditioner */
+/* Aggregation AMG of timing/t3d/amg3d.py (AMGGeom, AMG3D) for the SC operator on full boxes (FP32 coefficients,
+ * packed LPM_LAYOUT_SOA; nx a multiple of 4), used as the preconditioner of an FP32 PCG and, through lpm_ir_amg, of
+ * the mixed-precision solve.  Defaults (lpm_amg_default_opts) are the settings of timing/t3d/problems.py:19
+ * (AMG_CFG): agg 3, coarse_max 1000, nu 1, W-cycles (gamma 2) below the finest level, 5 power iterations. */
+typedef struct lpm_amg_opts {
+    int32_t agg;          /* aggregate edge in sites (>= 3); the remainder joins the last chunk (rule "merge") */
+    int32_t coarse_max;   /* the coarsest level is solved densely once 6 * nodes <= coarse_max */
+    int32_t max_levels;   /* limit on coarse levels below level 1 (<= 8) */
+    int32_t nu;           /* smoothing sweeps on the finest level before and after the coarse correction (1) */
+    int32_t nu_c;         /* sweeps on the coarse levels (>= 1) */
+    int32_t gamma;        /* cycle index on levels >= w_from (1 = V, 2 = W) */
+    int32_t w_from;       /* first level with gamma cycles (levels counted from 1 below the finest) */
+    int32_t power_its;    /* power iterations for rho(D^-1 A) of every smoothed level */
+    double omega;         /* smoother weight omega / rho */
+    int32_t rho0_per_box; /* 0: rho of the finest level from the first box of a set, reused for its other boxes
+                             (timing/t3d/problems.py:126-128); 1: one estimate per box */
+    int32_t reserved;
+} lpm_amg_opts;
+
+typedef struct lpm_amg lpm_amg; /* opaque: geometry, per-set hierarchies and solver state of one batch shape */
+
+void lpm_amg_default_opts(lpm_amg_opts* opts);
+/* Geometry of the hierarchy for a batch (host work and one device allocation, freed by lpm_amg_destroy).  boxes:
+ * (nbox, 6) int32 free boxes lo x, y, z, hi x, y, z (inclusive site indices); box_of_mask (batch->nmask): the box of
+ * DOF mask m -- system s is free exactly on the particles of box box_of_mask[s % nmask] (all three DOFs), as for
+ * every load case of geom3d.prescribed.  One hierarchy per (coefficient set, box), as timing/t3d/problems.py:112-132
+ * builds one per BC set.  Replaces amg3d.AMGGeom (timing/t3d/amg3d.py:440-497). */
+int lpm_amg_create(const lpm_lattice* lat, const lpm_batch* batch, const int32_t* boxes, int32_t nbox,
+                   const int32_t* box_of_mask, const lpm_amg_opts* opts, lpm_amg** out);
+void lpm_amg_destroy(lpm_amg* amg);
+/* Numeric setup for the batch's coefficient sets (replaces amg3d.AMG3D.__init__, timing/t3d/amg3d.py:522-570):
+ * Kn32/Tv32 packed FP32 (nset, 18, n), kept by reference until the next setup; Minv32 the FP32 block-Jacobi inverse
+ * (nset, n, 3, 3) of lpm_block_jacobi_f32.  Synchronises the stream. */
+int lpm_amg_setup(lpm_amg* amg, const float* Kn32, const float* Tv32, const float* Minv32, void* stream);
+/* rho of the finest level per (set, box estimate): (nset * nb) values, nb = nbox with rho0_per_box else 1.  set_rho0
+ * replaces the estimates (amg3d.AMG3D's rho0 argument: a value shared by the BC sets of one specimen). */
+int lpm_amg_get_rho0(const lpm_amg* amg, double* rho0_host);
+int lpm_amg_set_rho0(lpm_amg* amg, const double* rho0_host, void* stream);
+/* One preconditioner application z = B r for every system (amg3d.AMG3D.vcycle, timing/t3d/amg3d.py:609-637);
+ * r, z: (nsys, n, 3) FP32, r is masked to the free box first. */
+int lpm_amg_apply(lpm_amg* amg, const float* r, float* z, void* stream);
+/* FP32 AMG-preconditioned CG from x = 0 (amg3d.AMG3D.pcg, timing/t3d/amg3d.py:639-668, batched with freezing):
+ * b, x (nsys, n, 3) FP32; opts, outputs and stop rule as lpm_cg_batched_*. */
+int lpm_amg_pcg_f32(lpm_amg* amg, const float* b, float* x, const lpm_cg_opts* opts, int32_t* iters, double* relres,
+                    int32_t* status, void* stream);
+/* Mixed-precision solve as lpm_ir_batched with the FP32 AMG-PCG as the inner solver (the handle's coefficients and
+ * batch); workspace: lpm_ir_workspace_bytes(lat, batch, 0). */
+int lpm_ir_amg(const lpm_lattice* lat, const double* Kn64, const double* Tv64, int32_t coef_layout64, lpm_amg* amg,
+               const lpm_batch* batch, const uint8_t* mask, const double* b, double* x, const lpm_ir_opts* opts,
+               void* workspace, size_t workspace_bytes, int32_t* iters, double* relres, int32_t* status,
+               int32_t* outer_steps, void* stream);
+/* Levels of a box (nlev: stencil levels below the finest, the last one dense), their grids (nlev, 3) and the
+ * handle's device bytes. */
+int lpm_amg_info(const lpm_amg* amg, int32_t box, int32_t* nlev, int32_t* grids, int64_t* device_bytes);
+/* Level `level` (1..nlev) of the hierarchy (set, box) after setup, to host memory: A_host (nodes, 27, 6, 6) FP32
+ * stencil rows as amg3d.AMG3D.A, rho_host its rho (0 for the dense level), fw_host (nsys) the finest-level smoother
+ * weights omega / rho0; any output may be NULL.  Synchronises the device. */
+int lpm_amg_get_level(const lpm_amg* amg, int32_t box, int32_t set, int32_t level, float* A_host, double* rho_host,
+                      float* fw_host);
 
 /* ------------------------------------------------------------------------------------------------- tuning */
 /* Autotuner of the FP32 packed-coefficient SC operator used by the CG engines on full boxes: times its two variants

@@ -37,6 +37,12 @@ class IrOpts(ctypes.Structure):
                 ("poll", _c_i32), ("prof", _P(_c_d))]
 
 
+class AmgOpts(ctypes.Structure):
+    _fields_ = [("agg", _c_i32), ("coarse_max", _c_i32), ("max_levels", _c_i32), ("nu", _c_i32), ("nu_c", _c_i32),
+                ("gamma", _c_i32), ("w_from", _c_i32), ("power_its", _c_i32), ("omega", _c_d),
+                ("rho0_per_box", _c_i32), ("reserved", _c_i32)]
+
+
 _SIGS = {
     "lpm_abi_version": ([], ctypes.c_int),
     "lpm_status_string": ([ctypes.c_int], ctypes.c_char_p),
@@ -76,6 +82,18 @@ _SIGS = {
                          ctypes.c_int),
     "lpm_tune_kmv_set": ([_P(Lattice), _P(Batch), _c_i32, _c_i32], ctypes.c_int),
     "lpm_kmv_f64_static": ([_P(Lattice), _c_p, _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p], ctypes.c_int),
+    "lpm_amg_default_opts": ([_P(AmgOpts)], None),
+    "lpm_amg_create": ([_P(Lattice), _P(Batch), _c_p, _c_i32, _c_p, _P(AmgOpts), _P(_c_p)], ctypes.c_int),
+    "lpm_amg_destroy": ([_c_p], None),
+    "lpm_amg_setup": ([_c_p, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
+    "lpm_amg_get_rho0": ([_c_p, _c_p], ctypes.c_int),
+    "lpm_amg_set_rho0": ([_c_p, _c_p, _c_p], ctypes.c_int),
+    "lpm_amg_apply": ([_c_p, _c_p, _c_p, _c_p], ctypes.c_int),
+    "lpm_amg_pcg_f32": ([_c_p, _c_p, _c_p, _P(CgOpts), _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
+    "lpm_ir_amg": ([_P(Lattice), _c_p, _c_p, _c_i32, _c_p, _P(Batch), _c_p, _c_p, _c_p, _P(IrOpts), _c_p, _c_sz,
+                    _c_p, _c_p, _c_p, _P(_c_i32), _c_p], ctypes.c_int),
+    "lpm_amg_info": ([_c_p, _c_i32, _P(_c_i32), _c_p, _P(_c_i64)], ctypes.c_int),
+    "lpm_amg_get_level": ([_c_p, _c_i32, _c_i32, _c_i32, _c_p, _c_p, _c_p], ctypes.c_int),
 }
 
 _lib = None

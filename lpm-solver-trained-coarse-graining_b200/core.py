@@ -286,6 +286,9 @@ def ir(dl, Kn64, Tv64, b, x=None, free=None, tol=1e-8, inner_tol=1e-3, maxit=200
     m, nmask = dof_masks(free, dl, lead)
     xf = torch.zeros_like(bf) if x is None else _flat_vec(x, dl).to(_F64).clone()
     lib = L.load()
+    lay64 = L.LAYOUT_REF
+    if dl.dim == 3 and dl.nbr is None:      # full SC box: the FP64 residuals run on the TMA operator (packed SoA)
+        Kc, Tc, lay64 = pack(Kc, _F64), pack(Tc, _F64), L.LAYOUT_SOA
     b_ = _batch(nsys, rps, nmask)
     ws = _scratch(lib.lpm_ir_workspace_bytes(dl.ref, ctypes.byref(b_), int(M32 is not None)), bf.device)
     it = torch.zeros(nsys, dtype=torch.int32, device=bf.device)
@@ -294,7 +297,7 @@ def ir(dl, Kn64, Tv64, b, x=None, free=None, tol=1e-8, inner_tol=1e-3, maxit=200
     outer = ctypes.c_int32(0)
     opts = L.IrOpts(float(tol), float(inner_tol), int(maxit), int(max_outer), int(check), int(poll),
                     _prof_ptr(prof))
-    L.check(lib.lpm_ir_batched(dl.ref, L.ptr(Kc), L.ptr(Tc), L.LAYOUT_REF, L.ptr(K32), L.ptr(T32), L.ptr(M32),
+    L.check(lib.lpm_ir_batched(dl.ref, L.ptr(Kc), L.ptr(Tc), lay64, L.ptr(K32), L.ptr(T32), L.ptr(M32),
                                ctypes.byref(b_), L.ptr(m), L.ptr(bf), L.ptr(xf), ctypes.byref(opts), L.ptr(ws),
                                ws.numel(), L.ptr(it), L.ptr(rel), L.ptr(st), ctypes.byref(outer),
                                L.stream_ptr(bf.device)), "lpm_ir_batched")

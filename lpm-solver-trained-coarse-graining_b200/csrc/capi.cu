@@ -2,6 +2,7 @@
 #include <cstdint>
 
 #include "../../include/lpm_b200.h"
+#include "lpm_amg.h"
 #include "lpm_cg.h"
 #include "lpm_tma.h"
 #include "lpm_kernels.h"
@@ -285,6 +286,25 @@ int lpm_ir_batched(const lpm_lattice* lat, const double* Kn64, const double* Tv6
     if (!(opts->tol >= 0.0) || !(opts->inner_tol > 0.0)) return LPM_ERR_ARG;
     return ir_solve(L, Kn64, Tv64, cl64, Kn32, Tv32, cl32, Minv32, bt, mask, b, x, *opts, workspace,
                     workspace_bytes, iters, relres, status, outer_steps, S(stream));
+}
+
+int lpm_ir_amg(const lpm_lattice* lat, const double* Kn64, const double* Tv64, int32_t coef_layout64, lpm_amg* amg,
+               const lpm_batch* batch, const uint8_t* mask, const double* b, double* x, const lpm_ir_opts* opts,
+               void* workspace, size_t workspace_bytes, int32_t* iters, double* relres, int32_t* status,
+               int32_t* outer_steps, void* stream)
+{
+    Lattice L;
+    Batch bt;
+    CoefLayout cl64, cl32;
+    int rc = to_lattice(lat, L);
+    if (rc || (rc = to_batch(batch, bt)) || (rc = to_layout(coef_layout64, L, cl64)) ||
+        (rc = to_layout(LPM_LAYOUT_SOA, L, cl32)))
+        return rc;
+    if (!amg || !Kn64 || !Tv64 || !b || !x || !opts || !workspace || !iters || !relres || !status) return LPM_ERR_ARG;
+    if (!(opts->tol >= 0.0) || !(opts->inner_tol > 0.0)) return LPM_ERR_ARG;
+    if (!amg_matches(amg, L, bt)) return LPM_ERR_ARG;
+    return ir_solve(L, Kn64, Tv64, cl64, nullptr, nullptr, cl32, nullptr, bt, mask, b, x, *opts, workspace,
+                    workspace_bytes, iters, relres, status, outer_steps, S(stream), amg);
 }
 
 int64_t lpm_grad_scratch_bytes(const lpm_lattice* lat, int32_t nsys)

@@ -18,6 +18,7 @@
 #include <cstring>
 #include <vector>
 
+#include "lpm_amg.h"
 #include "lpm_cg.h"
 #include "lpm_graph.h"
 #include "lpm_tma.h"
@@ -523,7 +524,7 @@ template int cg_solve<double>(const Lattice&, const double*, const double*, cons
 int ir_solve(const Lattice& L, const double* Kn64, const double* Tv64, const CoefLayout& cl64, const float* Kn32,
              const float* Tv32, const CoefLayout& cl32, const float* Minv32, const Batch& bt, const uint8_t* mask,
              const double* b, double* x, const lpm_ir_opts& o, void* ws, size_t ws_bytes, int* iters,
-             double* relres, int* status, int* outer, cudaStream_t st)
+             double* relres, int* status, int* outer, cudaStream_t st, lpm_amg* amg)
 {
     if (o.maxit < 1 || o.max_outer < 1 || o.check < 1 || o.poll < 1 || bt.nsys < 1) return LPM_ERR_ARG;
     char* base = static_cast<char*>(ws);
@@ -546,7 +547,24 @@ int ir_solve(const Lattice& L, const double* Kn64, const double* Tv64, const Coe
     for (int k = 0;; ++k) {
         // true residual in FP64
         if (!x_zero) {
-            e = launch_kmv<double>(L, x, Kn64, Tv64, cl64, bt, w.Kx, w.st64, nullptr, st);
+            if (fused_ok(L, cl64, 8) && tma_aligned(x, Kn64, Tv64)) {  // packed FP64 coefficients: TMA operator
+                TmaArgs<double> a{};
+                a.nx = L.nx;
+                a.ny = L.ny;
+                a.nz = L.nz;
+                a.N = N;
+                a.nsys = bt.nsys;
+                a.rhs_per_set = bt.rhs_per_set;
+                a.nmask = bt.nmask;
+                tma_configure(a);
+                a.u = x;
+                a.Kn = Kn64;
+                a.Tv = Tv64;
+                a.out = w.Kx;
+                e = launch_sc_tma<double>(a, false, st);
+            } else {
+                e = launch_kmv<double>(L, x, Kn64, Tv64, cl64, bt, w.Kx, w.st64, nullptr, st);
+            }
             if (e != cudaSuccess) return (int)e;
         }
         for (int s0 = 0; s0 < ns; s0 += 65535) {
@@ -593,8 +611,9 @@ int ir_solve(const Lattice& L, const double* Kn64, const double* Tv64, const Coe
         e = cudaMemcpyAsync(w.itol, h_tol.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) return (int)e;
         lpm_cg_opts io{o.inner_tol, remaining, o.check, o.poll, 0, o.prof, w.itol};
-        rc = cg_solve<float>(L, Kn32, Tv32, cl32, bt, Minv32, mask, w.r32, w.d32, 1, io, w.cg_ws, w.cg_bytes,
-                             w.it_in, w.rel_in, w.st_in, st);
+        rc = amg ? amg_pcg(amg, w.r32, w.d32, io, w.it_in, w.rel_in, w.st_in, st)
+                 : cg_solve<float>(L, Kn32, Tv32, cl32, bt, Minv32, mask, w.r32, w.d32, 1, io, w.cg_ws, w.cg_bytes,
+                                   w.it_in, w.rel_in, w.st_in, st);
         if (rc != LPM_OK) return rc;
         e = cudaMemcpyAsync(h_it.data(), w.it_in, sizeof(int) * ns, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(h_st.data(), w.st_in, sizeof(int) * ns, cudaMemcpyDeviceToHost, st);

@@ -29,8 +29,11 @@
 // multiplied by zero, as in the reference.  (B, A) of sites outside the box is zero.  Every mbarrier wait is bounded;
 // on expiry the kernel records an error code, waits (bounded) for the copies it issued, and stops computing.
 //
-// Epilogue (EPI): per-system u.out partials in FP32 per thread, reduced in FP64 deterministically; the last block of
-// a system runs the CG alpha step.
+// Epilogues (PairMode): PM_NONE writes f = K u; PM_DOT also forms per-system u.f partials in FP32 per thread, reduced
+// in FP64 deterministically, and the last block of a system runs the CG alpha step.  The smoother epilogues of the
+// AMG preconditioner take a right-hand side b (pair layout) and each lane's free box: PM_RESID writes the masked
+// residual m (b - K u), PM_SMOOTH the damped block-Jacobi sweep u + w m M (b - K u) with the 3x3 inverse M of the
+// site (u from the shared-memory tile), and PM_SMOOTH_DOT adds b.out per system and the PCG beta step.
 #include <cudaTypedefs.h>
 
 #include <map>
@@ -110,7 +113,7 @@ __host__ __device__ constexpr SlotGeo slot_geo(int k)
 
 __device__ __forceinline__ pair_t ld2(const float* p) { return *reinterpret_cast<const pair_t*>(p); }
 
-template <bool EPI, bool LEAN>
+template <int MODE, bool LEAN>
 __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
     k_sc_pair(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ CUtensorMap tm_tv,
               const __grid_constant__ CUtensorMap tm_kn, PairArgs P)
@@ -143,6 +146,29 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
     const bool on0 = nr > 0 && (!P.act || P.act[sbase]);
     const bool on1 = nr > 1 && (!P.act || P.act[sbase + 1]);
     bool any_on = on0 || on1;
+    constexpr bool EPI = MODE == PM_DOT || MODE == PM_SMOOTH_DOT;
+    constexpr bool SMOOTH = MODE == PM_SMOOTH || MODE == PM_SMOOTH_DOT;
+    // free boxes and weights of the two lanes (smoother epilogues); a dummy lane has an empty box
+    int bl0[3] = {0, 0, 0}, bh0[3] = {-1, -1, -1}, bl1[3] = {0, 0, 0}, bh1[3] = {-1, -1, -1};
+    float w0 = 0.f, w1 = 0.f;
+    if constexpr (MODE >= PM_RESID) {
+        if (nr > 0) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                bl0[a] = P.fbox[6 * sbase + a];
+                bh0[a] = P.fbox[6 * sbase + 3 + a];
+            }
+            if (SMOOTH) w0 = P.fw[sbase];
+        }
+        if (nr > 1) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                bl1[a] = P.fbox[6 * sbase + 6 + a];
+                bh1[a] = P.fbox[6 * sbase + 9 + a];
+            }
+            if (SMOOTH) w1 = P.fw[sbase + 1];
+        }
+    }
 
     if (tid == 0) {
         for (int b = 0; b < 8; ++b) mbar_init(&bars[b], 1);
@@ -446,14 +472,44 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
             if (sc_shell(k) == 1) f[g.b] = g.sb > 0 ? sub2(f[g.b], gw) : add2(f[g.b], gw);
         }
         pair_t* o = reinterpret_cast<pair_t*>(P.out + (((int64_t)pr * P.N + i) * 3) * 2);
-        o[0] = f[0];
-        o[1] = f[1];
-        o[2] = f[2];
-        if constexpr (EPI) {
-            const float* pu = u_slot(z) + (ty + 2) * PUW + 6 * (tx + 2);
-            dotp = fma2(ld2(pu), f[0], dotp);
-            dotp = fma2(ld2(pu + 2), f[1], dotp);
-            dotp = fma2(ld2(pu + 4), f[2], dotp);
+        if constexpr (MODE <= PM_DOT) {
+            o[0] = f[0];
+            o[1] = f[1];
+            o[2] = f[2];
+            if constexpr (EPI) {
+                const float* pu = u_slot(z) + (ty + 2) * PUW + 6 * (tx + 2);
+                dotp = fma2(ld2(pu), f[0], dotp);
+                dotp = fma2(ld2(pu + 2), f[1], dotp);
+                dotp = fma2(ld2(pu + 4), f[2], dotp);
+            }
+        } else {
+            const bool in0 = gx >= bl0[0] && gx <= bh0[0] && gy >= bl0[1] && gy <= bh0[1] && z >= bl0[2] &&
+                             z <= bh0[2];
+            const bool in1 = gx >= bl1[0] && gx <= bh1[0] && gy >= bl1[1] && gy <= bh1[1] && z >= bl1[2] &&
+                             z <= bh1[2];
+            const pair_t* rh = reinterpret_cast<const pair_t*>(P.rhs + (((int64_t)pr * P.N + i) * 3) * 2);
+            float t0[3], t1[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) unpk(sub2(rh[a], f[a]), t0[a], t1[a]);
+            if constexpr (MODE == PM_RESID) {
+#pragma unroll
+                for (int a = 0; a < 3; ++a) o[a] = pk(in0 ? t0[a] : 0.f, in1 ? t1[a] : 0.f);
+            } else {
+                const float* ms = P.Ms + (int64_t)set * 9 * P.N + i;
+                float m9[9];
+#pragma unroll
+                for (int e = 0; e < 9; ++e) m9[e] = __ldg(ms + (int64_t)e * P.N);
+                const float* pu = u_slot(z) + (ty + 2) * PUW + 6 * (tx + 2);
+                const float c0 = in0 ? w0 : 0.f, c1 = in1 ? w1 : 0.f;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    const float z0 = m9[3 * a] * t0[0] + m9[3 * a + 1] * t0[1] + m9[3 * a + 2] * t0[2];
+                    const float z1 = m9[3 * a] * t1[0] + m9[3 * a + 1] * t1[1] + m9[3 * a + 2] * t1[2];
+                    const pair_t v = fma2(pk(c0, c1), pk(z0, z1), ld2(pu + 2 * a));
+                    o[a] = v;
+                    if constexpr (EPI) dotp = fma2(rh[a], v, dotp);
+                }
+            }
         }
     };
 
@@ -551,7 +607,12 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
                 acc = block_sum(acc, red);
                 if (tid == 0) {
                     P.cnt[s] = 0u;
-                    if (P.has_sc) cg_alpha_step(P.scv, s, acc, P.it);
+                    if (P.has_sc) {
+                        if constexpr (MODE == PM_DOT)
+                            cg_alpha_step(P.scv, s, acc, P.it);
+                        else
+                            cg_beta_step(P.scv, s, acc, P.it);
+                    }
                 }
             }
             __syncthreads();
@@ -559,7 +620,24 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
     }
 }
 
-template <bool EPI, bool LEAN>
+// Opt-in to the kernel's dynamic shared memory, once per device (outside any stream capture: pair_prepare).
+template <int MODE, bool LEAN>
+cudaError_t pair_attr()
+{
+    static unsigned long long attr_set = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!((attr_set >> dev) & 1ull)) {
+        cudaError_t e = cudaFuncSetAttribute(k_sc_pair<MODE, LEAN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)pair_bytes(LEAN));
+        if (e != cudaSuccess) return e;
+        attr_set |= 1ull << dev;
+    }
+    return cudaSuccess;
+}
+
+template <int MODE, bool LEAN>
 cudaError_t launch_pair(const PairArgs& a, cudaStream_t st)
 {
     const int nset = (a.nsys + a.rhs_per_set - 1) / a.rhs_per_set;
@@ -582,23 +660,15 @@ cudaError_t launch_pair(const PairArgs& a, cudaStream_t st)
         else if (!make_tensor_map4(&mkn, 4, a.Kn, dims, str, bkn))
             return cudaErrorInvalidValue;
     }
-    static unsigned long long attr_set = 0;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    if (!((attr_set >> dev) & 1ull)) {
-        cudaError_t e = cudaFuncSetAttribute(k_sc_pair<EPI, LEAN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)pair_bytes(LEAN));
-        if (e != cudaSuccess) return e;
-        attr_set |= 1ull << dev;
-    }
+    cudaError_t e = pair_attr<MODE, LEAN>();
+    if (e != cudaSuccess) return e;
     const int ntile = ((a.nx + PX - 1) / PX) * ((a.ny + PY - 1) / PY);
     const int nzc = (a.nz + a.zchunk - 1) / a.zchunk;
     for (int g0 = 0; g0 < a.npair; g0 += 65535) {
         PairArgs b = a;
         b.pair0 = g0;
         const int ng = a.npair - g0 < 65535 ? a.npair - g0 : 65535;
-        k_sc_pair<EPI, LEAN><<<dim3(ntile * nzc, ng), PNT, pair_bytes(LEAN), st>>>(mu, mtv, mkn, b);
+        k_sc_pair<MODE, LEAN><<<dim3(ntile * nzc, ng), PNT, pair_bytes(LEAN), st>>>(mu, mtv, mkn, b);
     }
     return cudaGetLastError();
 }
@@ -702,12 +772,42 @@ int pair_zchunk_max_chunks(int nz) { return nz / 8 > 1 ? nz / 8 : 1; }
 
 int pair_dot_blocks_max(int nx, int ny, int nz) { return ((nx + PX - 1) / PX) * ((ny + PY - 1) / PY) * (nz / 8 + 1); }
 
-cudaError_t launch_sc_pair(const PairArgs& a, bool epi, cudaStream_t st)
+cudaError_t launch_sc_pair_mode(const PairArgs& a, int mode, cudaStream_t st)
 {
     if (a.npair < 1 || a.npp < 1 || a.zchunk < 1) return cudaErrorInvalidValue;
-    if (a.variant)
-        return epi ? launch_pair<true, true>(a, st) : launch_pair<false, true>(a, st);
-    return epi ? launch_pair<true, false>(a, st) : launch_pair<false, false>(a, st);
+    if (mode >= PM_RESID && (!a.rhs || !a.fbox || (mode >= PM_SMOOTH && (!a.Ms || !a.fw))))
+        return cudaErrorInvalidValue;
+    const bool lean = a.variant != 0;
+    switch (mode) {
+    case PM_NONE: return lean ? launch_pair<PM_NONE, true>(a, st) : launch_pair<PM_NONE, false>(a, st);
+    case PM_DOT: return lean ? launch_pair<PM_DOT, true>(a, st) : launch_pair<PM_DOT, false>(a, st);
+    case PM_RESID: return lean ? launch_pair<PM_RESID, true>(a, st) : launch_pair<PM_RESID, false>(a, st);
+    case PM_SMOOTH: return lean ? launch_pair<PM_SMOOTH, true>(a, st) : launch_pair<PM_SMOOTH, false>(a, st);
+    case PM_SMOOTH_DOT:
+        return lean ? launch_pair<PM_SMOOTH_DOT, true>(a, st) : launch_pair<PM_SMOOTH_DOT, false>(a, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t pair_prepare()
+{
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = pair_attr<PM_NONE, false>();
+    if (e == cudaSuccess) e = pair_attr<PM_NONE, true>();
+    if (e == cudaSuccess) e = pair_attr<PM_DOT, false>();
+    if (e == cudaSuccess) e = pair_attr<PM_DOT, true>();
+    if (e == cudaSuccess) e = pair_attr<PM_RESID, false>();
+    if (e == cudaSuccess) e = pair_attr<PM_RESID, true>();
+    if (e == cudaSuccess) e = pair_attr<PM_SMOOTH, false>();
+    if (e == cudaSuccess) e = pair_attr<PM_SMOOTH, true>();
+    if (e == cudaSuccess) e = pair_attr<PM_SMOOTH_DOT, false>();
+    if (e == cudaSuccess) e = pair_attr<PM_SMOOTH_DOT, true>();
+    return e;
+}
+
+cudaError_t launch_sc_pair(const PairArgs& a, bool epi, cudaStream_t st)
+{
+    return launch_sc_pair_mode(a, epi ? PM_DOT : PM_NONE, st);
 }
 
 }  // namespace lpm

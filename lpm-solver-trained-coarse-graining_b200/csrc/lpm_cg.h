@@ -95,9 +95,10 @@ int cg_solve(const Lattice& L, const T* Kn, const T* Tv, const CoefLayout& cl, c
              const uint8_t* mask, const T* b, T* x, int x_is_zero, const lpm_cg_opts& o, void* ws, size_t ws_bytes,
              int* iters, double* relres, int* status, cudaStream_t st);
 
+// amg != nullptr: the inner solver is the AMG-preconditioned FP32 PCG of the handle (Kn32, Tv32, Minv32 unused).
 int ir_solve(const Lattice& L, const double* Kn64, const double* Tv64, const CoefLayout& cl64, const float* Kn32,
              const float* Tv32, const CoefLayout& cl32, const float* Minv32, const Batch& bt, const uint8_t* mask,
              const double* b, double* x, const lpm_ir_opts& o, void* ws, size_t ws_bytes, int* iters,
-             double* relres, int* status, int* outer, cudaStream_t st);
+             double* relres, int* status, int* outer, cudaStream_t st, lpm_amg* amg = nullptr);
 
 }  // namespace lpm

@@ -44,6 +44,25 @@ __device__ __forceinline__ void cg_alpha_step(const FcgScalars& sc, int s, doubl
     sc.alpha[s] = pAp != 0.0 ? rzc / pAp : 0.0;
 }
 
+// beta step of system s in a PCG whose preconditioner output z comes from an operator epilogue (AMG): run by the
+// last block once r.z is complete.  Iteration 0 is the initial preconditioner application (beta = 0).
+__device__ __forceinline__ void cg_beta_step(const FcgScalars& sc, int s, double rz, int it)
+{
+    if (sc.itp) it = *sc.itp;
+    if (!sc.act[s]) return;
+    const double rzo = sc.rz[((it + 1) & 1) * sc.nsys + s];
+    sc.rz[(it & 1) * sc.nsys + s] = rz;
+    if (!isfinite(rz)) {
+        sc.beta[s] = 0.0;
+        sc.act[s] = 0;
+        sc.iters[s] = it;
+        sc.status[s] = LPM_STATUS_BREAKDOWN;
+        atomicAdd(sc.nconv, 1u);
+        return;
+    }
+    sc.beta[s] = it > 0 && rzo != 0.0 ? rz / rzo : 0.0;
+}
+
 // Batched (P)CG on the TMA operator (dim 3, full box, packed coefficients, tma_supported(nx)).
 template <typename T>
 int cg_solve_fused(const Lattice& L, const T* Kn, const T* Tv, const Batch& bt, const T* Minv, const uint8_t* mask,

@@ -65,6 +65,20 @@ struct PairArgs {
     int has_sc;
     int it;
     int* err;
+    // AMG smoother epilogues (PM_RESID, PM_SMOOTH, PM_SMOOTH_DOT)
+    const float* rhs;  // pair layout: the right-hand side of the smoothing step
+    const float* Ms;   // (nset, 9, N) block-Jacobi inverse
+    const int* fbox;   // (nsys, 6) free box of every system: lo x, y, z, hi x, y, z (inclusive)
+    const float* fw;   // (nsys) smoother weight omega / rho
+};
+
+// Epilogues of the pair operator.  f = K u per site and lane; m = 1 inside the lane's free box, else 0.
+enum PairMode {
+    PM_NONE = 0,       // out = f
+    PM_DOT = 1,        // out = f; u.f per system, the last block runs the CG alpha step
+    PM_RESID = 2,      // out = m (rhs - f)
+    PM_SMOOTH = 3,     // out = u + w m M (rhs - f)            (damped block-Jacobi sweep)
+    PM_SMOOTH_DOT = 4  // as PM_SMOOTH; rhs.out per system, the last block runs the PCG beta step
 };
 
 bool pair_supported(int nx);
@@ -76,6 +90,9 @@ void pair_zchunk_record(int nx, int ny, int nz, int npair, int zchunk, int varia
 int pair_zchunk_max_chunks(int nz);                               // z chunks allowed (>= 8 planes each)
 int pair_dot_blocks_max(int nx, int ny, int nz);
 cudaError_t launch_sc_pair(const PairArgs& a, bool epi, cudaStream_t st);
+cudaError_t launch_sc_pair_mode(const PairArgs& a, int mode, cudaStream_t st);
+// Shared-memory opt-in of every pair-operator kernel on the current device (call before capturing launches).
+cudaError_t pair_prepare();
 // (nsys, N, 3) FP32 -> pair layout (dummy lanes written as zero) and back (real systems only); npair <= 65535.
 cudaError_t pair_pack(const float* x, float* xp, int64_t N, int nsys, int rps, cudaStream_t st);
 cudaError_t pair_unpack(const float* xp, float* x, int64_t N, int nsys, int rps, cudaStream_t st);

@@ -14,7 +14,8 @@ reference itself produced (tests/golden/make_golden.py, part "amg").
                                          colour classes of aggregates (aggregates at least 3 sites wide; the operator
                                          reaches 2 sites, so each probe meets one aggregate of its colour per row)
   st_galerkin        amg3d.py:253-295    Q^T A Q on 27-point 6x6-block stencils
-  power_rho          amg3d.py:506-519    rho(D^-1 A) by power iteration from rng(0)
+  power_rho          amg3d.py:506-519    rho(D^-1 A) by power iteration from rng(0) (or, to check the CUDA
+                                         hierarchy, from its counter-based start vectors: hash_normals)
   Hierarchy          amg3d.py:522-668    numeric setup, V/W-cycle (vcycle, _coarse, _vc) and PCG
 """
 import math
@@ -187,9 +188,31 @@ def bj(M, r, w):
     return w * np.einsum("nab,nb->na", M, r)
 
 
-def power_rho(mv, Minv, shape, its, seed=0):
-    """rho(D^-1 A) by `its` power steps from rng(seed) normals pre-multiplied by Minv (amg3d.py:506-519)."""
-    x = bj(Minv, np.random.default_rng(seed).standard_normal(shape), 1.0)
+def _mix64(z):
+    z = z + np.uint64(0x9E3779B97F4A7C15)
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def hash_normals(level, shape):
+    """The counter-based normals that the CUDA power iterations start from (csrc/amg.cu start_normal): element e of
+    level `level` (0 = finest) from the splitmix64 finaliser and Box-Muller, rounded to FP32 as the device does."""
+    n = int(np.prod(shape))
+    with np.errstate(over="ignore"):
+        e = np.arange(n, dtype=np.uint64)
+        k = (np.uint64(level + 1) << np.uint64(56)) ^ (e << np.uint64(1))
+        u1 = ((_mix64(k) >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
+        u2 = ((_mix64(k | np.uint64(1)) >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
+    z = np.sqrt(-2.0 * np.log(u1)) * np.cos(6.283185307179586 * u2)
+    return z.astype(np.float32).astype(np.float64).reshape(shape)
+
+
+def power_rho(mv, Minv, shape, its, seed=0, start=None):
+    """rho(D^-1 A) by `its` power steps from rng(seed) normals (or the given start) pre-multiplied by Minv
+    (amg3d.py:506-519)."""
+    x0 = np.random.default_rng(seed).standard_normal(shape) if start is None else start
+    x = bj(Minv, x0, 1.0)
     lam = 1.0
     for _ in range(its):
         x = x / np.linalg.norm(x)
@@ -231,7 +254,7 @@ class Hierarchy:
     solver.  Defaults are timing/t3d/problems.py:19 (AMG_CFG) apart from the geometry's agg and coarse_max."""
 
     def __init__(self, geo, Kn, Tv, nu=1, omega=1.32, power_its=5, Minv0=None, nu_c=None, gamma=2, w_from=1,
-                 rho0=None):
+                 rho0=None, start="numpy"):
         self.geo, self.Kn, self.Tv = geo, np.asarray(Kn, np.float64), np.asarray(Tv, np.float64)
         self.nu, self.omega = nu, omega
         self.nu_c = nu if nu_c is None else nu_c
@@ -244,14 +267,17 @@ class Hierarchy:
         else:
             Minv0 = Minv0 * free[:, None, None]
         self.M0 = Minv0
-        self.rho0 = power_rho(self.apply0, self.M0, (self.N, 3), power_its) if rho0 is None else rho0
+        st = (lambda lvl, shape: None) if start == "numpy" else hash_normals
+        self.rho0 = power_rho(self.apply0, self.M0, (self.N, 3), power_its, start=st(0, (self.N, 3))) \
+            if rho0 is None else rho0
         self.A = [galerkin0(geo, self.Kn, self.Tv)]
         self.Minv, self.rho = [], []
         for k, Lg in enumerate(geo.levels):
             A = self.A[-1]
             Mi = np.linalg.inv(A[:, 13])
             self.Minv.append(Mi)
-            self.rho.append(power_rho(lambda x, A=A, g=Lg["g"]: st_mv(A, g, x), Mi, (A.shape[0], 6), power_its))
+            self.rho.append(power_rho(lambda x, A=A, g=Lg["g"]: st_mv(A, g, x), Mi, (A.shape[0], 6), power_its,
+                                      start=st(k + 1, (A.shape[0], 6))))
             self.A.append(st_galerkin(A, Lg["g"], Lg["Q"], Lg["agg_of"], Lg["gc"]))
         D = dense_from_stencil(self.A[-1], geo.grids[-1])
         self.cho = sla.cho_factor(0.5 * (D + D.T), lower=False, check_finite=False)

@@ -32,7 +32,7 @@ def test_library_exports_header():
 
 def test_abi_version_and_strings():
     lib = L.load()
-    assert lib.lpm_abi_version() == 2
+    assert lib.lpm_abi_version() == 3
     assert lib.lpm_status_string(0) == b"ok"
     assert b"argument" in lib.lpm_status_string(-1)
     assert b"workspace" in lib.lpm_status_string(-2)
@@ -65,3 +65,31 @@ def test_no_cpu_fallback():
         pytest.skip("checks the no-GPU behaviour")
     with pytest.raises(L.LPMError):
         core.DeviceLattice(geom.LatticeGeom(4, 4, 4), device="cpu")
+
+
+def test_amg_create_validation():
+    """lpm_amg_create rejects bad boxes, masks and options on the host, before any device work."""
+    lib = L.load()
+    lat = L.Lattice(3, 12, 12, 12, 12 ** 3, None)
+    b = L.Batch(2, 2, 2, 0)
+    o = L.AmgOpts()
+    lib.lpm_amg_default_opts(ctypes.byref(o))
+    assert (o.agg, o.coarse_max, o.nu, o.gamma, o.power_its) == (3, 1000, 1, 2, 5) and abs(o.omega - 1.32) < 1e-15
+    h = ctypes.c_void_p(None)
+    box = (ctypes.c_int32 * 6)(1, 1, 1, 10, 10, 10)
+    of = (ctypes.c_int32 * 2)(0, 0)
+    bad_box = (ctypes.c_int32 * 6)(1, 1, 1, 12, 10, 10)           # hi beyond the lattice
+    assert lib.lpm_amg_create(ctypes.byref(lat), ctypes.byref(b), bad_box, 1, of, ctypes.byref(o),
+                              ctypes.byref(h)) == -1
+    bad_of = (ctypes.c_int32 * 2)(0, 1)                              # mask 1 names box 1 of a single box
+    assert lib.lpm_amg_create(ctypes.byref(lat), ctypes.byref(b), box, 1, bad_of, ctypes.byref(o),
+                              ctypes.byref(h)) == -1
+    thin = (ctypes.c_int32 * 6)(0, 0, 0, 0, 0, 11)                    # a line: rank-deficient aggregates
+    assert lib.lpm_amg_create(ctypes.byref(lat), ctypes.byref(b), thin, 1, of, ctypes.byref(o),
+                              ctypes.byref(h)) == -3
+    o2 = L.AmgOpts()
+    lib.lpm_amg_default_opts(ctypes.byref(o2))
+    o2.agg = 2                                                       # aggregates must be at least 3 sites wide
+    assert lib.lpm_amg_create(ctypes.byref(lat), ctypes.byref(b), box, 1, of, ctypes.byref(o2),
+                              ctypes.byref(h)) == -3
+    assert not h.value
