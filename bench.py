@@ -7,12 +7,14 @@ Workloads (one "step" = one batched solve of every system from scratch, inputs r
   ellipsoids192: 192^3, seeded randomly oriented prolate ellipsoids 3:1:1 (volume of a sphere of radius 4, volume
     fraction 0.30, contrast 15, nu = 0.2), 9 load cases (6 KUBC strains + uniaxial tension along x, y, z) as 9
     right-hand sides of one specimen.
-Each step forms b = -K u_p in FP64, packs FP32 coefficients, builds the 3x3 block-Jacobi preconditioner and runs FP32
-PCG inside FP64 iterative refinement until every system's FP64 true residual is <= 1e-8 |b|.  Synthetic data (no
-dataset is involved).
+Each step forms b = -K u_p in FP64, packs FP32 coefficients, builds the preconditioner -- by default the aggregation
+AMG of timing/t3d/amg3d.py (numeric setup of every specimen's hierarchies inside the step; the aggregation geometry is
+built once per lattice and BC set, as the reference does), or the 3x3 block Jacobi (--precond bj) -- and runs FP32 PCG
+inside FP64 iterative refinement until every system's FP64 true residual is <= 1e-8 |b|.  Synthetic data (no dataset
+is involved).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--workload spheres48|ellipsoids192]
-                    [--impl ours|reference]
+                    [--precond amg|bj] [--inner-tol T] [--impl ours|reference]
 
 Under torchrun (N > 1) every rank solves its own B specimens (weak scaling, no data-path collective); the step time
 is the max over ranks.  `--impl reference` times the CPU oracle (the reference's FP64 block-Jacobi PCG restated in C,
@@ -46,12 +48,17 @@ WORKLOADS = {
 TOL = 1e-8
 
 
-def workload_config(w, batch, n_gpus):
+PRECONDS = {"amg": "aggregation AMG, W(1,1) cycle, one hierarchy per specimen and BC box (timing/t3d/amg3d.py, "
+                   "settings of timing/t3d/problems.py:19); numeric setup inside every step",
+            "bj": "3x3 block Jacobi"}
+
+
+def workload_config(w, batch, n_gpus, precond="amg"):
     W = WORKLOADS[w]
     n, L = W["n"], len(W["loads"])
     return {"workload": W["label"], "lattice": [n] * 3, "specimens_per_gpu": batch, "rhs_per_specimen": L,
             "systems_per_gpu": L * batch, "tol": TOL, "precision": "fp32 inner PCG + fp64 refinement",
-            "preconditioner": "3x3 block Jacobi", "l2": "inputs larger than L2 (%.0f MB of FP64 coefficients per GPU)"
+            "preconditioner": PRECONDS[precond], "l2": "inputs larger than L2 (%.0f MB of FP64 coefficients per GPU)"
             % (batch * n ** 3 * 36 * 8 / 1e6), "parallelism": "dp%d (independent specimens per GPU)" % n_gpus}
 
 
@@ -220,7 +227,7 @@ def run_reference(a):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": 1e3 * tot / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(a.workload, a.batch, a.gpus),
+            "config": workload_config(a.workload, a.batch, a.gpus, a.precond),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port",
                              "sample": "%d load case(s) per step of specimen 0, FP64 block-Jacobi PCG to 1e-8 "
                                        "(oracle restating coarse3d/lin3d.py:464-532)" % nsolve},
@@ -570,8 +577,13 @@ def main():
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 CG comparator")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--inner-tol", type=float, default=1e-3)
+    ap.add_argument("--precond", default="amg", choices=sorted(PRECONDS),
+                    help="inner PCG preconditioner of the 3D workloads (default: AMG)")
+    ap.add_argument("--inner-tol", type=float, default=None,
+                    help="inner FP32 solve tolerance (default 1e-4 with AMG, 1e-3 with block Jacobi)")
     a = ap.parse_args()
+    if a.inner_tol is None:
+        a.inner_tol = 1e-4 if a.precond == "amg" else 1e-3
     if a.batch is None:
         a.batch = 16 if a.workload == "spheres48" else 1
     if a.workload == "serve":
@@ -611,10 +623,22 @@ def main():
     tiles = core.autotune(dl, core.pack(Kn[:, 0], torch.float32), core.pack(Tv[:, 0], torch.float32), nsys, Lc,
                           with_variant=True)
 
+    amgb = None
+    if a.precond == "amg":
+        # geometry of the hierarchies (aggregation, transfers): once per lattice and BC set, like the neighbour lists
+        from lpm_b200 import amg as GA
+        amgb = GA.AmgBatch(dl, nsys, Lc, free_h, **GA.AMG_CFG)
+
     def step(Kn, Tv, free, ups, prof=None):
         b = -core.kmv(dl, ups, Kn, Tv) * free[None, :, :, None]
-        x, info = core.ir(dl, Kn, Tv, b, free=free, tol=TOL, inner_tol=a.inner_tol, prof=prof)
-        return ups + x, info
+        if amgb is None:
+            x, info = core.ir(dl, Kn, Tv, b, free=free, tol=TOL, inner_tol=a.inner_tol, prof=prof)
+            return ups + x, info
+        # per-specimen numeric setup (block inverses, rho, Galerkin products, coarse inverse) is part of every step
+        K32, T32 = core.pack(Kn[:, 0], torch.float32), core.pack(Tv[:, 0], torch.float32)
+        amgb.setup(K32, T32, core.block_jacobi(dl, Kn[:, 0], Tv[:, 0], torch.float32))
+        x, info = amgb.ir(Kn[:, 0], Tv[:, 0], b.reshape(nsys, lat.N, 3), tol=TOL, inner_tol=a.inner_tol, prof=prof)
+        return ups + x.reshape(ups.shape), info
 
     def barrier():
         if world > 1:
@@ -625,7 +649,6 @@ def main():
         u, info = step(Kn, Tv, free, ups)
     barrier()
 
-    prof = core.new_prof()
     sampler = ClockSampler(local)
     sampler.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -633,11 +656,16 @@ def main():
     ev0.record()
     infos = []
     for _ in range(a.steps):
-        u, info = step(Kn, Tv, free, ups, prof)
+        u, info = step(Kn, Tv, free, ups)
         infos.append(info)
     ev1.record()
     barrier()
     clocks = sampler.stop()
+    # per-launch operator timings come from one more step outside the timed region (timing every launch with events
+    # turns off the CUDA-graph replay of the iteration blocks)
+    prof = core.new_prof()
+    step(Kn, Tv, free, ups, prof)
+    barrier()
     ms = max_over_ranks(ev0.elapsed_time(ev1), world, dev)
     value = job_throughput(world, nsys, a.steps, ms)
     ok = all((i.status == 0).all() and (i.relres <= TOL).all() for i in infos)
@@ -665,7 +693,8 @@ def main():
                 "traffic_source": "ncu dram bytes of a 4-specimen launch (profiles/k_sc_pair_48cube_batch4.md) scaled "
                                   "by systems",
                 "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": full_ms, "avg_launch_ms_all": all_ms,
-                "launches_timed": int(prof[1]), "peak_source": peak_src}
+                "launches_profiled": int(prof[1]), "peak_source": peak_src,
+                "timing_source": "CUDA events around every operator launch of one extra step outside the timed region"}
 
     # ---- end to end through the public API with host buffers (pinned), copies inside the timed region
     Kn_pin = torch.as_tensor(Kn_h).pin_memory()
@@ -748,15 +777,23 @@ def main():
     # epilogue, update, p-update); per step 2 (b = -K u_p) + 2 (FP32 packing) + 1 (block Jacobi); per refinement
     # step 2 (FP64 K.u) + 1 (residual) + 1 (scale) + 3 (preconditioner repack, PCG init, unpack) + 1 (correction);
     # plus the final residual check (3).  Iterations per inner solve are counted as the slowest system's.
+    # With AMG: per step 2 (b = -K u_p) + 2 (FP32 packing) + 1 (block Jacobi) + 2 (FP64 packing) + the AMG setup, and
+    # per inner iteration / inner solve / refinement step the counts of AmgBatch.launches (operator, update, cycle
+    # with every coarse-level kernel, p-update).
     total_inner = int(sum(int(i.iters.max()) for i in infos))
     outer = sum(int(i.outer) for i in infos)
-    gpu_launches = total_inner * 3 + a.steps * (5 + 3) + outer * 8
+    if amgb is None:
+        gpu_launches = total_inner * 3 + a.steps * (5 + 3) + outer * 8
+    else:
+        gpu_launches = a.steps * 7 + sum(amgb.launches(int(i.iters.max()), int(i.outer), int(i.outer)) for i in infos)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64", "data": "synthetic (seeded %s microstructures, shapes of the %d^3 config)"
             % ("spheres" if a.workload == "spheres48" else "prolate-ellipsoid", WORKLOADS[a.workload]["n"]),
-            "config": dict(workload_config(a.workload, B, world),
-                           operator_tiles={"zchunk": tiles[0], "variant": ["staged", "lean"][tiles[1]]}),
+            "config": dict(workload_config(a.workload, B, world, a.precond), inner_tol=a.inner_tol,
+                           operator_tiles={"zchunk": tiles[0], "variant": ["staged", "lean"][tiles[1]]},
+                           amg_levels=[[list(g) for g in amgb.grids(k)[0]] for k in range(len(amgb.boxes))]
+                           if amgb is not None else None),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "clocks": clocks, "gpu_launches": gpu_launches, "all_converged": bool(ok),
             "inner_iters_mean": float(iters.mean()), "outer_steps": [i.outer for i in infos][:1],

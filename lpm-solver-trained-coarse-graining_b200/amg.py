@@ -137,6 +137,42 @@ class AmgBatch:
                                            ctypes.byref(rho), None), "lpm_amg_get_level")
         return A, rho.value
 
+    # ------------------------------------------------------------------------------------------ launch counts
+    def _cycle_launches(self):
+        """Kernel launches of one finest-level cycle (csrc/amg.cu fine_cycle), from the level structure."""
+        o = self.opts
+        total = 2                                   # residual and smoothing epilogues of the pair operator
+        for k in range(len(self.boxes)):
+            nlev = len(self.grids(k)[0])
+
+            def vc(l):
+                if l == nlev - 1:
+                    return 1                        # dense coarsest level
+                return 1 + (o.nu_c - 1) + 1 + 1 + coarse(l + 1) + 1 + o.nu_c
+
+            def coarse(l):
+                n = vc(l)
+                if l < nlev - 1 and l + 1 >= o.w_from:
+                    n += (o.gamma - 1) * (1 + vc(l))
+                return n
+            total += 2 + coarse(0)                  # restriction, coarse levels, prolongation of the box
+        return total
+
+    def launches(self, inner_iters, inner_solves, outer_steps):
+        """Kernel launches of this library in one setup + mixed-precision solve with the given counts."""
+        o = self.opts
+        cyc = self._cycle_launches()
+        setup = 1 + 1 + 2 * o.power_its + 2
+        for k in range(len(self.boxes)):
+            grids = self.grids(k)[0]
+            nc = 6 * int(np.prod(grids[-1]))
+            nbk = -(-nc // 32)
+            setup += 27 // 3 * 3 + (len(grids) - 1) * (5 + 2 * o.power_its) + 3 + 4 * nbk
+        per_iter = 3 + cyc
+        per_solve = 3 + cyc
+        per_outer = 4
+        return setup + inner_iters * per_iter + inner_solves * per_solve + outer_steps * per_outer + 2
+
     # ------------------------------------------------------------------------------------------- applications
     def apply(self, r):
         """z = B r for every system: r (nsys, N, 3) FP32 CUDA tensor."""
