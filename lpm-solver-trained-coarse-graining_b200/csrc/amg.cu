@@ -895,35 +895,6 @@ __global__ void __launch_bounds__(LB) k_lv_bj(LvView V, const int* __restrict__ 
     }
 }
 
-// bc[j][J][c] = sum over the nodes m of coarse node J of (Q_m^T r[j][m])_c   (amg3d.py:298-310); one thread per
-// (coarse node, component) and system.
-__global__ void __launch_bounds__(LB) k_lv_restrict(int gx, int gy, int gz, int n, int cx, int cy, int cz, int a,
-                                                    const float* __restrict__ Q, const int* __restrict__ sys,
-                                                    const int* __restrict__ act, const float* __restrict__ r,
-                                                    float* __restrict__ bc)
-{
-    const int t = blockIdx.x * LB + threadIdx.x;
-    const int j = blockIdx.y;
-    const int nc = cx * cy * cz;
-    if (t >= 6 * nc || (act && !act[sys[j]])) return;
-    const int J = t / 6, cc = t % 6;
-    const int c[3] = {J % cx, (J / cx) % cy, J / (cx * cy)};
-    const int g[3] = {gx, gy, gz}, nch[3] = {cx, cy, cz};
-    int s0[3], w[3];
-#pragma unroll
-    for (int ax = 0; ax < 3; ++ax) chunk_range(c[ax], a, nch[ax], g[ax], s0[ax], w[ax]);
-    float acc = 0.f;
-    for (int dz = 0; dz < w[2]; ++dz)
-        for (int dy = 0; dy < w[1]; ++dy)
-            for (int dx = 0; dx < w[0]; ++dx) {
-                const int m = ((s0[2] + dz) * gy + s0[1] + dy) * gx + s0[0] + dx;
-                const float* rv = r + ((int64_t)j * n + m) * 6;
-                const float* q = Q + (int64_t)m * 36 + cc;
-#pragma unroll
-                for (int a2 = 0; a2 < 6; ++a2) acc += q[a2 * 6] * rv[a2];
-            }
-    bc[((int64_t)j * nc + J) * 6 + cc] = acc;
-}
 
 // x[j][m] += Q_m e[j][agg(m)]   (amg3d.py:313-326)
 __global__ void __launch_bounds__(LB) k_lv_prolong(int gx, int gy, int gz, int cx, int cy, int cz, int a,
@@ -949,6 +920,57 @@ __global__ void __launch_bounds__(LB) k_lv_prolong(int gx, int gy, int gz, int c
 #pragma unroll
         for (int cc = 0; cc < 6; ++cc) s += q[a2 * 6 + cc] * eg[cc];
         xo[a2] += s;
+    }
+}
+
+// bc[j][J] = sum over the nodes m of coarse node J of Q_m^T r[j][m]   (amg3d.py:298-310).  A block covers TXA coarse
+// nodes along x of one coarse row (Cy, Cz) for system j; thread (ia, rs) takes coarse node ia of the tile and its
+// member rows rs, rs + 8, ... -- runs of consecutive nodes, so both r (24 bytes per node) and Q (144 bytes per node)
+// are read contiguously across the warp.
+__global__ void __launch_bounds__(256) k_lv_restrict(int gx, int gy, int gz, int n, int cx, int cy, int cz, int a,
+                                                     const float* __restrict__ Q, const int* __restrict__ sys,
+                                                     const int* __restrict__ act, const float* __restrict__ r,
+                                                     float* __restrict__ bc)
+{
+    __shared__ float red[8][TXA][7];
+    const int j = blockIdx.y;
+    if (act && !act[sys[j]]) return;
+    const int ia = threadIdx.x & (TXA - 1), rs = threadIdx.x >> 5;
+    const int tiles_x = (cx + TXA - 1) / TXA;
+    const int tx = blockIdx.x % tiles_x, row = blockIdx.x / tiles_x;
+    const int Cy = row % cy, Cz = row / cy, Cx = tx * TXA + ia;
+    const bool valid = Cx < cx;
+    int sx, wx, sy, wy, sz, wz;
+    chunk_range(valid ? Cx : 0, a, cx, gx, sx, wx);
+    chunk_range(Cy, a, cy, gy, sy, wy);
+    chunk_range(Cz, a, cz, gz, sz, wz);
+    float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (valid) {
+        for (int rr = rs; rr < wy * wz; rr += 8) {
+            const int m0 = ((sz + rr / wy) * gy + sy + rr % wy) * gx + sx;
+            for (int px = 0; px < wx; ++px) {
+                const float* rv = r + ((int64_t)j * n + m0 + px) * 6;
+                const float* q = Q + (int64_t)(m0 + px) * 36;
+                float rl[6];
+#pragma unroll
+                for (int k = 0; k < 6; ++k) rl[k] = rv[k];
+#pragma unroll
+                for (int k = 0; k < 6; ++k)
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) acc[c] += q[k * 6 + c] * rl[k];
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) red[rs][ia][c] = acc[c];
+    __syncthreads();
+    for (int o = threadIdx.x; o < TXA * 6; o += blockDim.x) {
+        const int ib = o / 6, c = o % 6, Cxb = tx * TXA + ib;
+        if (Cxb >= cx) continue;
+        float v = 0.f;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v += red[q][ib][c];
+        bc[((int64_t)j * cx * cy * cz + (Cz * cy + Cy) * cx + Cxb) * 6 + c] = v;
     }
 }
 
@@ -1358,8 +1380,13 @@ struct lpm_amg {
     void* mem = nullptr;
     size_t bytes = 0;
     bool ready = false;
+    // the coarse cycles of different boxes run on their own streams (forked from and joined to the caller's)
+    std::vector<cudaStream_t> bst;
+    std::vector<cudaEvent_t> bev;  // [0]: fork, [1 + k]: join of box k
     ~lpm_amg()
     {
+        for (auto s : bst) cudaStreamDestroy(s);
+        for (auto e : bev) cudaEventDestroy(e);
         if (mem) cudaFree(mem);
     }
 };
@@ -1612,8 +1639,9 @@ cudaError_t vc(const CycleCtx& C, int l, const float* rhs, float* out, int acc)
     }
     k_lv_op<1><<<gg, LB, 0, C.st>>>(V, b.grp, b.sys, C.act, x, rhs, Lv.T, 0);
     const auto& Cl = b.lev[l + 1];
-    k_lv_restrict<<<grid2(6LL * Cl.n, LB, b.nsb), LB, 0, C.st>>>(Lv.g[0], Lv.g[1], Lv.g[2], Lv.n, Cl.g[0], Cl.g[1],
-                                                                 Cl.g[2], h.o.agg, Lv.Q, b.sys, C.act, Lv.T, Cl.B);
+    k_lv_restrict<<<dim3(transfer_tiles(Cl.g), b.nsb), 256, 0, C.st>>>(Lv.g[0], Lv.g[1], Lv.g[2], Lv.n, Cl.g[0],
+                                                                        Cl.g[1], Cl.g[2], h.o.agg, Lv.Q, b.sys, C.act,
+                                                                        Lv.T, Cl.B);
     cudaError_t e = coarse(C, l + 1);
     if (e != cudaSuccess) return e;
     k_lv_prolong<<<g, LB, 0, C.st>>>(Lv.g[0], Lv.g[1], Lv.g[2], Cl.g[0], Cl.g[1], Cl.g[2], h.o.agg, Lv.Q, b.sys, h.rps,
@@ -1646,8 +1674,17 @@ cudaError_t fine_cycle(const lpm_amg& h, const FcgScalars& sc, bool dot, cudaStr
     a.out = h.Ap;
     cudaError_t e = launch_sc_pair_mode(a, PM_RESID, st);
     if (e != cudaSuccess) return e;
-    for (const auto& b : h.box) {
+    // boxes in parallel: fork after the residual, join before the smoothing epilogue
+    const bool fork = h.bst.size() > 1;
+    if (fork) {
+        if ((e = cudaEventRecord(h.bev[0], st)) != cudaSuccess) return e;
+        for (auto sb : h.bst)
+            if ((e = cudaStreamWaitEvent(sb, h.bev[0], 0)) != cudaSuccess) return e;
+    }
+    for (size_t bi = 0; bi < h.box.size(); ++bi) {
+        const auto& b = h.box[bi];
         if (b.nsb == 0) continue;
+        cudaStream_t sb = fork ? h.bst[bi] : st;
         BoxDev B{};
         for (int ax = 0; ax < 3; ++ax) {
             B.lo[ax] = b.lo[ax];
@@ -1657,25 +1694,20 @@ cudaError_t fine_cycle(const lpm_amg& h, const FcgScalars& sc, bool dot, cudaStr
         B.n1 = b.lev[0].n;
         B.B1 = b.lev[0].B;
         B.E1 = b.lev[0].E;
-        k_restrict0<false><<<dim3(b.tiles, b.npent), 256, 0, st>>>(B, h.o.agg, h.L.nx, h.L.ny, h.L.N, b.pent, b.sys,
+        k_restrict0<false><<<dim3(b.tiles, b.npent), 256, 0, sb>>>(B, h.o.agg, h.L.nx, h.L.ny, h.L.N, b.pent, b.sys,
                                                                    sc.act, h.Ap, 0, nullptr);
-        CycleCtx C{&h, &b, sc.act, st};
+        CycleCtx C{&h, &b, sc.act, sb};
         if ((e = coarse(C, 0)) != cudaSuccess) return e;
-    }
-    for (const auto& b : h.box) {
-        if (b.nsb == 0) continue;
-        BoxDev B{};
-        for (int ax = 0; ax < 3; ++ax) {
-            B.lo[ax] = b.lo[ax];
-            B.L[ax] = b.L[ax];
-            B.nch[ax] = b.nch[ax];
-        }
-        B.n1 = b.lev[0].n;
+        // lanes of other boxes are never written, so the boxes' prolongations may run concurrently
         B.E1 = b.lev[0].E;
-        k_prolong0<<<dim3(b.tiles, b.npent), 256, 0, st>>>(B, h.o.agg, h.L.nx, h.L.ny, h.L.N, b.pent, b.sys, sc.act,
+        k_prolong0<<<dim3(b.tiles, b.npent), 256, 0, sb>>>(B, h.o.agg, h.L.nx, h.L.ny, h.L.N, b.pent, b.sys, sc.act,
                                                            h.v);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (fork) {
+            if ((e = cudaEventRecord(h.bev[1 + bi], sb)) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(st, h.bev[1 + bi], 0)) != cudaSuccess) return e;
+        }
     }
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     a.part = dot ? h.mpart : nullptr;
     a.cnt = h.mcnt;
     a.scv = sc;
@@ -2078,6 +2110,20 @@ int lpm_amg_create(const lpm_lattice* lat, const lpm_batch* batch, const int32_t
     h->zchunk = pair_zchunk(h->L.nx, h->L.ny, h->L.nz, h->npair);
     h->variant = pair_variant(h->L.nx, h->L.ny, h->L.nz, h->npair);
     h->zchunk_probe = pair_zchunk(h->L.nx, h->L.ny, h->L.nz, h->nset * PNP);
+    int nused = 0;
+    for (auto& b : h->box) nused += b.nsb > 0;
+    if (nused > 1) {
+        h->bst.assign(nbox, nullptr);
+        h->bev.assign(1 + nbox, nullptr);
+        for (int k = 0; k < nbox && e == cudaSuccess; ++k)
+            e = cudaStreamCreateWithFlags(&h->bst[k], cudaStreamNonBlocking);
+        for (int k = 0; k < 1 + nbox && e == cudaSuccess; ++k)
+            e = cudaEventCreateWithFlags(&h->bev[k], cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            delete h;
+            return (int)e;
+        }
+    }
     *out = h;
     return LPM_OK;
 }
