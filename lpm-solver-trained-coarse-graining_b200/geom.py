@@ -210,6 +210,22 @@ def free_surface_cells(load, nc):
     return face & ~grip
 
 
+def interface_cells(phase, n, s):
+    """Cells of size s whose block holds a voxel with a 6-neighbour of the other phase (coarse3d/geom3d.py:134-147)."""
+    p = np.asarray(phase).reshape(n, n, n)
+    b = np.zeros(p.shape, bool)
+    for ax in range(3):
+        d = np.diff(p, axis=ax) != 0
+        lo = [slice(None)] * 3
+        hi = [slice(None)] * 3
+        lo[ax] = slice(1, None)
+        hi[ax] = slice(None, -1)
+        b[tuple(lo)] |= d
+        b[tuple(hi)] |= d
+    nc = n // s
+    return b.reshape(nc, s, nc, s, nc, s).any(axis=(1, 3, 5)).ravel()
+
+
 def cell_ijk(nc):
     I, J, K = _site_coords(*nc)
     return np.stack([I, J, K], 1)

@@ -191,6 +191,41 @@ class LatticeOperator:
         info.raise_on_breakdown()
         return up + x, info
 
+    def solve_amg(self, Kn, Tv, up, free, tol=1e-8, inner_tol=1e-4, maxit=20000, **amg_cfg):
+        """Mixed-precision solve preconditioned by the aggregation AMG (``amg.AmgBatch``, settings of
+        timing/t3d/problems.py:19 unless overridden): full simple-cubic boxes whose free sets are boxes, as every load case
+        of geom.prescribed.  One hierarchy per (specimen, free box), rebuilt for the coefficients of every call; the
+        aggregation geometry is cached per batch shape and set of masks.  Returns (up + x, SolveInfo)."""
+        from . import amg as GA
+        if self.d != 3 or self.dl.nbr is not None:
+            raise ValueError("solve_amg needs a full simple-cubic box")
+        with torch.no_grad():
+            lead = tuple(torch.broadcast_shapes(up.shape[:-2], Kn.shape[:-2], free.shape[:-1]))
+            N, d = self.N, self.d
+            b = (-self.apply(up, Kn, Tv) * free[..., None]).expand(lead + (N, d))
+            Kc, rps = core.coef_sets(Kn.to(_F64), self.dl, lead)
+            Tc, _ = core.coef_sets(Tv.to(_F64), self.dl, lead)
+            nsys = int(np.prod(lead)) if lead else 1
+            fm = (free.expand(lead + (N,)) != 0).reshape(nsys, N)
+            per_set = fm.reshape(-1, rps, N)
+            masks = per_set[0] if bool((per_set == per_set[:1]).all()) else fm
+            mh = masks.cpu().numpy()
+            cfg = dict(GA.AMG_CFG, **amg_cfg)
+            key = (nsys, rps, mh.shape, hash(mh.tobytes()), tuple(sorted(cfg.items())))
+            cache = self.__dict__.setdefault("_amg_cache", {})
+            ab = cache.get(key)
+            if ab is None:
+                if len(cache) >= 4:
+                    for v in cache.values():
+                        v.close()
+                    cache.clear()
+                ab = cache[key] = GA.AmgBatch(self.dl, nsys, rps, mh, **cfg)
+            K32, T32 = core.pack(Kc, torch.float32), core.pack(Tc, torch.float32)
+            ab.setup(K32, T32, core.block_jacobi(self.dl, Kc, Tc, torch.float32))
+            x, info = ab.ir(Kc, Tc, b.reshape(nsys, N, d), tol=tol, inner_tol=inner_tol, maxit=maxit)
+        info.raise_on_breakdown()
+        return up + x.reshape(lead + (N, d)), info
+
 
 class LinSolve(torch.autograd.Function):
     """u = solve(Kn, Tv) with the exact adjoint gradient w.r.t. Kn, Tv (coarse3d/torch_lpm3d.py:151-175; for the

@@ -92,7 +92,7 @@ class FineRefT:
     reactions for the load cases, all samples of a batch at once (coarse3d/torch_lpm3d.py:230-263).
 
     precision="fp64" runs the reference's FP64 block-Jacobi PCG; "mixed" runs FP32 PCG inside FP64 refinement to the
-    same FP64 true-residual tolerance."""
+    same FP64 true-residual tolerance; "amg" the same refinement with the aggregation-AMG preconditioner."""
 
     def __init__(self, n, s, h=1.0, device="cuda", dtype=_F64, loads=G.LOADS, precision="fp64"):
         self.n, self.s, self.h = n, s, h
@@ -118,8 +118,9 @@ class FineRefT:
         B = Kn.shape[0]
         up = self.bc.up[None].expand(B, -1, -1, -1)
         free = self.bc.free[None].expand(B, -1, -1)
-        if self.precision == "mixed":
-            u, info = self.op.solve_mixed(Kn4, Tv4, up, free, tol=tol)
+        if self.precision in ("mixed", "amg"):
+            solve = self.op.solve_mixed if self.precision == "mixed" else self.op.solve_amg
+            u, info = solve(Kn4, Tv4, up, free, tol=tol)
             it, rel = int(info.iters.max()), float(info.relres.max())
         else:
             u, it, rel = self.op.solve(Kn4, Tv4, up, free, tol)

@@ -12,6 +12,8 @@ Parts:
   sq     2D square: timing/t2d/solver2d.py kernels, cg2plain / pcg_mf solves, SuperLU, masked connectivity, BCs
   grad   gradients: torch_lpm3d autograd of lam . K u, LinSolve through CoarseT.run (as coarse3d/check_torch3d.py),
          torch_lpm dense-assembly gradient of lam^T K u and of the CoarseT.run losses (as coarse2d/check_gradient.py)
+  amg    aggregation AMG of timing/t3d/amg3d.py with the settings of timing/t3d/problems.py (geometry, levels, rho,
+         one cycle, PCG iterations; 14^3 and the 48^3 bench specimen) and geom3d.interface_cells
 """
 import os
 import subprocess
@@ -428,6 +430,10 @@ def part_amg():
     x, it, rel = h.pcg(b, 1e-8)
     out.update(a48_it=it, a48_rel=rel, a48_rho=np.array([h.rho0] + list(h.rho)),
                a48_g=np.array([geo.l0["g"]] + [L["gc"] for L in geo.levels], np.int64))
+    # interface cells (coarse3d/geom3d.py:134-147) of the 14^3 specimen and a 12^3 spheres image
+    ph12, _ = micro3d.spheres(12, 12, 12, 0.25, 2.0, np.random.default_rng(4), rjit=0.0)
+    out.update(iface_ph12=ph12.astype(np.int8), iface_12_2=G.interface_cells(ph12, 12, 2),
+               iface_12_3=G.interface_cells(ph12, 12, 3))
     np.savez_compressed(os.path.join(HERE, "golden_amg.npz"), **out)
     print("golden_amg.npz:", len(out), "arrays")
 

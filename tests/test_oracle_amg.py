@@ -67,3 +67,9 @@ def test_amg_iterations_48(gamg):
     b[fixed] = 0.0
     x, it, rel = h.pcg(b, 1e-8)
     assert it == int(gamg["a48_it"]) and abs(rel - float(gamg["a48_rel"])) < 1e-12
+
+
+def test_interface_cells(gamg):
+    """geom.interface_cells restates coarse3d/geom3d.py:134-147 (the iface_s arrays of data/fine_*.npz)."""
+    for s in (2, 3):
+        assert np.array_equal(G.interface_cells(gamg["iface_ph12"], 12, s), gamg["iface_12_%d" % s])
