@@ -80,6 +80,8 @@ typedef struct lpm_ir_opts {
     int32_t check;       /* inner convergence-test interval */
     int32_t poll;        /* inner host polling interval */
     double* prof;        /* optional HOST array of 4, as lpm_cg_opts.prof, for the FP32 inner solves */
+    int32_t x_is_zero;   /* 1: x is zero on entry, so the first residual is b (no FP64 K x) */
+    int32_t reserved;
 } lpm_ir_opts;
 
 int lpm_abi_version(void);

@@ -34,7 +34,7 @@ class CgOpts(ctypes.Structure):
 
 class IrOpts(ctypes.Structure):
     _fields_ = [("tol", _c_d), ("inner_tol", _c_d), ("maxit", _c_i32), ("max_outer", _c_i32), ("check", _c_i32),
-                ("poll", _c_i32), ("prof", _P(_c_d))]
+                ("poll", _c_i32), ("prof", _P(_c_d)), ("x_is_zero", _c_i32), ("reserved", _c_i32)]
 
 
 class AmgOpts(ctypes.Structure):

@@ -213,7 +213,7 @@ class AmgBatch:
         st = torch.zeros(self.nsys, dtype=torch.int32, device=bf.device)
         outer = ctypes.c_int32(0)
         opts = L.IrOpts(float(tol), float(inner_tol), int(maxit), int(max_outer), int(check), int(poll),
-                        core._prof_ptr(prof))
+                        core._prof_ptr(prof), 1, 0)
         L.check(lib.lpm_ir_amg(dl.ref, L.ptr(Kc), L.ptr(Tc), L.LAYOUT_SOA, self._h, ctypes.byref(b_),
                                L.ptr(self.mask), L.ptr(bf), L.ptr(xf), ctypes.byref(opts), L.ptr(ws), ws.numel(),
                                L.ptr(it), L.ptr(rel), L.ptr(st), ctypes.byref(outer), L.stream_ptr(bf.device)),

@@ -296,7 +296,7 @@ def ir(dl, Kn64, Tv64, b, x=None, free=None, tol=1e-8, inner_tol=1e-3, maxit=200
     st = torch.zeros(nsys, dtype=torch.int32, device=bf.device)
     outer = ctypes.c_int32(0)
     opts = L.IrOpts(float(tol), float(inner_tol), int(maxit), int(max_outer), int(check), int(poll),
-                    _prof_ptr(prof))
+                    _prof_ptr(prof), int(x is None), 0)
     L.check(lib.lpm_ir_batched(dl.ref, L.ptr(Kc), L.ptr(Tc), lay64, L.ptr(K32), L.ptr(T32), L.ptr(M32),
                                ctypes.byref(b_), L.ptr(m), L.ptr(bf), L.ptr(xf), ctypes.byref(opts), L.ptr(ws),
                                ws.numel(), L.ptr(it), L.ptr(rel), L.ptr(st), ctypes.byref(outer),

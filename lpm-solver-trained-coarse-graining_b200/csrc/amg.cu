@@ -439,51 +439,80 @@ __global__ void __launch_bounds__(VB) k_amg_pupdate(PairGeom G, const float* __r
     }
 }
 
-// Finest-level transfers.  A block covers TXA aggregates along x of one aggregate row (cy, cz) of a box, for one pair
-// of systems; thread (ia, rs) of the block takes aggregate ia of the tile and its site rows rs, rs + 8, ...; a site
-// row of an aggregate is a contiguous run of 24-byte sites (both systems of the pair), so a warp reads TXA consecutive
-// runs.
-constexpr int TXA = 32;
-
-struct AggRow {
-    int cx, cy, cz, sx, wx, sy, wy, sz, wz;
-    float isn, i3, i4, i5;
+// Finest-level transfers.  A block covers a tile of tw x th aggregates (x, y) of one aggregate layer cz of a box, for
+// one pair of systems.  Its work items are (site row r of the aggregates, aggregate): a site row is a contiguous run
+// of 24-byte sites (both systems of the pair), and consecutive items take consecutive aggregates of the same row, so
+// a warp reads consecutive runs.  Per-item partial sums meet in shared memory and are reduced in a fixed order.
+struct TileGeo {
+    int cx0, cy0, cz, na, nb, sz, wz, wymax;
 };
 
-__device__ __forceinline__ AggRow agg_row(const BoxDev& B, int a, int bx, int ia, bool& valid)
+__host__ __device__ inline TileGeo tile_geo(const int nch[3], const int L[3], int a, int tw, int th, int bx)
 {
-    AggRow g;
-    const int tiles_x = (B.nch[0] + TXA - 1) / TXA;
-    const int tx = bx % tiles_x, row = bx / tiles_x;
-    g.cy = row % B.nch[1];
-    g.cz = row / B.nch[1];
-    g.cx = tx * TXA + ia;
-    valid = g.cx < B.nch[0];
-    chunk_range(valid ? g.cx : 0, a, B.nch[0], B.L[0], g.sx, g.wx);
-    chunk_range(g.cy, a, B.nch[1], B.L[1], g.sy, g.wy);
-    chunk_range(g.cz, a, B.nch[2], B.L[2], g.sz, g.wz);
-    const float s2x = (float)(g.wx * g.wx - 1) / 12.f, s2y = (float)(g.wy * g.wy - 1) / 12.f,
-                s2z = (float)(g.wz * g.wz - 1) / 12.f;
-    const float n = (float)(g.wx * g.wy * g.wz);
-    g.isn = 1.f / sqrtf(n);
-    g.i3 = 1.f / sqrtf(n * (s2x + s2y));
-    g.i4 = 1.f / sqrtf(n * (s2y + s2z));
-    g.i5 = 1.f / sqrtf(n * (s2x + s2z));
-    return g;
+    TileGeo T;
+    const int tiles_x = (nch[0] + tw - 1) / tw, tiles_y = (nch[1] + th - 1) / th;
+    const int tx = bx % tiles_x, ty = (bx / tiles_x) % tiles_y;
+    T.cz = bx / (tiles_x * tiles_y);
+    T.cx0 = tx * tw;
+    T.cy0 = ty * th;
+    T.na = min(tw, nch[0] - T.cx0);
+    T.nb = min(th, nch[1] - T.cy0);
+    chunk_range(T.cz, a, nch[2], L[2], T.sz, T.wz);
+    int s0, wl;
+    chunk_range(T.cy0 + T.nb - 1, a, nch[1], L[1], s0, wl);
+    T.wymax = max(wl, T.nb > 1 ? a : wl);
+    return T;
 }
 
-inline int transfer_tiles(const int nch[3]) { return (nch[0] + TXA - 1) / TXA * nch[1] * nch[2]; }
+// tile shape (tw, th) for an aggregate grid nch over extents L, with the shared-memory bytes of one block
+struct TileShape {
+    int tw, th, tiles;
+    size_t smem;
+};
+
+inline TileShape tile_shape(const int nch[3], const int L[3], int a, int floats_per_item)
+{
+    int wy = 0, wz = 0;
+    for (int c = 0; c < nch[1]; ++c) {
+        int s0, w;
+        chunk_range(c, a, nch[1], L[1], s0, w);
+        wy = std::max(wy, w);
+    }
+    for (int c = 0; c < nch[2]; ++c) {
+        int s0, w;
+        chunk_range(c, a, nch[2], L[2], s0, w);
+        wz = std::max(wz, w);
+    }
+    const int rows = wy * wz;
+    const int cap = std::max(1, std::min(32, (48 * 1024) / (rows * floats_per_item * 4)));
+    TileShape t;
+    t.tw = std::min(nch[0], cap);
+    t.th = std::max(1, std::min(nch[1], cap / t.tw));
+    t.tiles = (nch[0] + t.tw - 1) / t.tw * ((nch[1] + t.th - 1) / t.th) * nch[2];
+    t.smem = (size_t)rows * t.tw * t.th * floats_per_item * 4;
+    return t;
+}
+
+__device__ __forceinline__ void agg_scales(int wx, int wy, int wz, float& isn, float& i3, float& i4, float& i5)
+{
+    const float s2x = (float)(wx * wx - 1) / 12.f, s2y = (float)(wy * wy - 1) / 12.f, s2z = (float)(wz * wz - 1) / 12.f;
+    const float n = (float)(wx * wy * wz);
+    isn = 1.f / sqrtf(n);
+    i3 = 1.f / sqrtf(n * (s2x + s2y));
+    i4 = 1.f / sqrtf(n * (s2y + s2z));
+    i5 = 1.f / sqrtf(n * (s2x + s2z));
+}
 
 // PROBE = false: B1[j][I] = P_I^T t for the lanes of pair entry (pr, j lane 0, j lane 1) that belong to this box
 // (j = -1: lane of another box).  PROBE = true: t is K of probe pair pr = set * PNP + jp of chunk `chunk`; writes
 // A1[set][d, :, mode][I] for the colour-class neighbour J = I + off(d) of each aggregate I.
 template <bool PROBE>
-__global__ void __launch_bounds__(256) k_restrict0(BoxDev B, int a, int nx, int ny, int64_t N,
+__global__ void __launch_bounds__(256) k_restrict0(BoxDev B, int a, int tw, int th, int nx, int ny, int64_t N,
                                                    const int* __restrict__ pent, const int* __restrict__ sys,
                                                    const int* __restrict__ act, const float* __restrict__ t, int chunk,
                                                    float* __restrict__ A1)
 {
-    __shared__ float red[8][TXA][13];
+    extern __shared__ float red[];
     int pr, jl[2];
     bool on0, on1;
     if constexpr (PROBE) {
@@ -498,20 +527,22 @@ __global__ void __launch_bounds__(256) k_restrict0(BoxDev B, int a, int nx, int 
         on1 = jl[1] >= 0 && (!act || act[sys[jl[1]]]);
         if (!on0 && !on1) return;
     }
-    const int ia = threadIdx.x & (TXA - 1), rs = threadIdx.x >> 5;
-    bool valid;
-    const AggRow g = agg_row(B, a, blockIdx.x, ia, valid);
-    float acc[2][6] = {{0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}};
-    if (valid) {
-        const int nrow = g.wy * g.wz;
-        for (int r = rs; r < nrow; r += 8) {
-            const int ry = r % g.wy, rz = r / g.wy;
-            const float dy = (float)ry - 0.5f * (float)(g.wy - 1), dz = (float)rz - 0.5f * (float)(g.wz - 1);
-            const int y = B.lo[1] + g.sy + ry, z = B.lo[2] + g.sz + rz;
+    const TileGeo T = tile_geo(B.nch, B.L, a, tw, th, blockIdx.x);
+    const int rows = T.wymax * T.wz, nab = T.na * T.nb;
+    for (int it = threadIdx.x; it < rows * nab; it += blockDim.x) {
+        const int ia = it % T.na, iy = (it / T.na) % T.nb, r = it / nab;
+        const int ry = r % T.wymax, rz = r / T.wymax;
+        int sx, wx, sy, wy;
+        chunk_range(T.cx0 + ia, a, B.nch[0], B.L[0], sx, wx);
+        chunk_range(T.cy0 + iy, a, B.nch[1], B.L[1], sy, wy);
+        float acc[2][6] = {{0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}};
+        if (ry < wy) {
+            const float dy = (float)ry - 0.5f * (float)(wy - 1), dz = (float)rz - 0.5f * (float)(T.wz - 1);
+            const int y = B.lo[1] + sy + ry, z = B.lo[2] + T.sz + rz;
             const float2* rowp = reinterpret_cast<const float2*>(
-                t + ((int64_t)pr * N + ((int64_t)z * ny + y) * nx + B.lo[0] + g.sx) * 6);
-            for (int px = 0; px < g.wx; ++px) {
-                const float dx = (float)px - 0.5f * (float)(g.wx - 1);
+                t + ((int64_t)pr * N + ((int64_t)z * ny + y) * nx + B.lo[0] + sx) * 6);
+            for (int px = 0; px < wx; ++px) {
+                const float dx = (float)px - 0.5f * (float)(wx - 1);
                 const float2 v0 = rowp[3 * px], v1 = rowp[3 * px + 1], v2 = rowp[3 * px + 2];
                 const float t0[2] = {v0.x, v0.y}, t1[2] = {v1.x, v1.y}, t2[2] = {v2.x, v2.y};
 #pragma unroll
@@ -525,29 +556,33 @@ __global__ void __launch_bounds__(256) k_restrict0(BoxDev B, int a, int nx, int 
                 }
             }
         }
+        float* o = red + (size_t)it * 12;
+#pragma unroll
+        for (int l = 0; l < 2; ++l)
+#pragma unroll
+            for (int k = 0; k < 6; ++k) o[l * 6 + k] = acc[l][k];
     }
-#pragma unroll
-    for (int l = 0; l < 2; ++l)
-#pragma unroll
-        for (int k = 0; k < 6; ++k) red[rs][ia][l * 6 + k] = acc[l][k];
     __syncthreads();
-    for (int o = threadIdx.x; o < TXA * 12; o += blockDim.x) {
-        const int ib = o / 12, l = (o % 12) / 6, c = o % 6;
+    for (int o = threadIdx.x; o < nab * 12; o += blockDim.x) {
+        const int ab = o / 12, l = (o % 12) / 6, c = o % 6;
         if (!(l ? on1 : on0)) continue;
-        bool vb;
-        const AggRow gb = agg_row(B, a, blockIdx.x, ib, vb);
-        if (!vb) continue;
+        const int ia = ab % T.na, iy = ab / T.na;
         float v = 0.f;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) v += red[q][ib][l * 6 + c];
-        v *= c < 3 ? gb.isn : (c == 3 ? gb.i3 : (c == 4 ? gb.i4 : gb.i5));
-        const int I = (gb.cz * B.nch[1] + gb.cy) * B.nch[0] + gb.cx;
+        for (int r = 0; r < rows; ++r) v += red[((size_t)r * nab + ab) * 12 + l * 6 + c];
+        int sx, wx, sy, wy;
+        chunk_range(T.cx0 + ia, a, B.nch[0], B.L[0], sx, wx);
+        chunk_range(T.cy0 + iy, a, B.nch[1], B.L[1], sy, wy);
+        float isn, i3, i4, i5;
+        agg_scales(wx, wy, T.wz, isn, i3, i4, i5);
+        v *= c < 3 ? isn : (c == 3 ? i3 : (c == 4 ? i4 : i5));
+        const int cx = T.cx0 + ia, cy = T.cy0 + iy;
+        const int I = (T.cz * B.nch[1] + cy) * B.nch[0] + cx;
         if constexpr (!PROBE) {
             B.B1[((int64_t)jl[l] * B.n1 + I) * 6 + c] = v;
         } else {
             const int set = pr / PNP, qq = 2 * (pr % PNP) + l;
             const int colq = chunk * PCOL + qq / 6, mode = qq % 6;
-            const int cc[3] = {gb.cx, gb.cy, gb.cz}, gcol[3] = {colq % 3, (colq / 3) % 3, colq / 9};
+            const int cc[3] = {cx, cy, T.cz}, gcol[3] = {colq % 3, (colq / 3) % 3, colq / 9};
             int off[3];
             bool ok = true;
 #pragma unroll
@@ -565,44 +600,44 @@ __global__ void __launch_bounds__(256) k_restrict0(BoxDev B, int a, int nx, int 
 }
 
 // v += P e1 on the lanes of pair entry (pr, j lane 0, j lane 1) that belong to this box; a lane of another box is never
-// written (4-byte stores when only one lane is in the box).
-__global__ void __launch_bounds__(256) k_prolong0(BoxDev B, int a, int nx, int ny, int64_t N,
+// written (4-byte stores when only one lane is in the box).  Tiled as k_restrict0, one item per site row.
+__global__ void __launch_bounds__(256) k_prolong0(BoxDev B, int a, int tw, int th, int nx, int ny, int64_t N,
                                                   const int* __restrict__ pent, const int* __restrict__ sys,
                                                   const int* __restrict__ act, float* __restrict__ v)
 {
     const int pr = pent[3 * blockIdx.y], j0 = pent[3 * blockIdx.y + 1], j1 = pent[3 * blockIdx.y + 2];
     const bool on0 = j0 >= 0 && (!act || act[sys[j0]]), on1 = j1 >= 0 && (!act || act[sys[j1]]);
     if (!on0 && !on1) return;
-    const int ia = threadIdx.x & (TXA - 1), rs = threadIdx.x >> 5;
-    bool valid;
-    const AggRow g = agg_row(B, a, blockIdx.x, ia, valid);
-    if (!valid) return;
-    const int I = (g.cz * B.nch[1] + g.cy) * B.nch[0] + g.cx;
-    float e[2][6];
+    const TileGeo T = tile_geo(B.nch, B.L, a, tw, th, blockIdx.x);
+    const int rows = T.wymax * T.wz, nab = T.na * T.nb;
+    for (int it = threadIdx.x; it < rows * nab; it += blockDim.x) {
+        const int ia = it % T.na, iy = (it / T.na) % T.nb, r = it / nab;
+        const int ry = r % T.wymax, rz = r / T.wymax;
+        int sx, wx, sy, wy;
+        chunk_range(T.cx0 + ia, a, B.nch[0], B.L[0], sx, wx);
+        chunk_range(T.cy0 + iy, a, B.nch[1], B.L[1], sy, wy);
+        if (ry >= wy) continue;
+        float isn, i3, i4, i5;
+        agg_scales(wx, wy, T.wz, isn, i3, i4, i5);
+        const int I = (T.cz * B.nch[1] + T.cy0 + iy) * B.nch[0] + T.cx0 + ia;
+        float f[2][6];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        e[0][k] = on0 ? B.E1[((int64_t)j0 * B.n1 + I) * 6 + k] : 0.f;
-        e[1][k] = on1 ? B.E1[((int64_t)j1 * B.n1 + I) * 6 + k] : 0.f;
-    }
-    // scaled coarse values: translations isn e0..e2, rotations i3 e3, i4 e4, i5 e5
-    float f[2][6];
-#pragma unroll
-    for (int l = 0; l < 2; ++l) {
-        f[l][0] = g.isn * e[l][0];
-        f[l][1] = g.isn * e[l][1];
-        f[l][2] = g.isn * e[l][2];
-        f[l][3] = g.i3 * e[l][3];
-        f[l][4] = g.i4 * e[l][4];
-        f[l][5] = g.i5 * e[l][5];
-    }
-    const int nrow = g.wy * g.wz;
-    for (int r = rs; r < nrow; r += 8) {
-        const int ry = r % g.wy, rz = r / g.wy;
-        const float dy = (float)ry - 0.5f * (float)(g.wy - 1), dz = (float)rz - 0.5f * (float)(g.wz - 1);
-        const int y = B.lo[1] + g.sy + ry, z = B.lo[2] + g.sz + rz;
-        float* rowp = v + ((int64_t)pr * N + ((int64_t)z * ny + y) * nx + B.lo[0] + g.sx) * 6;
-        for (int px = 0; px < g.wx; ++px) {
-            const float dx = (float)px - 0.5f * (float)(g.wx - 1);
+        for (int l = 0; l < 2; ++l) {
+            const int jj = l ? j1 : j0;
+            const bool on = l ? on1 : on0;
+            const float* e = B.E1 + ((int64_t)(on ? jj : 0) * B.n1 + I) * 6;
+            f[l][0] = on ? isn * e[0] : 0.f;
+            f[l][1] = on ? isn * e[1] : 0.f;
+            f[l][2] = on ? isn * e[2] : 0.f;
+            f[l][3] = on ? i3 * e[3] : 0.f;
+            f[l][4] = on ? i4 * e[4] : 0.f;
+            f[l][5] = on ? i5 * e[5] : 0.f;
+        }
+        const float dy = (float)ry - 0.5f * (float)(wy - 1), dz = (float)rz - 0.5f * (float)(T.wz - 1);
+        const int y = B.lo[1] + sy + ry, z = B.lo[2] + T.sz + rz;
+        float* rowp = v + ((int64_t)pr * N + ((int64_t)z * ny + y) * nx + B.lo[0] + sx) * 6;
+        for (int px = 0; px < wx; ++px) {
+            const float dx = (float)px - 0.5f * (float)(wx - 1);
             float add[2][3];
 #pragma unroll
             for (int l = 0; l < 2; ++l) {
@@ -639,11 +674,11 @@ __global__ void __launch_bounds__(VB) k_probe_gen(BoxDev B, int a, int nx, int n
     const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((int64_t)nx * ny));
     Agg g;
     const bool in = agg_at(B, a, x, y, z, g);
-    int col = -1;
-    if (in) {
-        const int cx = g.I % B.nch[0], cy = (g.I / B.nch[0]) % B.nch[1], cz = g.I / (B.nch[0] * B.nch[1]);
-        col = (cz % 3) * 9 + (cy % 3) * 3 + cx % 3;
-    }
+    if (!in) return;  // zero from the memset before the first chunk
+    const int cx = g.I % B.nch[0], cy = (g.I / B.nch[0]) % B.nch[1], cz = g.I / (B.nch[0] * B.nch[1]);
+    const int col = (cz % 3) * 9 + (cy % 3) * 3 + cx % 3;
+    // the sites of other colour classes hold zero already: write this chunk's classes and clear the previous chunk's
+    if (col / PCOL != chunk && col / PCOL != chunk - 1) return;
     float val[2][3];
 #pragma unroll
     for (int l = 0; l < 2; ++l) {
@@ -923,31 +958,28 @@ __global__ void __launch_bounds__(LB) k_lv_prolong(int gx, int gy, int gz, int c
     }
 }
 
-// bc[j][J] = sum over the nodes m of coarse node J of Q_m^T r[j][m]   (amg3d.py:298-310).  A block covers TXA coarse
-// nodes along x of one coarse row (Cy, Cz) for system j; thread (ia, rs) takes coarse node ia of the tile and its
-// member rows rs, rs + 8, ... -- runs of consecutive nodes, so both r (24 bytes per node) and Q (144 bytes per node)
-// are read contiguously across the warp.
+// bc[j][J] = sum over the nodes m of coarse node J of Q_m^T r[j][m]   (amg3d.py:298-310), for system j, tiled as the
+// finest-level restriction: items are runs of consecutive fine nodes (24 bytes of r and 144 bytes of Q per node).
 __global__ void __launch_bounds__(256) k_lv_restrict(int gx, int gy, int gz, int n, int cx, int cy, int cz, int a,
-                                                     const float* __restrict__ Q, const int* __restrict__ sys,
-                                                     const int* __restrict__ act, const float* __restrict__ r,
-                                                     float* __restrict__ bc)
+                                                     int tw, int th, const float* __restrict__ Q,
+                                                     const int* __restrict__ sys, const int* __restrict__ act,
+                                                     const float* __restrict__ r, float* __restrict__ bc)
 {
-    __shared__ float red[8][TXA][7];
+    extern __shared__ float red[];
     const int j = blockIdx.y;
     if (act && !act[sys[j]]) return;
-    const int ia = threadIdx.x & (TXA - 1), rs = threadIdx.x >> 5;
-    const int tiles_x = (cx + TXA - 1) / TXA;
-    const int tx = blockIdx.x % tiles_x, row = blockIdx.x / tiles_x;
-    const int Cy = row % cy, Cz = row / cy, Cx = tx * TXA + ia;
-    const bool valid = Cx < cx;
-    int sx, wx, sy, wy, sz, wz;
-    chunk_range(valid ? Cx : 0, a, cx, gx, sx, wx);
-    chunk_range(Cy, a, cy, gy, sy, wy);
-    chunk_range(Cz, a, cz, gz, sz, wz);
-    float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (valid) {
-        for (int rr = rs; rr < wy * wz; rr += 8) {
-            const int m0 = ((sz + rr / wy) * gy + sy + rr % wy) * gx + sx;
+    const int nch[3] = {cx, cy, cz}, L[3] = {gx, gy, gz};
+    const TileGeo T = tile_geo(nch, L, a, tw, th, blockIdx.x);
+    const int rows = T.wymax * T.wz, nab = T.na * T.nb;
+    for (int it = threadIdx.x; it < rows * nab; it += blockDim.x) {
+        const int ia = it % T.na, iy = (it / T.na) % T.nb, rr = it / nab;
+        const int ry = rr % T.wymax, rz = rr / T.wymax;
+        int sx, wx, sy, wy;
+        chunk_range(T.cx0 + ia, a, cx, gx, sx, wx);
+        chunk_range(T.cy0 + iy, a, cy, gy, sy, wy);
+        float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (ry < wy) {
+            const int m0 = ((T.sz + rz) * gy + sy + ry) * gx + sx;
             for (int px = 0; px < wx; ++px) {
                 const float* rv = r + ((int64_t)j * n + m0 + px) * 6;
                 const float* q = Q + (int64_t)(m0 + px) * 36;
@@ -960,17 +992,17 @@ __global__ void __launch_bounds__(256) k_lv_restrict(int gx, int gy, int gz, int
                     for (int c = 0; c < 6; ++c) acc[c] += q[k * 6 + c] * rl[k];
             }
         }
+        float* o = red + (size_t)it * 6;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) o[c] = acc[c];
     }
-#pragma unroll
-    for (int c = 0; c < 6; ++c) red[rs][ia][c] = acc[c];
     __syncthreads();
-    for (int o = threadIdx.x; o < TXA * 6; o += blockDim.x) {
-        const int ib = o / 6, c = o % 6, Cxb = tx * TXA + ib;
-        if (Cxb >= cx) continue;
+    for (int o = threadIdx.x; o < nab * 6; o += blockDim.x) {
+        const int ab = o / 6, c = o % 6;
+        const int ia = ab % T.na, iy = ab / T.na;
         float v = 0.f;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) v += red[q][ib][c];
-        bc[((int64_t)j * cx * cy * cz + (Cz * cy + Cy) * cx + Cxb) * 6 + c] = v;
+        for (int rr = 0; rr < rows; ++rr) v += red[((size_t)rr * nab + ab) * 6 + c];
+        bc[((int64_t)j * cx * cy * cz + (T.cz * cy + T.cy0 + iy) * cx + T.cx0 + ia) * 6 + c] = v;
     }
 }
 
@@ -1119,7 +1151,7 @@ __global__ void __launch_bounds__(LB) k_pow_lv_step(int n, const float* __restri
 }
 
 // Ac[set][dd][:, :, J] = sum over nodes m of J and stencil offsets d of Q_m^T A[set][d][m] Q_{m+d}
-// (amg3d.py:253-295); one block per (coarse node, set), FP64 accumulation in shared memory.
+// (amg3d.py:253-295); one block per (coarse node, set), FP32 products accumulated in FP64 in shared memory.
 __global__ void __launch_bounds__(256) k_galerkin(int gx, int gy, int gz, int cx, int cy, int cz, int a,
                                                   const float* __restrict__ A, const float* __restrict__ Q,
                                                   float* __restrict__ Ac)
@@ -1143,21 +1175,29 @@ __global__ void __launch_bounds__(256) k_galerkin(int gx, int gy, int gz, int cx
         const int Jx = chunk_of(nxq, a, cx), Jy = chunk_of(nyq, a, cy), Jz = chunk_of(nzq, a, cz);
         const int dd = ((Jz - c[2] + 1) * 3 + Jy - c[1] + 1) * 3 + Jx - c[0] + 1;
         const float* Ad = A + ((int64_t)set * ST + d * 36) * n + m;
-        double Ab[36], Cq[36];
-        for (int e = 0; e < 36; ++e) Ab[e] = (double)Ad[(int64_t)e * n];
+        float Ab[36], Cq[36];
+#pragma unroll
+        for (int e = 0; e < 36; ++e) Ab[e] = __ldg(Ad + (int64_t)e * n);
         const float* Qm = Q + (int64_t)m * 36;
         const float* Qq = Q + (int64_t)q * 36;
+#pragma unroll
         for (int r = 0; r < 6; ++r)  // C = A Q_q
+#pragma unroll
             for (int cc = 0; cc < 6; ++cc) {
-                double s = 0.0;
-                for (int b = 0; b < 6; ++b) s += Ab[r * 6 + b] * (double)Qq[b * 6 + cc];
+                float s = 0.f;
+#pragma unroll
+                for (int b = 0; b < 6; ++b) s += Ab[r * 6 + b] * __ldg(Qq + b * 6 + cc);
                 Cq[r * 6 + cc] = s;
             }
-        for (int r = 0; r < 6; ++r)  // Q_m^T C
+        // Q_m^T C in FP32, accumulated over the members and offsets in FP64
+#pragma unroll
+        for (int r = 0; r < 6; ++r)
+#pragma unroll
             for (int cc = 0; cc < 6; ++cc) {
-                double s = 0.0;
-                for (int b = 0; b < 6; ++b) s += (double)Qm[b * 6 + r] * Cq[b * 6 + cc];
-                atomicAdd(&acc[dd * 36 + r * 6 + cc], s);
+                float s = 0.f;
+#pragma unroll
+                for (int b = 0; b < 6; ++b) s += __ldg(Qm + b * 6 + r) * Cq[b * 6 + cc];
+                atomicAdd(&acc[dd * 36 + r * 6 + cc], (double)s);
             }
     }
     __syncthreads();
@@ -1337,6 +1377,7 @@ struct lpm_amg {
     struct Level {
         int g[3] = {0, 0, 0};
         int n = 0;
+        lpm::TileShape tr{};  // tiles of the restriction to the next level
         float *A = nullptr, *Minv = nullptr, *Q = nullptr, *w = nullptr;
         double* rho = nullptr;
         float *B = nullptr, *E = nullptr, *RB = nullptr, *X = nullptr, *X2 = nullptr, *T = nullptr;
@@ -1352,7 +1393,7 @@ struct lpm_amg {
         int* sys = nullptr;
         std::vector<int> sys_h;
         int ngrp = 0, npent = 0;
-        int tiles = 1;              // blocks of the finest-level transfers (x tiles x aggregate rows)
+        lpm::TileShape t0{};        // tiles of the finest-level transfers
         float* Ainv32 = nullptr;    // FP32 copy of the dense inverse, applied in the cycle
         int *grp = nullptr, *pent = nullptr;  // system groups (set, j0, cnt); pair entries (pr, j lane 0, j lane 1)
         std::vector<int> grp_h, pent_h;
@@ -1639,9 +1680,9 @@ cudaError_t vc(const CycleCtx& C, int l, const float* rhs, float* out, int acc)
     }
     k_lv_op<1><<<gg, LB, 0, C.st>>>(V, b.grp, b.sys, C.act, x, rhs, Lv.T, 0);
     const auto& Cl = b.lev[l + 1];
-    k_lv_restrict<<<dim3(transfer_tiles(Cl.g), b.nsb), 256, 0, C.st>>>(Lv.g[0], Lv.g[1], Lv.g[2], Lv.n, Cl.g[0],
-                                                                        Cl.g[1], Cl.g[2], h.o.agg, Lv.Q, b.sys, C.act,
-                                                                        Lv.T, Cl.B);
+    k_lv_restrict<<<dim3(Lv.tr.tiles, b.nsb), 256, Lv.tr.smem, C.st>>>(Lv.g[0], Lv.g[1], Lv.g[2], Lv.n, Cl.g[0],
+                                                                         Cl.g[1], Cl.g[2], h.o.agg, Lv.tr.tw, Lv.tr.th,
+                                                                         Lv.Q, b.sys, C.act, Lv.T, Cl.B);
     cudaError_t e = coarse(C, l + 1);
     if (e != cudaSuccess) return e;
     k_lv_prolong<<<g, LB, 0, C.st>>>(Lv.g[0], Lv.g[1], Lv.g[2], Cl.g[0], Cl.g[1], Cl.g[2], h.o.agg, Lv.Q, b.sys, h.rps,
@@ -1694,14 +1735,14 @@ cudaError_t fine_cycle(const lpm_amg& h, const FcgScalars& sc, bool dot, cudaStr
         B.n1 = b.lev[0].n;
         B.B1 = b.lev[0].B;
         B.E1 = b.lev[0].E;
-        k_restrict0<false><<<dim3(b.tiles, b.npent), 256, 0, sb>>>(B, h.o.agg, h.L.nx, h.L.ny, h.L.N, b.pent, b.sys,
-                                                                   sc.act, h.Ap, 0, nullptr);
+        k_restrict0<false><<<dim3(b.t0.tiles, b.npent), 256, b.t0.smem, sb>>>(
+            B, h.o.agg, b.t0.tw, b.t0.th, h.L.nx, h.L.ny, h.L.N, b.pent, b.sys, sc.act, h.Ap, 0, nullptr);
         CycleCtx C{&h, &b, sc.act, sb};
         if ((e = coarse(C, 0)) != cudaSuccess) return e;
         // lanes of other boxes are never written, so the boxes' prolongations may run concurrently
         B.E1 = b.lev[0].E;
-        k_prolong0<<<dim3(b.tiles, b.npent), 256, 0, sb>>>(B, h.o.agg, h.L.nx, h.L.ny, h.L.N, b.pent, b.sys, sc.act,
-                                                           h.v);
+        k_prolong0<<<dim3(b.t0.tiles, b.npent), 256, 0, sb>>>(B, h.o.agg, b.t0.tw, b.t0.th, h.L.nx, h.L.ny, h.L.N,
+                                                              b.pent, b.sys, sc.act, h.v);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         if (fork) {
             if ((e = cudaEventRecord(h.bev[1 + bi], sb)) != cudaSuccess) return e;
@@ -1773,11 +1814,12 @@ int amg_setup(lpm_amg& h, const float* Kn, const float* Tv, const float* Minv, c
         a.variant = pair_variant(h.L.nx, h.L.ny, h.L.nz, a.npair);
         a.u = pv;
         a.out = py;
+        if ((e = cudaMemsetAsync(pv, 0, sizeof(float) * (size_t)h.nset * PNP * N * 6, st)) != cudaSuccess) return (int)e;
         for (int chunk = 0; chunk < 27 / PCOL; ++chunk) {
             k_probe_gen<<<grid2(N, VB, h.nset * PNP), VB, 0, st>>>(B, h.o.agg, h.L.nx, h.L.ny, N, chunk, pv);
             if ((e = launch_sc_pair_mode(a, PM_NONE, st)) != cudaSuccess) return (int)e;
-            k_restrict0<true><<<dim3(b.tiles, h.nset * PNP), 256, 0, st>>>(B, h.o.agg, h.L.nx, h.L.ny, N, nullptr,
-                                                                           nullptr, nullptr, py, chunk, L1.A);
+            k_restrict0<true><<<dim3(b.t0.tiles, h.nset * PNP), 256, b.t0.smem, st>>>(
+                B, h.o.agg, b.t0.tw, b.t0.th, h.L.nx, h.L.ny, N, nullptr, nullptr, nullptr, py, chunk, L1.A);
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
         // ---- levels below: block inverses, rho, Galerkin products
@@ -2024,7 +2066,8 @@ int lpm_amg_create(const lpm_lattice* lat, const lpm_batch* batch, const int32_t
             delete h;
             return rc;
         }
-        b.tiles = transfer_tiles(b.nch);
+        b.t0 = tile_shape(b.nch, b.L, o.agg, 12);
+        for (int l = 0; l + 1 < b.nlev; ++l) b.lev[l].tr = tile_shape(b.lev[l + 1].g, b.lev[l].g, o.agg, 6);
     }
     if (!pair_supported(lat->nx)) {  // the finest level runs on the pair-packed TMA operator
         delete h;

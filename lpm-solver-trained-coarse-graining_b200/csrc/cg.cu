@@ -543,7 +543,7 @@ int ir_solve(const Lattice& L, const double* Kn64, const double* Tv64, const Coe
     if (e != cudaSuccess) return (int)e;
     const int nb = vec_blocks(N);
     int steps = 0, rc = LPM_OK;
-    bool x_zero = false;
+    bool x_zero = o.x_is_zero != 0;
     for (int k = 0;; ++k) {
         // true residual in FP64
         if (!x_zero) {
@@ -571,9 +571,11 @@ int ir_solve(const Lattice& L, const double* Kn64, const double* Tv64, const Coe
             const int nss = ns - s0 < 65535 ? ns - s0 : 65535;
             const dim3 g(nb, nss);
             if (L.dim == 3)
-                k_ir_residual<3><<<g, VB, 0, st>>>(N, s0, bt, b, w.Kx, mask, w.r64, w.part, w.cnt, rn2, bn2);
+                k_ir_residual<3><<<g, VB, 0, st>>>(N, s0, bt, b, x_zero ? nullptr : w.Kx, mask, w.r64, w.part,
+                                                   w.cnt, rn2, bn2);
             else
-                k_ir_residual<2><<<g, VB, 0, st>>>(N, s0, bt, b, w.Kx, mask, w.r64, w.part, w.cnt, rn2, bn2);
+                k_ir_residual<2><<<g, VB, 0, st>>>(N, s0, bt, b, x_zero ? nullptr : w.Kx, mask, w.r64, w.part,
+                                                   w.cnt, rn2, bn2);
         }
         e = cudaMemcpyAsync(h.data(), w.scal, sizeof(double) * 2 * ns, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);

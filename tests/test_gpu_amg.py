@@ -151,3 +151,36 @@ def test_amg3d_mirror(case24):
     assert relmax(ups[0] + x, uref) < 1e-6
     z = h.vcycle(b)
     assert z.shape == b.shape and np.isfinite(z).all()
+
+
+def test_repeated_solves_with_reused_workspace(case24):
+    """Back-to-back solves reuse the caching allocator's blocks: a solve must not depend on what an earlier solve left
+    in its workspace (the zero start skips the first FP64 K x)."""
+    ab, lat, Kn, Tv = case24["ab"], case24["lat"], case24["Kn"], case24["Tv"]
+    ups, free = case24["ups"], case24["free"]
+    b = torch.as_tensor(np.stack([-O.sc_apply(lat, ups[k], Kn, Tv) * free[k][:, None] for k in range(3)]),
+                        device="cuda")
+    x1, i1 = ab.ir(case24["Kd"], case24["Td"], b, tol=1e-8)
+    x2, i2 = ab.ir(case24["Kd"], case24["Td"], 3.0 * b, tol=1e-8)
+    x3, i3 = ab.ir(case24["Kd"], case24["Td"], b, tol=1e-8)
+    for i in (i1, i2, i3):
+        assert (i.status == 0).all() and (i.relres <= 1e-8).all() and (i.iters > 0).all()
+    assert relmax(x2.cpu().numpy(), 3.0 * x1.cpu().numpy()) < 1e-7
+    assert relmax(x3.cpu().numpy(), x1.cpu().numpy()) < 1e-12
+
+
+def test_core_ir_repeated_solves():
+    """The block-Jacobi mixed solve (core.ir) twice on one batch: the second from zero again, same answer."""
+    n = 16
+    lat, Kn, Tv = specimen(n, 7, 2.5)
+    free, ups = bcs(lat, n)
+    dl = core.DeviceLattice(lat, "cuda")
+    Kd = torch.as_tensor(Kn, device="cuda")[None, None]
+    Td = torch.as_tensor(Tv, device="cuda")[None, None]
+    upd = torch.as_tensor(ups, device="cuda")[None]
+    fr = torch.as_tensor(free, device="cuda", dtype=torch.float64)
+    b = -core.kmv(dl, upd, Kd, Td) * fr[None, :, :, None]
+    x1, i1 = core.ir(dl, Kd, Td, b, free=fr, tol=1e-8)
+    x2, i2 = core.ir(dl, Kd, Td, 2.0 * b, free=fr, tol=1e-8)
+    assert (i1.status == 0).all() and (i2.status == 0).all() and (i2.iters > 0).all()
+    assert relmax(x2.cpu().numpy(), 2.0 * x1.cpu().numpy()) < 1e-7
