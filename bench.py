@@ -411,7 +411,7 @@ def plain2d_specimens(seeds, n=128):
 def run_plain2d(a):
     """cfg 1: FP64 unpreconditioned CG to rel. residual 1e-10 on ten 128^2 specimens (one batched solve per step)."""
     import torch
-    from lpm_b200 import core
+    from lpm_b200 import _lib as L, core
     if int(os.environ.get("RANK", "0")) != 0:
         return
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
@@ -424,9 +424,10 @@ def run_plain2d(a):
     up = torch.as_tensor(np.where(fixed, up_h, 0.0), device=dev)
     B = len(seeds)
 
-    def step(Kn, Tv, free, up):
+    def step(Kn, Tv, free, up, engine=L.ENGINE_AUTO):
         b = -core.kmv(dl, up[None].expand(B, -1, -1), Kn, Tv) * free
-        x, info = core.cg(dl, Kn, Tv, b, free=free, tol=1e-10, maxit=200000, check=1, poll=50, precheck=True)
+        x, info = core.cg(dl, Kn, Tv, b, free=free, tol=1e-10, maxit=200000, check=1, poll=50, precheck=True,
+                          engine=engine)
         return up + x, info
 
     for _ in range(max(a.warmup, 3)):
@@ -453,6 +454,16 @@ def run_plain2d(a):
     ev1.record()
     torch.cuda.synchronize(dev)
     ms_e2e = ev0.elapsed_time(ev1)
+    # comparator: the same solves on the graph-launched engine (one launch per step, host polls)
+    engine = "persistent" if L.load().lpm_cg_persistent_fits(dl.ref, core._batch(B, 1, B)) else "launched"
+    step(Kn, Tv, free, up, L.ENGINE_LAUNCHED)
+    torch.cuda.synchronize(dev)
+    ev0.record()
+    for _ in range(a.steps):
+        _, linfo = step(Kn, Tv, free, up, L.ENGINE_LAUNCHED)
+    ev1.record()
+    torch.cuda.synchronize(dev)
+    ms_launched = ev0.elapsed_time(ev1)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     O.set_threads(os.cpu_count() or 1)
@@ -467,7 +478,8 @@ def run_plain2d(a):
             "data": "synthetic (seeded Gaussian random fields, shapes of the 128^2 config)",
             "config": {"workload": "2D square 128^2 GRF corr6 phi0.30 contrast10 nu0.25 plane stress, uniaxial "
                                    "tension, FP64 plain CG to 1e-10 (cg2plain semantics)", "specimens": B,
-                       "l2": "L2-resident (%.1f MB of FP64 coefficients)" % (Kn_h.nbytes * 2 / 1e6)},
+                       "l2": "L2-resident (%.1f MB of FP64 coefficients)" % (Kn_h.nbytes * 2 / 1e6),
+                       "engine": engine},
             "iters_mean": float(its.mean()), "all_converged": bool((info.status == 0).all()),
             "kmv_effective_gbs": None,
             "e2e": {"value": B * a.steps / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(Kp.numel() * 16),
@@ -475,6 +487,8 @@ def run_plain2d(a):
             "cpu_baseline": {"value": 1.0 / cpu_s, "unit": UNIT, "cores": O.get_threads(), "kind": "port",
                              "sample": "specimen 0 by the C oracle's plain CG (timing/t2d/cg2plain.py:11-68), "
                                        "%d iterations, %.2f s" % (cinfo["iters"], cpu_s)},
+            "launched_engine": {"solves_per_s": B * a.steps / (ms_launched / 1e3),
+                                "iters_mean": float(linfo.iters.mean())},
             "clocks": clocks}
     line["kmv_effective_gbs"] = bytes_per_it * float(its.max()) / (ms / a.steps / 1e3) / 1e9
     print(json.dumps(line), flush=True)

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define LPM_ABI_VERSION 3
+#define LPM_ABI_VERSION 4
 
 /* return codes */
 #define LPM_OK 0
@@ -41,6 +41,11 @@ extern "C" {
 #define LPM_STATUS_OK 0
 #define LPM_STATUS_NOT_CONVERGED 1 /* maxit reached (mirrors lin3d._pcg returning maxit, solver2d's iters = -1) */
 #define LPM_STATUS_BREAKDOWN 2     /* p.Ap < 0 or a non-finite scalar (mirrors torch_lpm's FloatingPointError) */
+
+/* CG engines (lpm_cg_opts.engine, lpm_ir_opts.engine) */
+#define LPM_ENGINE_AUTO 0       /* persistent where lpm_cg_persistent_fits says so and no timing is asked, else launched */
+#define LPM_ENGINE_LAUNCHED 1   /* one launch per step; iteration blocks replayed as CUDA graphs, host polls */
+#define LPM_ENGINE_PERSISTENT 2 /* one cooperative launch runs the whole solve (small batches) */
 
 /* precisions and coefficient layouts */
 #define LPM_F64 0
@@ -70,6 +75,8 @@ typedef struct lpm_cg_opts {
     int32_t precheck; /* 1: test the initial residual before iterating (cg2plain.cg_mf / solver2d.pcg_mf) */
     double* prof;     /* optional HOST array of 4: K.u ms / launches, and the same for full-batch launches */
     const double* tol_sys; /* optional DEVICE array (nsys): per-system tolerance used instead of tol */
+    int32_t engine;   /* LPM_ENGINE_*: 0 = auto */
+    int32_t reserved;
 } lpm_cg_opts;
 
 typedef struct lpm_ir_opts {
@@ -81,7 +88,7 @@ typedef struct lpm_ir_opts {
     int32_t poll;        /* inner host polling interval */
     double* prof;        /* optional HOST array of 4, as lpm_cg_opts.prof, for the FP32 inner solves */
     int32_t x_is_zero;   /* 1: x is zero on entry, so the first residual is b (no FP64 K x) */
-    int32_t reserved;
+    int32_t engine;      /* LPM_ENGINE_* of the FP32 inner solves: 0 = auto */
 } lpm_ir_opts;
 
 int lpm_abi_version(void);
@@ -149,6 +156,12 @@ int lpm_cg_batched_f32(const lpm_lattice* lat, const float* Kn, const float* Tv,
                        const lpm_batch* batch, const float* Minv, const uint8_t* mask, const float* b, float* x,
                        int32_t x_is_zero, const lpm_cg_opts* opts, void* workspace, size_t workspace_bytes,
                        int32_t* iters, double* relres, int32_t* status, void* stream);
+
+/* 1 if the automatic engine choice runs this batch on the persistent engine: square-lattice batches of at most 2^20
+ * particle-systems that fit on teams of co-resident blocks (every system's particles on one team).  The persistent engine keeps the launched engine's algorithm, tests and
+ * freezing (same iteration counts up to the rounding of its reductions) and runs one cooperative kernel per solve:
+ * three team barriers per iteration, each wait bounded in time (LPM_ERR_TIMEOUT on expiry). */
+int lpm_cg_persistent_fits(const lpm_lattice* lat, const lpm_batch* batch);
 
 /* ------------------------------------------------------------------------------- mixed-precision refinement */
 int64_t lpm_ir_workspace_bytes(const lpm_lattice* lat, const lpm_batch* batch, int32_t precond);

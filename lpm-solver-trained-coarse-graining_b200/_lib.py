@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(HERE, "liblpm_b200.so")
 
 LPM_F64, LPM_F32 = 0, 1
 LAYOUT_REF, LAYOUT_SOA = 0, 1
+ENGINE_AUTO, ENGINE_LAUNCHED, ENGINE_PERSISTENT = 0, 1, 2
 STATUS_OK, STATUS_NOT_CONVERGED, STATUS_BREAKDOWN = 0, 1, 2
 
 _c_i32, _c_i64, _c_p, _c_sz, _c_d = ctypes.c_int32, ctypes.c_int64, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_double
@@ -29,12 +30,12 @@ class Batch(ctypes.Structure):
 
 class CgOpts(ctypes.Structure):
     _fields_ = [("tol", _c_d), ("maxit", _c_i32), ("check", _c_i32), ("poll", _c_i32), ("precheck", _c_i32),
-                ("prof", _P(_c_d)), ("tol_sys", _c_p)]
+                ("prof", _P(_c_d)), ("tol_sys", _c_p), ("engine", _c_i32), ("reserved", _c_i32)]
 
 
 class IrOpts(ctypes.Structure):
     _fields_ = [("tol", _c_d), ("inner_tol", _c_d), ("maxit", _c_i32), ("max_outer", _c_i32), ("check", _c_i32),
-                ("poll", _c_i32), ("prof", _P(_c_d)), ("x_is_zero", _c_i32), ("reserved", _c_i32)]
+                ("poll", _c_i32), ("prof", _P(_c_d)), ("x_is_zero", _c_i32), ("engine", _c_i32)]
 
 
 class AmgOpts(ctypes.Structure):
@@ -56,6 +57,7 @@ _SIGS = {
     "lpm_block_jacobi_f64": ([_P(Lattice), _c_p, _c_p, _c_i32, _c_i32, _c_p, _c_p, _c_p], ctypes.c_int),
     "lpm_block_jacobi_f32": ([_P(Lattice), _c_p, _c_p, _c_i32, _c_i32, _c_p, _c_p, _c_p], ctypes.c_int),
     "lpm_cg_workspace_bytes": ([_P(Lattice), _P(Batch), _c_i32, _c_i32], _c_i64),
+    "lpm_cg_persistent_fits": ([_P(Lattice), _P(Batch)], ctypes.c_int),
     "lpm_cg_batched_f64": ([_P(Lattice), _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p, _c_p, _c_p, _c_i32, _P(CgOpts),
                             _c_p, _c_sz, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
     "lpm_cg_batched_f32": ([_P(Lattice), _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p, _c_p, _c_p, _c_i32, _P(CgOpts),

@@ -223,12 +223,13 @@ class SolveInfo:
 
 
 def cg(dl, Kn, Tv, b, x=None, Minv=None, free=None, tol=1e-10, maxit=20000, check=1, poll=None, precheck=False,
-       layout=L.LAYOUT_REF, rhs_per_set=None, prof=None):
+       layout=L.LAYOUT_REF, rhs_per_set=None, prof=None, engine=L.ENGINE_AUTO):
     """Batched (P)CG on the free DOFs.  b (..., N, d) zero on fixed DOFs; x start (zero if None), returned updated.
 
     dtype of b decides the precision (float64 or float32); Kn/Tv/Minv must match it.  With rhs_per_set given, Kn/Tv
     are the coefficient sets themselves ((nset, N, NN) for the reference layout, packed for SoA), systems
-    s*rhs_per_set .. (s+1)*rhs_per_set-1 using set s.  Returns (x, SolveInfo).
+    s*rhs_per_set .. (s+1)*rhs_per_set-1 using set s.  engine: L.ENGINE_AUTO / ENGINE_LAUNCHED / ENGINE_PERSISTENT
+    (one cooperative kernel per solve, small batches).  Returns (x, SolveInfo).
     """
     lead = b.shape[:-2]
     bf = _flat_vec(b, dl)
@@ -257,7 +258,7 @@ def cg(dl, Kn, Tv, b, x=None, Minv=None, free=None, tol=1e-10, maxit=20000, chec
     rel = torch.zeros(nsys, dtype=_F64, device=bf.device)
     st = torch.zeros(nsys, dtype=torch.int32, device=bf.device)
     opts = L.CgOpts(float(tol), int(maxit), int(check), int(poll or max(check, 10)), int(bool(precheck)),
-                    _prof_ptr(prof), None)
+                    _prof_ptr(prof), None, int(engine), 0)
     fn = lib.lpm_cg_batched_f64 if prec == L.LPM_F64 else lib.lpm_cg_batched_f32
     L.check(fn(dl.ref, L.ptr(Kc), L.ptr(Tc), layout, ctypes.byref(b_), L.ptr(Minv), L.ptr(m), L.ptr(bf), L.ptr(xf),
                int(x0_zero), ctypes.byref(opts), L.ptr(ws), ws.numel(), L.ptr(it), L.ptr(rel), L.ptr(st),
@@ -267,10 +268,11 @@ def cg(dl, Kn, Tv, b, x=None, Minv=None, free=None, tol=1e-10, maxit=20000, chec
 
 
 def ir(dl, Kn64, Tv64, b, x=None, free=None, tol=1e-8, inner_tol=1e-3, maxit=20000, max_outer=20, check=1,
-       poll=10, precond=True, packed=None, prof=None):
+       poll=10, precond=True, packed=None, prof=None, engine=L.ENGINE_AUTO):
     """Mixed-precision solve: FP32 inner PCG, FP64 iterative refinement to |b - K x| <= tol |b| (FP64 operator).
 
     b (..., N, d) float64, zero on fixed DOFs.  `packed` may pass a precomputed (Kn32, Tv32, Minv32) triple.
+    engine selects the inner solves' CG engine (see cg).
     Returns (x, SolveInfo) with total inner iterations and the final FP64 relative residual per system.
     """
     lead = b.shape[:-2]
@@ -296,7 +298,7 @@ def ir(dl, Kn64, Tv64, b, x=None, free=None, tol=1e-8, inner_tol=1e-3, maxit=200
     st = torch.zeros(nsys, dtype=torch.int32, device=bf.device)
     outer = ctypes.c_int32(0)
     opts = L.IrOpts(float(tol), float(inner_tol), int(maxit), int(max_outer), int(check), int(poll),
-                    _prof_ptr(prof), int(x is None), 0)
+                    _prof_ptr(prof), int(x is None), int(engine))
     L.check(lib.lpm_ir_batched(dl.ref, L.ptr(Kc), L.ptr(Tc), lay64, L.ptr(K32), L.ptr(T32), L.ptr(M32),
                                ctypes.byref(b_), L.ptr(m), L.ptr(bf), L.ptr(xf), ctypes.byref(opts), L.ptr(ws),
                                ws.numel(), L.ptr(it), L.ptr(rel), L.ptr(st), ctypes.byref(outer),

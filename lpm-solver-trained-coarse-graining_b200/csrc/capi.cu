@@ -242,6 +242,14 @@ int64_t lpm_cg_workspace_bytes(const lpm_lattice* lat, const lpm_batch* batch, i
     return (int64_t)cg_workspace_bytes(L, bt, precision, precond) + 256;
 }
 
+int lpm_cg_persistent_fits(const lpm_lattice* lat, const lpm_batch* batch)
+{
+    Lattice L;
+    Batch bt;
+    if (to_lattice(lat, L) || to_batch(batch, bt)) return LPM_ERR_ARG;
+    return persist_auto(L, bt) ? 1 : 0;
+}
+
 int lpm_cg_batched_f64(const lpm_lattice* lat, const double* Kn, const double* Tv, int32_t coef_layout,
                        const lpm_batch* batch, const double* Minv, const uint8_t* mask, const double* b, double* x,
                        int32_t x_is_zero, const lpm_cg_opts* opts, void* workspace, size_t workspace_bytes,

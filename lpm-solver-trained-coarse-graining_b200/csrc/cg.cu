@@ -417,6 +417,7 @@ size_t cg_workspace_bytes(const Lattice& L, const Batch& bt, int precision, int 
     const int es = precision == LPM_F32 ? 4 : 8;
     if (L.dim == 3 && L.nbr == nullptr && tma_supported(L.nx, es))
         n = std::max(n, cg_fused_workspace_bytes(L, bt.nsys, bt.rhs_per_set, es, precond));
+    if (persist_fits(L, bt)) n = std::max(n, persist_workspace_bytes(L, bt, es));
     return n;
 }
 
@@ -434,6 +435,10 @@ int cg_solve(const Lattice& L, const T* Kn, const T* Tv, const CoefLayout& cl, c
              int* iters, double* relres, int* status, cudaStream_t st)
 {
     if (o.maxit < 0 || o.check < 1 || o.poll < 1 || bt.nsys < 1) return LPM_ERR_ARG;
+    if (o.engine < LPM_ENGINE_AUTO || o.engine > LPM_ENGINE_PERSISTENT) return LPM_ERR_ARG;
+    if (o.engine == LPM_ENGINE_PERSISTENT || (o.engine == LPM_ENGINE_AUTO && !o.prof && persist_auto(L, bt)))
+        return cg_solve_persist<T>(L, Kn, Tv, cl, bt, Minv, mask, b, x, x_is_zero, o, ws, ws_bytes, iters, relres,
+                                   status, st);
     if (fused_ok(L, cl, (int)sizeof(T)) && tma_aligned(Kn, Tv, b))
         return cg_solve_fused<T>(L, Kn, Tv, bt, Minv, mask, b, x, x_is_zero, o, ws, ws_bytes, iters, relres, status,
                                  st);
@@ -612,7 +617,7 @@ int ir_solve(const Lattice& L, const double* Kn64, const double* Tv64, const Coe
         }
         e = cudaMemcpyAsync(w.itol, h_tol.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) return (int)e;
-        lpm_cg_opts io{o.inner_tol, remaining, o.check, o.poll, 0, o.prof, w.itol};
+        lpm_cg_opts io{o.inner_tol, remaining, o.check, o.poll, 0, o.prof, w.itol, o.engine, 0};
         rc = amg ? amg_pcg(amg, w.r32, w.d32, io, w.it_in, w.rel_in, w.st_in, st)
                  : cg_solve<float>(L, Kn32, Tv32, cl32, bt, Minv32, mask, w.r32, w.d32, 1, io, w.cg_ws, w.cg_bytes,
                                    w.it_in, w.rel_in, w.st_in, st);

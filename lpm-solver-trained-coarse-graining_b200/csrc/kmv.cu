@@ -13,6 +13,7 @@
 // Structured boxes use implicit neighbours (site id (z*ny + y)*nx + x); other lattices (active-site masks) use an
 // int32 neighbour table.  The fused single-pass z-marching SC kernel for full boxes lives in kmv_fused.cu.
 #include "lpm_kernels.h"
+#include "lpm_sqtile.cuh"
 #include "lpm_stencil.cuh"
 
 namespace lpm {
@@ -27,7 +28,6 @@ __global__ void __launch_bounds__(256) k_shell_sums(NB nb, int nx, int ny, int n
                                                     const T* __restrict__ u, const T* __restrict__ Tv, CoefLayout cl,
                                                     Batch bt, T* __restrict__ st, const int* __restrict__ act)
 {
-    using S = Slots<DIM>;
     const Site p = locate<NB>(nx, ny, nz, N, sys0);
     if (!p.ok || (act && !act[p.s])) return;
     const T* us = u + (int64_t)p.s * N * DIM;
@@ -35,26 +35,17 @@ __global__ void __launch_bounds__(256) k_shell_sums(NB nb, int nx, int ny, int n
     T ui[3];
 #pragma unroll
     for (int a = 0; a < DIM; ++a) ui[a] = us[DIM * p.i + a];
-    T s0 = 0, s1 = 0, t0 = 0, t1 = 0;
+    auto load = [&](int64_t q, T* uq) {
 #pragma unroll
-    for (int k = 0; k < S::NN; ++k) {
-        int64_t q;
-        if (!nb.get(p, k, q)) continue;
-        const T d = dl_of<T, DIM>(us, p.i, q, k, ui);
-        const T tvk = tv[k * cl.slot_stride];
-        if (S::shell(k) == 0) {
-            s0 += d;
-            t0 += tvk * d;
-        } else {
-            s1 += d;
-            t1 += tvk * d;
-        }
-    }
+        for (int a = 0; a < DIM; ++a) uq[a] = us[DIM * q + a];
+    };
+    T v[4];
+    shell_sums_at<T, DIM>(nb, p, ui, load, tv, cl.slot_stride, v);
     T* o = st + ((int64_t)p.s * N + p.i) * 4;
-    o[0] = s0;
-    o[1] = s1;
-    o[2] = t0;
-    o[3] = t1;
+    o[0] = v[0];
+    o[1] = v[1];
+    o[2] = v[2];
+    o[3] = v[3];
 }
 
 // ------------------------------------------------------------------------------------------------------ pass 2
@@ -67,7 +58,6 @@ __global__ void __launch_bounds__(256) k_apply(NB nb, int nx, int ny, int nz, in
                                                double* __restrict__ dot_final, unsigned* __restrict__ counter,
                                                const int* __restrict__ act, int nblk)
 {
-    using S = Slots<DIM>;
     const Site p = locate<NB>(nx, ny, nz, N, sys0);
     double dot = 0.0;
     if (p.ok && (!act || act[p.s])) {
@@ -81,30 +71,13 @@ __global__ void __launch_bounds__(256) k_apply(NB nb, int nx, int ny, int nz, in
         for (int a = 0; a < DIM; ++a) ui[a] = us[DIM * p.i + a];
         T Si[2], TSi[2];
         load4(sts + 4 * p.i, Si[0], Si[1], TSi[0], TSi[1]);
-        T f[3] = {T(0), T(0), T(0)};
+        auto load = [&](int64_t q, T* uq) {
 #pragma unroll
-        for (int k = 0; k < S::NN; ++k) {
-            int64_t q;
-            if (!nb.get(p, k, q)) continue;
-            const int c = S::shell(k);
-            const T d = dl_of<T, DIM>(us, p.i, q, k, ui);
-            T Sq[2], TSq[2];
-            load4(sts + 4 * q, Sq[0], Sq[1], TSq[0], TSq[1]);
-            const T knk = kn[k * cl.slot_stride], tvk = tv[k * cl.slot_stride];
-            T F;
-            if constexpr (DIM == 3) {
-                F = T(2) * knk * d + T(0.5) * (TSi[c] + TSq[c]) + T(0.5) * tvk * (Si[c] + Sq[c]);
-            } else {
-                const int64_t qo = (int64_t)q * cl.site_stride + (k ^ 1) * cl.slot_stride;
-                const T knq = Kn[cbase + qo], tvq = Tv[cbase + qo];
-                F = (knk + knq) * d + T(0.5) * (tvk * Si[c] + TSi[c]) + T(0.5) * (tvq * Sq[c] + TSq[c]);
-            }
-            // f += F n_k with n_k = -o_k w_k
-            const T Fw = F * bond_w<T>(c);
-            f[0] -= T(S::dx(k)) * Fw;
-            f[1] -= T(S::dy(k)) * Fw;
-            if constexpr (DIM == 3) f[2] -= T(S::dz(k)) * Fw;
-        }
+            for (int a = 0; a < DIM; ++a) uq[a] = us[DIM * q + a];
+        };
+        auto sums = [&](int64_t q, T (&Sq)[2], T (&TSq)[2]) { load4(sts + 4 * q, Sq[0], Sq[1], TSq[0], TSq[1]); };
+        T f[3];
+        force_at<T, DIM>(nb, p, ui, load, sums, Si, TSi, kn, tv, Kn + cbase, Tv + cbase, cl, f);
         T* o = out + ((int64_t)p.s * N + p.i) * DIM;
         if (EPI && mask) {
             const uint8_t* m = mask + ((int64_t)(p.s % bt.nmask) * N + p.i) * DIM;
@@ -144,10 +117,92 @@ __global__ void __launch_bounds__(256) k_apply(NB nb, int nx, int ny, int nz, in
     }
 }
 
+// Full 2D boxes: both passes in one kernel (lpm_sqtile.cuh), one 32 x 8 tile of one system per block.  The
+// optional epilogue masks the output and reduces u.out per system like k_apply (same block numbering).
+template <typename T, bool EPI>
+__global__ void __launch_bounds__(sqtile::NT) k_sq_fused(int nx, int ny, int64_t N, int sys0, const T* __restrict__ u,
+                                                         const T* __restrict__ Kn, const T* __restrict__ Tv,
+                                                         CoefLayout cl, Batch bt, T* __restrict__ out,
+                                                         const uint8_t* __restrict__ mask, double* __restrict__ part,
+                                                         double* __restrict__ dot_final,
+                                                         unsigned* __restrict__ counter, const int* __restrict__ act)
+{
+    __shared__ sqtile::Smem<T> sm;
+    const int s = sys0 + blockIdx.z;
+    if (act && !act[s]) return;
+    const int x0 = blockIdx.x * sqtile::TX, y0 = blockIdx.y * sqtile::TY;
+    const T* us = u + (int64_t)s * N * 2;
+    const int64_t cbase = (int64_t)(s / bt.rhs_per_set) * cl.set_stride;
+    auto load = [&](int64_t q, T* v) {
+        v[0] = us[2 * q];
+        v[1] = us[2 * q + 1];
+    };
+    sqtile::stage(nx, ny, x0, y0, load, sm);
+    __syncthreads();
+    sqtile::sums(nx, ny, x0, y0, Tv + cbase, cl, sm);
+    __syncthreads();
+    double dot = 0.0;
+    sqtile::forces(nx, ny, x0, y0, Kn + cbase, Tv + cbase, cl, sm, [&](int64_t i, T (&f)[2], const T* ui) {
+        if (EPI && mask) {
+            const uint8_t* m = mask + ((int64_t)(s % bt.nmask) * N + i) * 2;
+            f[0] = m[0] ? f[0] : T(0);
+            f[1] = m[1] ? f[1] : T(0);
+        }
+        T* o = out + ((int64_t)s * N + i) * 2;
+        o[0] = f[0];
+        o[1] = f[1];
+        dot += (double)ui[0] * (double)f[0] + (double)ui[1] * (double)f[1];
+    });
+    if constexpr (EPI) {
+        if (part == nullptr) return;
+        __shared__ double sh[32];
+        __shared__ bool last;
+        const int nblk = gridDim.x * gridDim.y;
+        const int b = blockIdx.x + gridDim.x * blockIdx.y;
+        const double v = block_sum(dot, sh);
+        if (threadIdx.x == 0) {
+            part[(int64_t)s * nblk + b] = v;
+            __threadfence();
+            last = atomicAdd(counter + s, 1u) == (unsigned)(nblk - 1);
+        }
+        __syncthreads();
+        if (last) {
+            double acc = 0.0;
+            for (int j = threadIdx.x; j < nblk; j += sqtile::NT) acc += __ldcg(part + (int64_t)s * nblk + j);
+            acc = block_sum(acc, sh);
+            if (threadIdx.x == 0) {
+                dot_final[s] = acc;
+                counter[s] = 0u;
+            }
+        }
+    }
+}
+
+template <typename T>
+cudaError_t run_sq_fused(const Lattice& L, const T* u, const T* Kn, const T* Tv, const CoefLayout& cl,
+                         const Batch& bt, T* out, const MvEpilogue* ep, cudaStream_t st)
+{
+    const bool epi = ep && (ep->mask || ep->dot_part);
+    const int* act = ep ? ep->act : nullptr;
+    const dim3 grid(sqtile::tiles_x(L.nx), sqtile::tiles_y(L.ny), 1);
+    for (int s0 = 0; s0 < bt.nsys; s0 += 65535) {
+        dim3 g = grid;
+        g.z = bt.nsys - s0 < 65535 ? bt.nsys - s0 : 65535;
+        if (epi)
+            k_sq_fused<T, true><<<g, sqtile::NT, 0, st>>>(L.nx, L.ny, L.N, s0, u, Kn, Tv, cl, bt, out, ep->mask,
+                                                          ep->dot_part, ep->dot_final, ep->counter, act);
+        else
+            k_sq_fused<T, false><<<g, sqtile::NT, 0, st>>>(L.nx, L.ny, L.N, s0, u, Kn, Tv, cl, bt, out, nullptr,
+                                                           nullptr, nullptr, nullptr, act);
+    }
+    return cudaGetLastError();
+}
+
 template <typename T, int DIM, class NB>
 cudaError_t run_kmv(NB nb, const Lattice& L, const T* u, const T* Kn, const T* Tv, const CoefLayout& cl,
                     const Batch& bt, T* out, T* scratch, const MvEpilogue* ep, cudaStream_t st)
 {
+    if constexpr (DIM == 2 && NB::structured) return run_sq_fused<T>(L, u, Kn, Tv, cl, bt, out, ep, st);
     const int nz = DIM == 3 ? L.nz : 1;
     const bool epi = ep && (ep->mask || ep->dot_part);  // act alone needs no epilogue
     int chunk, nblk;
@@ -217,6 +272,7 @@ cudaError_t run_sums(NB nb, const Lattice& L, const T* u, const T* Tv, const Coe
 int kmv_dot_blocks(const Lattice& L)
 {
     if (L.nbr) return (int)((L.N + TB - 1) / TB);
+    if (L.dim == 2) return sqtile::tiles_x(L.nx) * sqtile::tiles_y(L.ny);
     const int nz = L.dim == 3 ? L.nz : 1;
     return ((L.nx + BX - 1) / BX) * ((L.ny + BY - 1) / BY) * nz;
 }

@@ -95,6 +95,16 @@ int cg_solve(const Lattice& L, const T* Kn, const T* Tv, const CoefLayout& cl, c
              const uint8_t* mask, const T* b, T* x, int x_is_zero, const lpm_cg_opts& o, void* ws, size_t ws_bytes,
              int* iters, double* relres, int* status, cudaStream_t st);
 
+// Persistent engine (cg_persist.cu): one cooperative launch per solve.  persist_fits: the batch has a team shape on
+// this device; persist_auto: LPM_ENGINE_AUTO picks it (small batches).  cg_solve routes to it by opts.engine.
+bool persist_fits(const Lattice& L, const Batch& bt);
+bool persist_auto(const Lattice& L, const Batch& bt);
+size_t persist_workspace_bytes(const Lattice& L, const Batch& bt, int elem_bytes);
+template <typename T>
+int cg_solve_persist(const Lattice& L, const T* Kn, const T* Tv, const CoefLayout& cl, const Batch& bt,
+                     const T* Minv, const uint8_t* mask, const T* b, T* x, int x_is_zero, const lpm_cg_opts& o,
+                     void* ws, size_t ws_bytes, int* iters, double* relres, int* status, cudaStream_t st);
+
 // amg != nullptr: the inner solver is the AMG-preconditioned FP32 PCG of the handle (Kn32, Tv32, Minv32 unused).
 int ir_solve(const Lattice& L, const double* Kn64, const double* Tv64, const CoefLayout& cl64, const float* Kn32,
              const float* Tv32, const CoefLayout& cl32, const float* Minv32, const Batch& bt, const uint8_t* mask,

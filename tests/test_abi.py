@@ -32,7 +32,7 @@ def test_library_exports_header():
 
 def test_abi_version_and_strings():
     lib = L.load()
-    assert lib.lpm_abi_version() == 3
+    assert lib.lpm_abi_version() == 4
     assert lib.lpm_status_string(0) == b"ok"
     assert b"argument" in lib.lpm_status_string(-1)
     assert b"workspace" in lib.lpm_status_string(-2)

@@ -9,12 +9,14 @@ import pytest
 
 import oracle as O
 from conftest import relmax
+from lpm_b200 import _lib as L
 from lpm_b200 import core, geom as G
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 DEV = "cuda"
+ENGINES = pytest.mark.parametrize("engine", [L.ENGINE_LAUNCHED, L.ENGINE_PERSISTENT], ids=["launched", "persistent"])
 
 
 def T(a, dt=torch.float64):
@@ -138,19 +140,22 @@ def _bc(lat, ld, s):
     return fixed, up, mov
 
 
-def test_cg_fp64_matches_oracle(gsc, sc12):
-    """Plain FP64 CG (cgplain.cg3) and block-Jacobi PCG (lin3d.solve_pcg): same iterations, same answer."""
+@ENGINES
+def test_cg_fp64_matches_oracle(gsc, sc12, engine):
+    """Plain FP64 CG (cgplain.cg3) and block-Jacobi PCG (lin3d.solve_pcg): same iterations, same answer, on both
+    engines (graph-launched kernels; one persistent cooperative kernel)."""
     lat, dl, Kn, Tv = sc12
     for ld in ("k_xx", "tb_sx"):
         fixed, up, _ = _bc(lat, ld, 2)
         free = ~fixed
         upm = np.where(fixed[:, None], up, 0.0)
         b = -O.sc_apply(lat, upm, Kn, Tv) * free[:, None]
-        x, info = core.cg(dl, T(Kn), T(Tv), T(b), free=T(free), tol=1e-8, maxit=5000, check=1)
+        x, info = core.cg(dl, T(Kn), T(Tv), T(b), free=T(free), tol=1e-8, maxit=5000, check=1, engine=engine)
         assert abs(int(info.iters[0]) - int(gsc["cg_it_%s" % ld])) <= 1
         assert relmax(x.cpu().numpy() + upm, gsc["cg_u_%s" % ld]) < 1e-6
         M = core.block_jacobi(dl, T(Kn), T(Tv), torch.float64)
-        x, info = core.cg(dl, T(Kn), T(Tv), T(b), Minv=M, free=T(free), tol=1e-8, maxit=5000, check=1)
+        x, info = core.cg(dl, T(Kn), T(Tv), T(b), Minv=M, free=T(free), tol=1e-8, maxit=5000, check=1,
+                          engine=engine)
         assert abs(int(info.iters[0]) - int(gsc["pcg_it_%s" % ld])) <= 1
         assert relmax(x.cpu().numpy() + upm, gsc["pcg_u_%s" % ld]) < 1e-6
 
@@ -176,7 +181,8 @@ def test_pcg_batched_vs_superlu(gsc, sc12):
         assert relmax(ub, gsc["u_2_%s" % ld]) < 1e-9
 
 
-def test_mixed_precision_ir(gsc, sc12):
+@ENGINES
+def test_mixed_precision_ir(gsc, sc12, engine):
     """FP32 inner PCG + FP64 refinement to 1e-8: FP64 true residual <= 1e-8 and <= 1e-6 rel. error vs SuperLU."""
     lat, dl, Kn, Tv = sc12
     for ld in ("k_xx", "lr_tx", "tb_tz"):
@@ -185,7 +191,7 @@ def test_mixed_precision_ir(gsc, sc12):
         free = ~fixed
         upm = np.where(fixed[:, None], up, 0.0)
         b = -O.sc_apply(lat, upm, Kn, Tv) * free[:, None]
-        x, info = core.ir(dl, T(Kn), T(Tv), T(b), free=T(free), tol=1e-8, inner_tol=1e-5)
+        x, info = core.ir(dl, T(Kn), T(Tv), T(b), free=T(free), tol=1e-8, inner_tol=1e-5, engine=engine)
         xn = x.cpu().numpy()
         r = (b - O.sc_apply(lat, xn, Kn, Tv)) * free[:, None]
         assert np.linalg.norm(r) <= 1.0000001e-8 * np.linalg.norm(b)
@@ -193,7 +199,8 @@ def test_mixed_precision_ir(gsc, sc12):
         assert rel_l2(xn + upm, gsc["ufull_%d_%s" % (s, ld)]) < 1e-6
 
 
-def test_cg_2d_per_dof_mask(gsq):
+@ENGINES
+def test_cg_2d_per_dof_mask(gsq, engine):
     """cg2plain.cg_mf semantics (per-DOF mask, initial-residual test) in FP64, and the mixed-precision path."""
     lat = G.Lattice2D("square", 16, 12, 1.0)
     dl = core.DeviceLattice(lat)
@@ -201,14 +208,17 @@ def test_cg_2d_per_dof_mask(gsq):
     ub = np.where(fd, up, 0.0)
     Kn, Tv = gsq["Kn"], gsq["Tv"]
     b = (-O.sq_kmv(lat, ub, Kn, Tv) * (~fd).ravel()).reshape(-1, 2)
-    x, info = core.cg(dl, T(Kn), T(Tv), T(b), free=T(~fd), tol=1e-10, maxit=100000, check=1, precheck=True)
+    x, info = core.cg(dl, T(Kn), T(Tv), T(b), free=T(~fd), tol=1e-10, maxit=100000, check=1, precheck=True,
+                      engine=engine)
     assert abs(int(info.iters[0]) - int(gsq["cg_it"])) <= 1
     assert relmax(x.cpu().numpy().ravel() + ub.ravel(), gsq["cg_u"]) < 1e-8
-    x, info = core.ir(dl, T(Kn), T(Tv), T(b), free=T(~fd), tol=1e-10, inner_tol=1e-5, precond=False)
+    x, info = core.ir(dl, T(Kn), T(Tv), T(b), free=T(~fd), tol=1e-10, inner_tol=1e-5, precond=False,
+                      engine=engine)
     assert rel_l2(x.cpu().numpy().ravel() + ub.ravel(), gsq["lu_u"]) < 1e-6
 
 
-def test_cg_freezing_and_status():
+@ENGINES
+def test_cg_freezing_and_status(engine):
     """Systems converge independently; a zero right-hand side returns 0 iterations; maxit reports NOT_CONVERGED."""
     lat = G.LatticeGeom(6, 6, 6)
     dl = core.DeviceLattice(lat)
@@ -218,12 +228,12 @@ def test_cg_freezing_and_status():
     free = ~fixed
     b0 = -O.sc_apply(lat, np.where(fixed[:, None], up, 0.0), Kn, Tv) * free[:, None]
     b = np.stack([b0, 0 * b0, 3 * b0])
-    x, info = core.cg(dl, T(Kn), T(Tv), T(b), free=T(free), tol=1e-10, maxit=2000)
+    x, info = core.cg(dl, T(Kn), T(Tv), T(b), free=T(free), tol=1e-10, maxit=2000, engine=engine)
     assert info.iters[1] == 0 and info.relres[1] == 0.0
     assert info.iters[0] == info.iters[2] and (info.status == 0).all()
     xa = x.cpu().numpy()
     assert relmax(xa[2], 3 * xa[0]) < 1e-9 and np.abs(xa[1]).max() == 0.0
-    _, info = core.cg(dl, T(Kn), T(Tv), T(b0), free=T(free), tol=1e-14, maxit=3)
+    _, info = core.cg(dl, T(Kn), T(Tv), T(b0), free=T(free), tol=1e-14, maxit=3, engine=engine)
     assert info.status[0] == 1 and info.iters[0] == 3
 
 
