@@ -16,6 +16,10 @@ is involved).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--workload spheres48|ellipsoids192]
                     [--precond amg|bj] [--inner-tol T] [--impl ours|reference]
 
+Other workloads (one JSON line each): plain2d (cfg 1, FP64 plain CG on ten 128^2 specimens), coarse2d (cfg 3,
+differentiable 2D coarse solve), serve (cfg 4, the serving stream), kernels (achieved bandwidth of the hot-path
+kernels in single calls).
+
 Under torchrun (N > 1) every rank solves its own B specimens (weak scaling, no data-path collective); the step time
 is the max over ranks.  `--impl reference` times the CPU oracle (the reference's FP64 block-Jacobi PCG restated in C,
 all host threads) on a bounded sample of the same workload.
@@ -578,6 +582,88 @@ def run_coarse2d(a):
     print(json.dumps(line), flush=True)
 
 
+def run_kernels(a):
+    """Achieved bandwidth of the hot-path kernels outside the solver loop: CUDA events around single C-ABI calls (one
+    kernel each, except where named), the L2 flushed by a 256 MB write before every timed call, mean of 10 calls after
+    3 warm-up calls.  Bytes are algorithmic (every input read once, every output written once)."""
+    import torch
+    from lpm_b200 import _lib as L
+    from lpm_b200 import core, geom, micro
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    T = lambda x, dt=torch.float64: torch.as_tensor(np.asarray(x), device=dev, dtype=dt)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak = json.load(open(pp))["hbm_gbs"] if os.path.exists(pp) else 6650.0
+    rows = []
+
+    def timed(fn, reps=10):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize(dev)
+        tot = 0.0
+        for _ in range(reps):
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize(dev)
+            tot += e0.elapsed_time(e1)
+        return tot / reps
+
+    def row(row_id, what, kernels, fn, nbytes):
+        ms = timed(fn)
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        rows.append({"row": row_id, "what": what, "kernels": kernels, "ms": ms, "bytes": int(nbytes),
+                     "achieved_gbs": gbs, "frac": gbs / peak})
+
+    # 3D: 48^3 two-phase microstructure, 16 coefficient sets x 6 systems
+    n, S, R = 48, 16, 6
+    lat = geom.LatticeGeom(n, n, n, 1.0)
+    rng = np.random.default_rng(0)
+    C = geom.iso_C(np.where(rng.random(lat.N) < 0.3, 10.0, 1.0), 0.2)
+    Kn, Tv = geom.bond_params_two_end_mean(lat, geom.sc_params_from_C(C, 0.5))
+    dl = core.DeviceLattice(lat, dev)
+    N = lat.N
+    Kd = T(Kn)[None].expand(S, -1, -1).contiguous()
+    Td = T(Tv)[None].expand(S, -1, -1).contiguous()
+    K64, T64 = core.pack(Kd, torch.float64), core.pack(Td, torch.float64)
+    u64 = torch.randn(S * R, N, 3, device=dev, dtype=torch.float64)
+    u1 = u64[:R].contiguous()
+    lam = torch.randn(R, N, 3, device=dev, dtype=torch.float64)
+    row("a3", "SC K.u FP64 packed, 48^3 x 16 sets x 6", "k_sc_tma<double>",
+        lambda: core.kmv(dl, u64, K64, T64, layout=L.LAYOUT_SOA, rhs_per_set=R), S * N * 288 + S * R * N * 48)
+    row("a4", "SC K.u FP64 reference layout, 48^3 x 6", "k_shell_sums + k_apply",
+        lambda: core.kmv(dl, u1, Kd[:1], Td[:1]), N * 288 + R * N * 48)
+    row("a11", "SC block Jacobi, 48^3 x 16 sets (FP64 in, FP32 out)", "k_block_jacobi",
+        lambda: core.block_jacobi(dl, Kd, Td, torch.float32), S * N * (288 + 36))
+    row("a12", "SC bond gradient, 48^3 x 6 systems of 1 set", "bond-gradient kernels",
+        lambda: core.bond_grad(dl, u1, lam, Kd[:1], Td[:1]), 2 * N * 288 + 2 * R * N * 24)
+    row("a14", "SC particle stress, 48^3 x 6", "stress kernels",
+        lambda: core.stress(dl, u1, Kd[:1], Td[:1]), N * 288 + R * N * (24 + 48))
+    # 2D: 512^2 random-field specimen
+    n2 = 512
+    lat2 = geom.SquareLattice(n2, n2, 1.0)
+    C2 = geom.iso_C2d(np.where(micro.grf_two_phase(n2, n2, 6.0, 0.30, 0) == 1, 10.0, 1.0), 0.25, plane="stress")
+    k2, t2 = geom.bond_params_two_end_mean(lat2, geom.square_params_from_C(C2))
+    dl2 = core.DeviceLattice(lat2, dev)
+    N2 = lat2.N
+    for dt, es, nm in ((torch.float64, 8, "FP64"), (torch.float32, 4, "FP32")):
+        for S2, R2 in ((8, 1), (1, 6)):
+            K2 = core.pack(T(k2)[None].expand(S2, -1, -1).contiguous(), dt)
+            T2 = core.pack(T(t2)[None].expand(S2, -1, -1).contiguous(), dt)
+            u2 = torch.randn(S2 * R2, N2, 2, device=dev, dtype=dt)
+            row("a5", "SQ K.u %s packed, 512^2 x %d sets x %d" % (nm, S2, R2), "k_sq_fused",
+                lambda: core.kmv(dl2, u2, K2, T2, layout=L.LAYOUT_SOA, rhs_per_set=R2),
+                S2 * N2 * 16 * es + S2 * R2 * N2 * 4 * es)
+    print(json.dumps({"metric": "achieved GB/s of the hot-path kernels (single calls, L2 flushed)", "unit": "GB/s",
+                      "peak": peak, "peak_source": "measured" if os.path.exists(pp) else "fallback",
+                      "rows": rows}), flush=True)
+
+
 # ------------------------------------------------------------------------------------------------- GPU side
 def main():
     ap = argparse.ArgumentParser()
@@ -585,7 +671,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--batch", type=int, default=None, help="specimens per GPU (default 16 for spheres48, 1 else)")
-    ap.add_argument("--workload", default="spheres48", choices=sorted(WORKLOADS) + ["serve", "plain2d", "coarse2d"])
+    ap.add_argument("--workload", default="spheres48", choices=sorted(WORKLOADS) + ["serve", "plain2d", "coarse2d", "kernels"])
     ap.add_argument("--requests", type=int, default=40, help="serving stream: number of requests")
     ap.add_argument("--load-factor", type=float, default=0.7, help="serving stream: arrival rate / capacity")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 CG comparator")
@@ -606,6 +692,8 @@ def main():
         return run_plain2d(a)
     if a.workload == "coarse2d":
         return run_coarse2d(a)
+    if a.workload == "kernels":
+        return run_kernels(a)
     if a.impl == "reference":
         return run_reference(a)
 
@@ -719,19 +807,44 @@ def main():
     h2d = Kn_pin.numel() * 8 + Tv_pin.numel() * 8 + fr_pin.numel() * 8 + up_pin.numel() * 8
     d2h = u_host.numel() * 8
 
-    def e2e_step():
-        k = Kn_pin.to(dev, non_blocking=True)[:, None]
-        t = Tv_pin.to(dev, non_blocking=True)[:, None]
-        f = fr_pin.to(dev, non_blocking=True)
-        up = up_pin.to(dev, non_blocking=True)[None].expand(B, -1, -1, -1)
-        uu, _ = step(k, t, f, up)
-        u_host.copy_(uu, non_blocking=True)
+    # Copies run on their own stream, double-buffered: step k+1's inputs go up while step k computes, and step k's
+    # solution comes down while step k+1 computes.  Every step still moves its own inputs and result.
+    cstream = torch.cuda.Stream(dev)
+    dbuf = [[torch.empty(t.shape, dtype=t.dtype, device=dev) for t in (Kn_pin, Tv_pin, fr_pin, up_pin)]
+            for _ in range(2)]
+    ev_in = [torch.cuda.Event() for _ in range(2)]
+    ev_used = [torch.cuda.Event() for _ in range(2)]
 
-    e2e_step()
+    def upload(j):
+        with torch.cuda.stream(cstream):
+            cstream.wait_event(ev_used[j])              # the step that read this buffer set has finished
+            for d, h in zip(dbuf[j], (Kn_pin, Tv_pin, fr_pin, up_pin)):
+                d.copy_(h, non_blocking=True)
+            ev_in[j].record(cstream)
+
+    def e2e_run(nsteps):
+        main = torch.cuda.current_stream(dev)
+        for j in range(2):
+            ev_used[j].record(main)
+        upload(0)
+        for k in range(nsteps):
+            j = k & 1
+            main.wait_event(ev_in[j])
+            if k + 1 < nsteps:
+                upload(1 - j)
+            kd, td, fd, ud = dbuf[j]
+            uu, _ = step(kd[:, None], td[:, None], fd, ud[None].expand(B, -1, -1, -1))
+            ev_used[j].record(main)
+            with torch.cuda.stream(cstream):
+                cstream.wait_event(ev_used[j])
+                u_host.copy_(uu, non_blocking=True)
+                uu.record_stream(cstream)
+        main.wait_stream(cstream)
+
+    e2e_run(2)
     barrier()
     ev0.record()
-    for _ in range(a.steps):
-        e2e_step()
+    e2e_run(a.steps)
     ev1.record()
     barrier()
     ms_e2e = max_over_ranks(ev0.elapsed_time(ev1), world, dev)

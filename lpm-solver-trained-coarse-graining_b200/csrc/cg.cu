@@ -142,14 +142,15 @@ __global__ void __launch_bounds__(VB) k_cg_update(int64_t N, int sys0, Batch bt,
     const int it = sc.itp ? *sc.itp : it_host;
     const int s = sys0 + blockIdx.y;
     const int cur = (it - 1) & 1, nxt = it & 1;
-    const int act = sc.act[s];
+    // a frozen system: every block of it leaves before the reduction, so its counter stays at zero
+    if (!sc.act[s]) return;
     const double pAp = sc.pAp[s];
     const double rzc = sc.rz[cur * bt.nsys + s];
     const bool good = pAp > 0.0 && isfinite(pAp) && isfinite(rzc);
-    const double alpha = (act && good) ? rzc / pAp : 0.0;
-    const int64_t i = (int64_t)blockIdx.x * VB + threadIdx.x;
+    const double alpha = good ? rzc / pAp : 0.0;
     double v[2] = {0.0, 0.0};  // r.z, r.r
-    if (i < N && act) {
+    // grid-stride over particles: a few blocks per system, so the reduction epilogue is amortised
+    for (int64_t i = (int64_t)blockIdx.x * VB + threadIdx.x; i < N; i += (int64_t)gridDim.x * VB) {
         const int64_t o = ((int64_t)s * N + i) * DIM;
         const T al = (T)alpha;
         T rv[DIM], zv[DIM];
@@ -179,7 +180,6 @@ __global__ void __launch_bounds__(VB) k_cg_update(int64_t N, int sys0, Batch bt,
     }
     double tot[2];
     if (!reduce_last<2>(v, sc.part, sc.cnt, s, bt.nsys, blockIdx.x, gridDim.x, sh, tot) || threadIdx.x != 0) return;
-    if (!act) return;
     const double rzn = tot[0], rrn = tot[1];
     sc.rz[nxt * bt.nsys + s] = rzn;
     sc.rr[s] = rrn;
@@ -370,16 +370,31 @@ void carve_ir(Carver& cv, const Lattice& L, const Batch& bt, bool precond, IrWor
     w.cg_ws = cv.take<char>(w.cg_bytes);
 }
 
+// Blocks per system of the update kernel: about eight resident blocks per SM over the whole launch, at most one
+// per 256 particles.
+inline int update_blocks(int nb, int ns)
+{
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) ||
+            sms < 1)
+            sms = 148;
+    }
+    return std::max(1, std::min(nb, (8 * sms + ns - 1) / ns));
+}
+
 template <typename T, int DIM>
 void launch_update(dim3 g, cudaStream_t st, bool precond, const Batch& bt, int64_t N, int s0, int it,
                    const lpm_cg_opts& o, const uint8_t* mask, const T* Minv, T* x, CgWork<T>& w)
 {
+    const dim3 gu(update_blocks((int)g.x, (int)g.y), g.y);
     if (precond)
-        k_cg_update<T, DIM, true><<<g, VB, 0, st>>>(N, s0, bt, it, o.check, o.maxit, o.tol, mask, Minv, x, w.r, w.z,
-                                                    w.p, w.Ap, w.sc);
+        k_cg_update<T, DIM, true><<<gu, VB, 0, st>>>(N, s0, bt, it, o.check, o.maxit, o.tol, mask, Minv, x, w.r,
+                                                     w.z, w.p, w.Ap, w.sc);
     else
-        k_cg_update<T, DIM, false><<<g, VB, 0, st>>>(N, s0, bt, it, o.check, o.maxit, o.tol, mask, Minv, x, w.r, w.z,
-                                                     w.p, w.Ap, w.sc);
+        k_cg_update<T, DIM, false><<<gu, VB, 0, st>>>(N, s0, bt, it, o.check, o.maxit, o.tol, mask, Minv, x, w.r,
+                                                      w.z, w.p, w.Ap, w.sc);
     k_cg_pupdate<T, DIM><<<g, VB, 0, st>>>(N, s0, precond ? w.z : w.r, w.p, w.sc);
 }
 

@@ -98,8 +98,10 @@ class Bucket:
         dv = self.device
         self.stream = torch.cuda.Stream(dv)
         with torch.cuda.stream(self.stream):
-            self.K64 = torch.zeros((S, N, NN), dtype=_F64, device=dv)
-            self.T64 = torch.zeros((S, N, NN), dtype=_F64, device=dv)
+            # FP64 coefficients packed (S, NN, N): the refinement's FP64 residuals and the right-hand sides run on the
+            # packed operators (TMA-fed in 3D, shared-memory tiles in 2D)
+            self.K64 = torch.zeros((S, NN, N), dtype=_F64, device=dv)
+            self.T64 = torch.zeros((S, NN, N), dtype=_F64, device=dv)
             self.K32 = torch.zeros((S, NN, N), dtype=_F32, device=dv)
             self.T32 = torch.zeros((S, NN, N), dtype=_F32, device=dv)
             self.M32 = torch.zeros((S, N, d, d), dtype=_F32, device=dv)
@@ -151,19 +153,21 @@ class Bucket:
         t_adm = time.perf_counter()
         with torch.cuda.stream(self.stream):
             dv = self.device
-            self.K64[s].copy_(torch.as_tensor(req.Kn), non_blocking=False)
-            self.T64[s].copy_(torch.as_tensor(req.Tv), non_blocking=False)
-            self.K32[s:s + 1] = core.pack(self.K64[s:s + 1], _F32)
-            self.T32[s:s + 1] = core.pack(self.T64[s:s + 1], _F32)
-            self.M32[s:s + 1] = core.block_jacobi(self.dl, self.K64[s:s + 1], self.T64[s:s + 1], _F32)
+            Kr = torch.as_tensor(req.Kn).to(dv)[None]          # reference layout (1, N, NN), FP64
+            Tr = torch.as_tensor(req.Tv).to(dv)[None]
+            self.K64[s:s + 1] = core.pack(Kr, _F64)
+            self.T64[s:s + 1] = core.pack(Tr, _F64)
+            self.K32[s:s + 1] = core.pack(Kr, _F32)
+            self.T32[s:s + 1] = core.pack(Tr, _F32)
+            self.M32[s:s + 1] = core.block_jacobi(self.dl, Kr, Tr, _F32)
             free = torch.ones((R, N, d), dtype=torch.uint8)
             up = torch.zeros((R, N, d), dtype=torch.float64)
             free[:req.nloads] = torch.as_tensor(req.free.reshape(req.nloads, N, d))
             up[:req.nloads] = torch.as_tensor(req.up.reshape(req.nloads, N, d))
             self.mask[sl].copy_(free.to(dv))
             self.up[sl].copy_((up * (1 - free.double())).to(dv))
-            Ku = core.kmv(self.dl, self.up[sl], self.K64[s:s + 1].expand(R, N, self.NN).contiguous(),
-                          self.T64[s:s + 1].expand(R, N, self.NN).contiguous())
+            Ku = core.kmv(self.dl, self.up[sl], self.K64[s:s + 1], self.T64[s:s + 1], layout=L.LAYOUT_SOA,
+                          rhs_per_set=R)
             self.b[sl] = -Ku * self.mask[sl]
             self.b[s * R + req.nloads:(s + 1) * R] = 0.0
             self.x[sl] = 0.0
@@ -178,7 +182,7 @@ class Bucket:
         outer = ctypes.c_int32(0)
         t0 = time.perf_counter()
         with torch.cuda.stream(self.stream):
-            L.check(lib.lpm_ir_batched(self.dl.ref, L.ptr(self.K64), L.ptr(self.T64), L.LAYOUT_REF, L.ptr(self.K32),
+            L.check(lib.lpm_ir_batched(self.dl.ref, L.ptr(self.K64), L.ptr(self.T64), L.LAYOUT_SOA, L.ptr(self.K32),
                                        L.ptr(self.T32), L.ptr(self.M32), ctypes.byref(self._batch), L.ptr(self.mask),
                                        L.ptr(self.b), L.ptr(self.x), ctypes.byref(opts), L.ptr(self.ws),
                                        self.ws.numel(), L.ptr(self.it), L.ptr(self.rel), L.ptr(self.st),
