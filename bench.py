@@ -656,7 +656,8 @@ def run_kernels(a):
             K2 = core.pack(T(k2)[None].expand(S2, -1, -1).contiguous(), dt)
             T2 = core.pack(T(t2)[None].expand(S2, -1, -1).contiguous(), dt)
             u2 = torch.randn(S2 * R2, N2, 2, device=dev, dtype=dt)
-            row("a5", "SQ K.u %s packed, 512^2 x %d sets x %d" % (nm, S2, R2), "k_sq_fused",
+            kern = "k_sq_multi" if (es == 4 and R2 > 1) else "k_sq_fused"
+            row("a5", "SQ K.u %s packed, 512^2 x %d sets x %d" % (nm, S2, R2), kern,
                 lambda: core.kmv(dl2, u2, K2, T2, layout=L.LAYOUT_SOA, rhs_per_set=R2),
                 S2 * N2 * 16 * es + S2 * R2 * N2 * 4 * es)
     print(json.dumps({"metric": "achieved GB/s of the hot-path kernels (single calls, L2 flushed)", "unit": "GB/s",

@@ -30,7 +30,6 @@
 #include <map>
 #include <mutex>
 #include <tuple>
-
 #include <type_traits>
 
 #include "lpm_cg.h"
@@ -281,11 +280,13 @@ __global__ void __launch_bounds__(PB) k_cg_persist(NB nb, PersistArgs<T> a)
                 double dot = 0.0;
                 for (int t = rb; t < ntile; t += a.B) {
                     const int x0 = (t % ntx) * sqtile::TX, y0 = (t / ntx) * sqtile::TY;
+                    const sqtile::GlobalCoef<T> kn{a.Kn + cbase, a.cl, a.nx, x0, y0};
+                    const sqtile::GlobalCoef<T> tv{a.Tv + cbase, a.cl, a.nx, x0, y0};
                     sqtile::stage(a.nx, a.ny, x0, y0, load, tsm);
                     __syncthreads();
-                    sqtile::sums(a.nx, a.ny, x0, y0, a.Tv + cbase, a.cl, tsm);
+                    sqtile::sums(a.nx, a.ny, x0, y0, tv, tsm);
                     __syncthreads();
-                    sqtile::forces(a.nx, a.ny, x0, y0, a.Kn + cbase, a.Tv + cbase, a.cl, tsm,
+                    sqtile::forces(a.nx, a.ny, x0, y0, kn, tv, tsm,
                                    [&](int64_t i, T (&f)[2], const T* ui) {
                                        pns[2 * i] = ui[0];
                                        pns[2 * i + 1] = ui[1];

@@ -137,12 +137,13 @@ __global__ void __launch_bounds__(sqtile::NT) k_sq_fused(int nx, int ny, int64_t
         v[0] = us[2 * q];
         v[1] = us[2 * q + 1];
     };
+    const sqtile::GlobalCoef<T> kn{Kn + cbase, cl, nx, x0, y0}, tv{Tv + cbase, cl, nx, x0, y0};
     sqtile::stage(nx, ny, x0, y0, load, sm);
     __syncthreads();
-    sqtile::sums(nx, ny, x0, y0, Tv + cbase, cl, sm);
+    sqtile::sums(nx, ny, x0, y0, tv, sm);
     __syncthreads();
     double dot = 0.0;
-    sqtile::forces(nx, ny, x0, y0, Kn + cbase, Tv + cbase, cl, sm, [&](int64_t i, T (&f)[2], const T* ui) {
+    sqtile::forces(nx, ny, x0, y0, kn, tv, sm, [&](int64_t i, T (&f)[2], const T* ui) {
         if (EPI && mask) {
             const uint8_t* m = mask + ((int64_t)(s % bt.nmask) * N + i) * 2;
             f[0] = m[0] ? f[0] : T(0);
@@ -178,10 +179,110 @@ __global__ void __launch_bounds__(sqtile::NT) k_sq_fused(int nx, int ny, int64_t
     }
 }
 
+// Several systems sharing a coefficient set: one block per tile and set stages the tile's coefficients (tile + ring,
+// both arrays) in shared memory once and applies the operator to every system of the set in turn, so a set's
+// coefficients cross L2 once per tile instead of once per system.  Same arithmetic, output, epilogue and block
+// numbering as k_sq_fused.
+template <typename T, bool EPI>
+__global__ void __launch_bounds__(sqtile::NT) k_sq_multi(int nx, int ny, int64_t N, int set0, const T* __restrict__ u,
+                                                         const T* __restrict__ Kn, const T* __restrict__ Tv,
+                                                         CoefLayout cl, Batch bt, T* __restrict__ out,
+                                                         const uint8_t* __restrict__ mask, double* __restrict__ part,
+                                                         double* __restrict__ dot_final,
+                                                         unsigned* __restrict__ counter, const int* __restrict__ act)
+{
+    constexpr int NC = 8 * sqtile::SH * sqtile::SW;
+    __shared__ sqtile::Smem<T> sm;
+    __shared__ T ck[NC], ct[NC];
+    __shared__ double sh[32];
+    __shared__ bool last;
+    const int set = set0 + blockIdx.z;
+    const int s0 = set * bt.rhs_per_set;
+    const int ns = min(bt.rhs_per_set, bt.nsys - s0);
+    bool any = false;
+    for (int j = 0; j < ns; ++j) any = any || !act || act[s0 + j];
+    if (!any) return;
+    const int x0 = blockIdx.x * sqtile::TX, y0 = blockIdx.y * sqtile::TY;
+    const int64_t cbase = (int64_t)set * cl.set_stride;
+    sqtile::stage_coef(nx, ny, x0, y0, Kn + cbase, cl, ck);
+    sqtile::stage_coef(nx, ny, x0, y0, Tv + cbase, cl, ct);
+    const sqtile::SharedCoef<T> kn{ck}, tv{ct};
+    const int nblk = gridDim.x * gridDim.y;
+    const int b = blockIdx.x + gridDim.x * blockIdx.y;
+    for (int j = 0; j < ns; ++j) {
+        const int s = s0 + j;
+        if (act && !act[s]) continue;
+        const T* us = u + (int64_t)s * N * 2;
+        auto load = [&](int64_t q, T* v) {
+            v[0] = us[2 * q];
+            v[1] = us[2 * q + 1];
+        };
+        __syncthreads();  // the coefficients are staged and the previous system's tile is no longer read
+        sqtile::stage(nx, ny, x0, y0, load, sm);
+        __syncthreads();
+        sqtile::sums(nx, ny, x0, y0, tv, sm);
+        __syncthreads();
+        double dot = 0.0;
+        sqtile::forces(nx, ny, x0, y0, kn, tv, sm, [&](int64_t i, T (&f)[2], const T* ui) {
+            if (EPI && mask) {
+                const uint8_t* m = mask + ((int64_t)(s % bt.nmask) * N + i) * 2;
+                f[0] = m[0] ? f[0] : T(0);
+                f[1] = m[1] ? f[1] : T(0);
+            }
+            T* o = out + ((int64_t)s * N + i) * 2;
+            o[0] = f[0];
+            o[1] = f[1];
+            dot += (double)ui[0] * (double)f[0] + (double)ui[1] * (double)f[1];
+        });
+        if constexpr (EPI) {
+            if (part == nullptr) continue;
+            const double v = block_sum(dot, sh);
+            if (threadIdx.x == 0) {
+                part[(int64_t)s * nblk + b] = v;
+                __threadfence();
+                last = atomicAdd(counter + s, 1u) == (unsigned)(nblk - 1);
+            }
+            __syncthreads();
+            if (last) {
+                double acc = 0.0;
+                for (int q = threadIdx.x; q < nblk; q += sqtile::NT) acc += __ldcg(part + (int64_t)s * nblk + q);
+                acc = block_sum(acc, sh);
+                if (threadIdx.x == 0) {
+                    dot_final[s] = acc;
+                    counter[s] = 0u;
+                }
+            }
+        }
+    }
+}
+
+template <typename T>
+cudaError_t run_sq_multi(const Lattice& L, const T* u, const T* Kn, const T* Tv, const CoefLayout& cl,
+                         const Batch& bt, T* out, const MvEpilogue* ep, cudaStream_t st)
+{
+    const bool epi = ep && (ep->mask || ep->dot_part);
+    const int* act = ep ? ep->act : nullptr;
+    const int nset = (bt.nsys + bt.rhs_per_set - 1) / bt.rhs_per_set;
+    for (int c0 = 0; c0 < nset; c0 += 65535) {
+        const dim3 g(sqtile::tiles_x(L.nx), sqtile::tiles_y(L.ny), nset - c0 < 65535 ? nset - c0 : 65535);
+        if (epi)
+            k_sq_multi<T, true><<<g, sqtile::NT, 0, st>>>(L.nx, L.ny, L.N, c0, u, Kn, Tv, cl, bt, out, ep->mask,
+                                                          ep->dot_part, ep->dot_final, ep->counter, act);
+        else
+            k_sq_multi<T, false><<<g, sqtile::NT, 0, st>>>(L.nx, L.ny, L.N, c0, u, Kn, Tv, cl, bt, out, nullptr,
+                                                           nullptr, nullptr, nullptr, act);
+    }
+    return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t run_sq_fused(const Lattice& L, const T* u, const T* Kn, const T* Tv, const CoefLayout& cl,
                          const Batch& bt, T* out, const MvEpilogue* ep, cudaStream_t st)
 {
+    // FP32 only: an FP64 tile's coefficients (43 KB) with its staging exceed the 48 KB of static shared memory
+    if constexpr (sizeof(T) == 4) {
+        if (bt.rhs_per_set > 1) return run_sq_multi<T>(L, u, Kn, Tv, cl, bt, out, ep, st);
+    }
     const bool epi = ep && (ep->mask || ep->dot_part);
     const int* act = ep ? ep->act : nullptr;
     const dim3 grid(sqtile::tiles_x(L.nx), sqtile::tiles_y(L.ny), 1);

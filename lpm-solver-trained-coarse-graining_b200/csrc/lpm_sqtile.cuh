@@ -41,11 +41,28 @@ __device__ __forceinline__ void stage(int nx, int ny, int x0, int y0, const LD& 
     }
 }
 
-// Shell sums {S^0, S^1, TS^0, TS^1} of the tile and its 1-site ring from the staged displacements (zero outside the
-// box).  tv: the coefficient set's Tv, slot k of particle i at tv[i * site_stride + k * slot_stride].
+// Coefficient accessors address a site by its ring coordinates (lx, ly) = (x - x0 + 1, y - y0 + 1), 0 <= lx < SW,
+// 0 <= ly < SH: the tile and its 1-site ring, where every coefficient a tile's forces and shell sums read lives.
 template <typename T>
-__device__ __forceinline__ void sums(int nx, int ny, int x0, int y0, const T* __restrict__ tv, const CoefLayout& cl,
-                                     Smem<T>& sm)
+struct GlobalCoef {  // a coefficient set in global memory (any layout)
+    const T* c;
+    CoefLayout cl;
+    int nx, x0, y0;
+    __device__ __forceinline__ T operator()(int lx, int ly, int k) const
+    {
+        return c[((int64_t)(y0 - 1 + ly) * nx + (x0 - 1 + lx)) * cl.site_stride + k * cl.slot_stride];
+    }
+};
+template <typename T>
+struct SharedCoef {  // the ring region's coefficients staged in shared memory, slot-major
+    const T* c;
+    __device__ __forceinline__ T operator()(int lx, int ly, int k) const { return c[k * (SH * SW) + ly * SW + lx]; }
+};
+
+// Shell sums {S^0, S^1, TS^0, TS^1} of the tile and its 1-site ring from the staged displacements (zero outside the
+// box).  tv(lx, ly, k): Tv of slot k of a ring site.
+template <typename T, class TVA>
+__device__ __forceinline__ void sums(int nx, int ny, int x0, int y0, const TVA& tv, Smem<T>& sm)
 {
     using S = Slots<2>;
     for (int e = threadIdx.x; e < SH * SW; e += NT) {
@@ -55,7 +72,6 @@ __device__ __forceinline__ void sums(int nx, int ny, int x0, int y0, const T* __
         if (gx >= 0 && gx < nx && gy >= 0 && gy < ny) {
             const int c = (ly + 1) * UW + (lx + 1);
             const T ui[2] = {sm.u[2 * c], sm.u[2 * c + 1]};
-            const T* tvi = tv + ((int64_t)gy * nx + gx) * cl.site_stride;
 #pragma unroll
             for (int k = 0; k < S::NN; ++k) {
                 const int qx = gx + S::dx(k), qy = gy + S::dy(k);
@@ -63,7 +79,7 @@ __device__ __forceinline__ void sums(int nx, int ny, int x0, int y0, const T* __
                 const int cq = c + S::dy(k) * UW + S::dx(k);
                 const T uq[2] = {sm.u[2 * cq], sm.u[2 * cq + 1]};
                 const T d = stencil::dl_from<T, 2>(k, uq, ui);
-                const T tvk = tvi[k * cl.slot_stride];
+                const T tvk = tv(lx, ly, k);
                 if (S::shell(k) == 0) {
                     s0 += d;
                     t0 += tvk * d;
@@ -82,11 +98,10 @@ __device__ __forceinline__ void sums(int nx, int ny, int x0, int y0, const T* __
 }
 
 // Force on this thread's particle of the tile (if it is in the box): emit(i, f, ui) receives the particle index, the
-// force and the particle's staged displacement.  kn / tv: the coefficient set's arrays.
-template <typename T, class EMIT>
-__device__ __forceinline__ void forces(int nx, int ny, int x0, int y0, const T* __restrict__ kn,
-                                       const T* __restrict__ tv, const CoefLayout& cl, const Smem<T>& sm,
-                                       const EMIT& emit)
+// force and the particle's staged displacement.  kn(lx, ly, k), tv(lx, ly, k): coefficients of the ring sites.
+template <typename T, class KNA, class TVA, class EMIT>
+__device__ __forceinline__ void forces(int nx, int ny, int x0, int y0, const KNA& kn, const TVA& tv,
+                                       const Smem<T>& sm, const EMIT& emit)
 {
     using S = Slots<2>;
     const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
@@ -97,8 +112,6 @@ __device__ __forceinline__ void forces(int nx, int ny, int x0, int y0, const T* 
     const int cs = (ty + 1) * SW + (tx + 1);
     const T ui[2] = {sm.u[2 * c], sm.u[2 * c + 1]};
     const T Si[2] = {sm.st[4 * cs], sm.st[4 * cs + 1]}, TSi[2] = {sm.st[4 * cs + 2], sm.st[4 * cs + 3]};
-    const T* kni = kn + i * cl.site_stride;
-    const T* tvi = tv + i * cl.site_stride;
     T f[2] = {T(0), T(0)};
 #pragma unroll
     for (int k = 0; k < S::NN; ++k) {
@@ -110,15 +123,29 @@ __device__ __forceinline__ void forces(int nx, int ny, int x0, int y0, const T* 
         const T uq[2] = {sm.u[2 * cq], sm.u[2 * cq + 1]};
         const T d = stencil::dl_from<T, 2>(k, uq, ui);
         const T Sq[2] = {sm.st[4 * csq], sm.st[4 * csq + 1]}, TSq[2] = {sm.st[4 * csq + 2], sm.st[4 * csq + 3]};
-        const T knk = kni[k * cl.slot_stride], tvk = tvi[k * cl.slot_stride];
-        const int64_t qo = ((int64_t)qy * nx + qx) * cl.site_stride + (k ^ 1) * cl.slot_stride;
-        const T knq = kn[qo], tvq = tv[qo];
+        const T knk = kn(tx + 1, ty + 1, k), tvk = tv(tx + 1, ty + 1, k);
+        const int qlx = tx + 1 + S::dx(k), qly = ty + 1 + S::dy(k);
+        const T knq = kn(qlx, qly, k ^ 1), tvq = tv(qlx, qly, k ^ 1);
         const T F = (knk + knq) * d + T(0.5) * (tvk * Si[c_] + TSi[c_]) + T(0.5) * (tvq * Sq[c_] + TSq[c_]);
         const T Fw = F * bond_w<T>(c_);
         f[0] -= T(S::dx(k)) * Fw;
         f[1] -= T(S::dy(k)) * Fw;
     }
     emit(i, f, ui);
+}
+
+// Stage the coefficients of the tile and its 1-site ring (slot-major, zero outside the box) for SharedCoef.
+template <typename T>
+__device__ __forceinline__ void stage_coef(int nx, int ny, int x0, int y0, const T* __restrict__ c,
+                                           const CoefLayout& cl, T* sc)
+{
+    for (int e = threadIdx.x; e < 8 * SH * SW; e += NT) {
+        const int k = e / (SH * SW), r = e - k * (SH * SW);
+        const int gx = x0 - 1 + r % SW, gy = y0 - 1 + r / SW;
+        sc[e] = (gx >= 0 && gx < nx && gy >= 0 && gy < ny)
+                    ? c[((int64_t)gy * nx + gx) * cl.site_stride + k * cl.slot_stride]
+                    : T(0);
+    }
 }
 
 }  // namespace sqtile

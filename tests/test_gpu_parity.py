@@ -199,6 +199,35 @@ def test_mixed_precision_ir(gsc, sc12, engine):
         assert rel_l2(xn + upm, gsc["ufull_%d_%s" % (s, ld)]) < 1e-6
 
 
+def test_kmv_sq_sets_of_several_systems():
+    """FP32 2D K.u with three systems per coefficient set (one block per tile and set, coefficients staged once) vs
+    the oracle, and launched-engine FP32 PCG over such sets equals each set's systems solved alone."""
+    lat = G.Lattice2D("square", 40, 19, 1.0)
+    dl = core.DeviceLattice(lat)
+    rng = np.random.default_rng(11)
+    KT = [sym_params(lat, rng) for _ in range(2)]
+    Kn, Tv = np.array([k for k, _ in KT]), np.array([t for _, t in KT])
+    u = rng.standard_normal((2, 3, lat.N, 2))
+    f = core.kmv(dl, T(u, torch.float32), T(Kn, torch.float32)[:, None], T(Tv, torch.float32)[:, None])
+    f = f.cpu().numpy()
+    for c in range(2):
+        for j in range(3):
+            ref = O.sq_kmv(lat, u[c, j].ravel(), Kn[c], Tv[c]).reshape(-1, 2)
+            assert relmax(f[c, j], ref) < 2e-6, (c, j)
+    fixed, _, _ = G.uniaxial_tension_2d(lat, 1e-3)
+    b = rng.standard_normal((2, 3, lat.N, 2)) * (~fixed)
+    K32, T32 = T(Kn, torch.float32)[:, None], T(Tv, torch.float32)[:, None]
+    M = core.block_jacobi(dl, T(Kn), T(Tv), torch.float32)
+    kw = dict(free=T(~fixed), tol=1e-5, maxit=5000, check=1, engine=L.ENGINE_LAUNCHED)
+    xb, ib = core.cg(dl, K32, T32, T(b, torch.float32), Minv=M, **kw)
+    for c in range(2):
+        for j in range(3):
+            xa, ia = core.cg(dl, K32[c:c + 1], T32[c:c + 1], T(b[c:c + 1, j:j + 1], torch.float32), Minv=M[c:c + 1],
+                             **kw)
+            assert ib.status[3 * c + j] == 0 and abs(int(ib.iters[3 * c + j]) - int(ia.iters[0])) <= 1
+            assert relmax(xb[c, j].cpu().numpy(), xa[0, 0].cpu().numpy()) < 1e-4
+
+
 @ENGINES
 def test_cg_2d_per_dof_mask(gsq, engine):
     """cg2plain.cg_mf semantics (per-DOF mask, initial-residual test) in FP64, and the mixed-precision path."""

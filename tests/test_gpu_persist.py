@@ -5,10 +5,9 @@ oracle and the reference's golden vectors.
 Both engines run the same algorithm with the same stopping and freezing rules; only the grouping of the FP64 inner
 product partials differs, so iteration counts agree within 1 on short solves and within 0.5% on runs of thousands of
 iterations of ill-conditioned problems (where rounding differences shift the last test), and solutions agree to the
-solve tolerance.  Covered: 2D and
-3D, plain CG and block-Jacobi PCG, FP64 and FP32 (inside the mixed-precision refinement), per-DOF masks, empty and
-early-converging systems, a nonzero start, team shapes with one system per team over several blocks and with several
-systems per single-block team, and a masked lattice (table neighbours).
+solve tolerance.  Covered: 2D and 3D, plain CG and block-Jacobi PCG, FP64 and FP32 (inside the mixed-precision
+refinement), per-DOF masks, empty and early-converging systems, a nonzero start, team shapes with one system per team
+over several blocks and with several systems per single-block team, and a masked lattice (table neighbours).
 """
 import numpy as np
 import pytest
