@@ -303,7 +303,7 @@ def run_serve(a):
     specs = serve_requests(n_req, 1234)
     nsolve = sum(sp[4].shape[0] for sp in specs)
     srv = serve.Server(device=dev, rmax=9, rmax2d=6, max_slots=8, tol=TOL, inner_tol=a.inner_tol,
-                       idle_release_s=1e9)
+                       idle_release_s=1e9, amg3d=a.precond == "amg")
 
     def stream(arrivals):
         reqs = [serve.Request(*sp) for sp in specs]
@@ -382,7 +382,10 @@ def run_serve(a):
                                    "phi U(0.15,0.40), contrast U(5,15), 1-6 / 1-9 load cases",
                        "requests": n_req, "systems": nsolve, "arrival": "Poisson, rate %.3f req/s = %.2f x measured "
                        "capacity %.3f req/s" % (rate, a.load_factor, cap), "tol": TOL,
-                       "buckets": "per lattice size, up to 8 specimens x 9 systems, HBM budget 60% of free memory"},
+                       "buckets": "per lattice size, up to 8 specimens x 9 systems, HBM budget 60% of free memory",
+                       "inner_solvers": ("3D on the standard load boxes: AMG-PCG (inner tol 1e-4); other 3D and 2D: "
+                                         "block-Jacobi PCG (inner tol %g)" % a.inner_tol) if a.precond == "amg" else
+                                        "block-Jacobi PCG (inner tol %g)" % a.inner_tol},
             "latency_ms": lat_ms, "poisson_run": {"solves_per_s": nsolve / t_run, "seconds": t_run,
                                                     "requests_per_s": n_req / t_run},
             "capacity_run": {"requests_per_s": cap, "seconds": t_cap, "latency_ms": lat_cap},
@@ -683,8 +686,8 @@ def main():
     ap.add_argument("--inner-tol", type=float, default=None,
                     help="inner FP32 solve tolerance (default 1e-4 with AMG, 1e-3 with block Jacobi)")
     a = ap.parse_args()
-    if a.inner_tol is None:
-        a.inner_tol = 1e-4 if a.precond == "amg" else 1e-3
+    if a.inner_tol is None:  # serving: the block-Jacobi buckets' value (AMG buckets use 1e-4 themselves)
+        a.inner_tol = 1e-4 if a.precond == "amg" and a.workload != "serve" else 1e-3
     if a.batch is None:
         a.batch = 16 if a.workload == "spheres48" else 1
     if a.workload == "serve":

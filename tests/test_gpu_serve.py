@@ -37,6 +37,20 @@ def spec2(nx, ny, seed, nloads):
     return serve.Request(2, (nx, ny), Kn, Tv, np.array(free), np.array(up))
 
 
+def spec3_custom(n, seed):
+    """A 3D request with a boundary mask outside the standard load set (bottom and top faces and the x = 0 face held,
+    the top face pulled along z): it is served by a block-Jacobi bucket."""
+    lat = G.LatticeGeom(n, n, n, 1.0)
+    ph, _ = micro.spheres(n, n, n, 0.25, 3.0, np.random.default_rng(seed), rjit=0.0)
+    C = G.iso_C(np.where(ph == 1, 8.0, 1.0), 0.2)
+    Kn, Tv = G.bond_params_two_end_mean(lat, G.sc_params_from_C(C, 0.5))
+    i, k = lat.ijk[:, 0], lat.ijk[:, 2]
+    fixed = (k == 0) | (k == n - 1) | (i == 0)
+    up = np.zeros((lat.N, 3))
+    up[(k == n - 1) & (i > 0), 2] = 1e-3 * (n - 1)
+    return serve.Request(3, (n,) * 3, Kn, Tv, np.repeat(~fixed[:, None], 3, 1)[None], up[None])
+
+
 def fp64_reference(r):
     lat = G.LatticeGeom(*r.shape, 1.0) if r.dim == 3 else G.SquareLattice(*r.shape, 1.0)
     dl = core.DeviceLattice(lat)
@@ -51,13 +65,16 @@ def fp64_reference(r):
     return (up + x).cpu().numpy()
 
 
-def run(reqs, gaps):
+def run(reqs, gaps, keys=None):
     srv = serve.Server(budget_bytes=8 << 30, rmax=6, max_slots=3)
     try:
         for r, g in zip(reqs, gaps):
             srv.submit(r)
             time.sleep(g)
-        return srv.wait_all(len(reqs), timeout=600)
+        done = srv.wait_all(len(reqs), timeout=600)
+        if keys is not None:
+            keys.extend(srv.bucket_log)
+        return done
     finally:
         srv.close()
 
@@ -65,9 +82,12 @@ def run(reqs, gaps):
 def test_alone_equals_in_the_mix():
     def make():
         return [spec3(24, 1, ["k_xx", "k_yy", "k_xy"]), spec2(40, 32, 2, 2), spec3(24, 3, ["k_zz", "tb_tz"]),
-                spec3(16, 4, G.LOADS[:5]), spec2(40, 32, 5, 1), spec3(24, 6, ["lr_tx"])]
+                spec3(16, 4, G.LOADS[:5]), spec2(40, 32, 5, 1), spec3(24, 6, ["lr_tx"]), spec3_custom(24, 7)]
     mixed = make()
-    run(mixed, [0.0, 0.01, 0.02, 0.0, 0.03, 0.0])
+    keys = []
+    run(mixed, [0.0, 0.01, 0.02, 0.0, 0.03, 0.0, 0.0], keys)
+    # standard load boxes in AMG buckets, the custom mask in a block-Jacobi bucket of the same size
+    assert {(3, 24, 24, 24, "amg"), (3, 16, 16, 16, "amg"), (3, 24, 24, 24), (2, 40, 32, 1)} <= set(keys)
     for r in mixed:
         assert r.status == 0 and (r.relres <= 1e-8).all(), (r.key, r.relres)
     alone = make()
