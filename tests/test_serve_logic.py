@@ -130,3 +130,44 @@ def test_latency_stats():
         r.arrival, r.done = 0.0, 0.01 * (k + 1)
     st = serve.latency_stats(rs)
     assert abs(st["p50_ms"] - 25.0) < 1e-6 and st["max_ms"] == pytest.approx(40.0)
+
+
+def std_req(n, loads, need=1):
+    """A 3D request whose load cases use the reference's standard boundary boxes (geom.prescribed)."""
+    from lpm_b200 import geom as G
+    lat = G.LatticeGeom(n, n, n, 1.0)
+    free, up = [], []
+    for ld in loads:
+        fixed, u, _ = G.prescribed(ld, lat.x, lat.ijk, (n,) * 3, 1)
+        free.append(np.repeat(~fixed[:, None], 3, 1))
+        up.append(np.where(fixed[:, None], u, 0.0))
+    r = serve.Request(3, (n,) * 3, np.zeros((lat.N, 18)), np.zeros((lat.N, 18)), np.array(free), np.array(up))
+    r.need = need
+    return r
+
+
+def test_amg_bucket_routing_and_slots():
+    """3D requests on the standard load boxes are keyed to AMG buckets, one slot per load type (the six KUBC loads
+    share the ring mask, the two plate loads the z-plate mask); any other mask keeps the plain key; 2D never uses AMG."""
+    from lpm_b200 import geom as G
+    srv = make_server(budget=1000)
+    try:
+        r = std_req(9, ["tb_sx", "k_xx", "lr_tx", "k_yz", "tb_tz"])
+        assert srv.bucket_key(r) == (3, 9, 9, 9, "amg")
+        slots = serve.amg_slots(r)
+        masks = serve.standard_masks((9, 9, 9))
+        assert len(set(slots)) == 5
+        for l, j in enumerate(slots):
+            assert np.array_equal(masks[j], r.free[l][:, 0])
+        assert slots[1] == G.LOADS.index("k_xx") and slots[2] == G.LOADS.index("lr_tx")
+        assert srv._rmax(srv.bucket_key(r)) == len(G.LOADS)
+        all_ring = std_req(9, G.LOADS[:6])
+        assert sorted(serve.amg_slots(all_ring)) == list(range(6))
+        assert srv.bucket_key(req(3, 8, 2, need=1)) == (3, 8, 8, 8)     # all-free masks: not a standard box
+        assert srv.bucket_key(req(2, 16, 2, need=1)) == (2, 16, 16, 1)
+        srv.amg3d = False
+        assert srv.bucket_key(r) == (3, 9, 9, 9)
+        key = (3, 9, 9, 9, "amg")
+        assert serve.bucket_bytes(key, 2, 9) > serve.bucket_bytes(key[:4], 2, 9)
+    finally:
+        srv.close()
