@@ -307,6 +307,7 @@ __global__ void __launch_bounds__(TX* TY, 1)
     const unsigned own_mxy = xy_mask(gx, gy);
     // halo-ring work item of this thread: ring site rs (0..NRING-1) for system rj
     constexpr int NITEM = Lay::NRING * NR;
+    static_assert(NITEM <= Lay::NT, "one ring item per thread: the ring sites of all NR systems must fit the block");
     const bool has_item = tid < NITEM;
     const int rs = has_item ? tid % Lay::NRING : 0, rj = has_item ? tid / Lay::NRING : 0;
     int rqx, rqy;
