@@ -8,8 +8,8 @@
 // i.e. F_ik = 2 Kn dL + (TS_i + TS_q)/2 + Tv (S_i + S_q)/2 against n_k, regrouped so a particle's own terms are formed
 // while its dL are in registers and only (B, A) of the neighbours is exchanged through shared memory.
 //
-// Tiling: a CTA owns a TX x TY column of the box, a range of z planes and NR systems of one coefficient set, and
-// marches in z.  Step z: phase 1 on plane z+1 (shell sums of tile + 1-site ring, own terms of the tile), phase 2 on
+// Tiling: a CTA owns a TX x TY column of the box, a range of z planes and NR systems of one coefficient set (FP32:
+// up to 3, FP64: up to 2), and marches in z.  Step z: phase 1 on plane z+1 (shell sums of tile + 1-site ring, own terms of the tile), phase 2 on
 // plane z (neighbour terms, output).  All global inputs arrive by TMA (cp.async.bulk.tensor, no multicast), issued by
 // one thread a full step ahead into shared-memory rings guarded by mbarriers:
 //   u  : 4 planes x NR systems x (TY+4) rows x 112 values (AoS x,y,z interleaved; x window x0-2 .. x0+33)
@@ -305,32 +305,43 @@ __global__ void __launch_bounds__(TX* TY, 1)
     const int gx = x0 + tx, gy = y0 + ty;
     const bool own_xy = gx < nx && gy < ny;
     const unsigned own_mxy = xy_mask(gx, gy);
-    // halo-ring work item of this thread: ring site rs (0..NRING-1) for system rj
+    // halo-ring work items of this thread: item e = tid + it * NT (it < NIT) is ring site e % NRING of system
+    // e / NRING; NIT = 1 unless the ring sites of all NR systems outnumber the block's threads (FP64, two systems).
+    // With one item it is resolved once; with more, each z step resolves them again (fewer live registers).
     constexpr int NITEM = Lay::NRING * NR;
-    static_assert(NITEM <= Lay::NT, "one ring item per thread: the ring sites of all NR systems must fit the block");
-    const bool has_item = tid < NITEM;
-    const int rs = has_item ? tid % Lay::NRING : 0, rj = has_item ? tid / Lay::NRING : 0;
-    int rqx, rqy;
-    if (rs < SW) {
-        rqx = rs;
-        rqy = 0;
-    } else if (rs < 2 * SW) {
-        rqx = rs - SW;
-        rqy = SH - 1;
-    } else if (rs < 2 * SW + TY) {
-        rqx = 0;
-        rqy = rs - 2 * SW + 1;
-    } else {
-        rqx = SW - 1;
-        rqy = rs - 2 * SW - TY + 1;
-    }
-    const int rX = x0 - 1 + rqx, rY = y0 - 1 + rqy;
-    bool ring_on = false;
+    constexpr int NIT = (NITEM + Lay::NT - 1) / Lay::NT;
+    struct RingItem {
+        int rj, rqx, rqy;
+        bool in;
+        unsigned mxy;
+    };
+    auto ring_item = [&](int it) {
+        const int e = tid + it * Lay::NT;
+        const bool has_item = e < NITEM;
+        const int rs = has_item ? e % Lay::NRING : 0, rj = has_item ? e / Lay::NRING : 0;
+        int rqx, rqy;
+        if (rs < SW) {
+            rqx = rs;
+            rqy = 0;
+        } else if (rs < 2 * SW) {
+            rqx = rs - SW;
+            rqy = SH - 1;
+        } else if (rs < 2 * SW + TY) {
+            rqx = 0;
+            rqy = rs - 2 * SW + 1;
+        } else {
+            rqx = SW - 1;
+            rqy = rs - 2 * SW - TY + 1;
+        }
+        const int rX = x0 - 1 + rqx, rY = y0 - 1 + rqy;
+        bool ring_on = false;
 #pragma unroll
-    for (int j = 0; j < NR; ++j)
-        if (j == rj) ring_on = on[j];
-    const bool ring_in = has_item && rX >= 0 && rX < nx && rY >= 0 && rY < ny && ring_on;
-    const unsigned ring_mxy = xy_mask(rX, rY);
+        for (int q = 0; q < NR; ++q)
+            if (q == rj) ring_on = on[q];
+        return RingItem{rj, rqx, rqy, has_item && rX >= 0 && rX < nx && rY >= 0 && rY < ny && ring_on,
+                        xy_mask(rX, rY)};
+    };
+    const RingItem ring0 = ring_item(0);
 
     auto phase1 = [&](int zp, bool own) {
         if (zp < 0 || zp >= nz) {
@@ -382,8 +393,12 @@ __global__ void __launch_bounds__(TX* TY, 1)
                     if (on[j]) site_sys(j, tx + 1, ty + 1, zp, vk, tv, nullptr, std::false_type{}, nullptr, nullptr);
             }
         }
-        if (ring_in) {
-            const unsigned vm = ring_mxy & zm;
+#pragma unroll
+        for (int it = 0; it < NIT; ++it) {
+            const RingItem ri = it == 0 ? ring0 : ring_item(it);
+            if (!ri.in) continue;
+            const int rj = ri.rj, rqx = ri.rqx, rqy = ri.rqy;
+            const unsigned vm = ri.mxy & zm;
             T vk[18];
 #pragma unroll
             for (int k = 0; k < 18; ++k) vk[k] = ((vm >> k) & 1u) ? T(1) : T(0);
@@ -607,7 +622,9 @@ bool tma_supported(int nx, int elem_bytes)
 
 int tma_group_size(int rhs_per_set, int elem_bytes)
 {
-    if (elem_bytes == 8) return 1;
+    // FP64: two systems per CTA (198 KB of shared memory; three do not fit), so a set's coefficients cross HBM half
+    // as often
+    if (elem_bytes == 8) return rhs_per_set >= 2 ? 2 : 1;
     for (int g = 3; g > 1; --g)
         if (rhs_per_set % g == 0) return g;
     return rhs_per_set >= 3 ? 3 : rhs_per_set;
@@ -637,8 +654,11 @@ cudaError_t launch_sc_tma(const TmaArgs<T>& a, bool epi, cudaStream_t st)
     const int ngt = nset * a.ngrp;
     const int nzc = (a.nz + a.zchunk - 1) / a.zchunk;
     if constexpr (sizeof(T) == 8) {
-        if (a.nr != 1) return cudaErrorInvalidValue;
-        return epi ? launch_one<T, 1, 4, true>(a, ngt, nzc, st) : launch_one<T, 1, 4, false>(a, ngt, nzc, st);
+        switch (a.nr) {
+        case 1: return epi ? launch_one<T, 1, 4, true>(a, ngt, nzc, st) : launch_one<T, 1, 4, false>(a, ngt, nzc, st);
+        case 2: return epi ? launch_one<T, 2, 4, true>(a, ngt, nzc, st) : launch_one<T, 2, 4, false>(a, ngt, nzc, st);
+        default: return cudaErrorInvalidValue;
+        }
     } else {
         switch (a.nr) {
         case 1: return epi ? launch_one<T, 1, 8, true>(a, ngt, nzc, st) : launch_one<T, 1, 8, false>(a, ngt, nzc, st);
