@@ -306,12 +306,12 @@ __global__ void __launch_bounds__(VB) k_amg_init(PairGeom G, const float* __rest
     if (threadIdx.x == 0) cnt[q.pr] = 0u;
 }
 
-// x += alpha p, r -= alpha m Ap, r.r; v = w m M r (the first smoothing step of the cycle); the last block of a pair
-// tests convergence every `check` iterations and freezes converged systems.
+// r -= alpha m Ap, r.r; v = w m M r (the first smoothing step of the cycle); the last block of a pair tests
+// convergence every `check` iterations and freezes converged systems.  x += alpha p is left to the p-update, which
+// reads p anyway (alpha stays set for a system frozen here until the next operator launch zeroes it).
 __global__ void __launch_bounds__(VB) k_amg_update(PairGeom G, int it_host, int check, int maxit, double tol,
                                                    const int* __restrict__ fbox, const float* __restrict__ fw,
-                                                   const float* __restrict__ Ms, float* __restrict__ xp,
-                                                   float* __restrict__ r, const float* __restrict__ p,
+                                                   const float* __restrict__ Ms, float* __restrict__ r,
                                                    const float* __restrict__ Ap, float* __restrict__ v,
                                                    FcgScalars sc, double* part, unsigned* cnt)
 {
@@ -328,21 +328,15 @@ __global__ void __launch_bounds__(VB) k_amg_update(PairGeom G, int it_host, int 
         int x, y, z;
         site_xyz(G, i, x, y, z);
         const int64_t po = ((int64_t)q.pr * G.N + i) * 6;
-        float2* x2 = reinterpret_cast<float2*>(xp + po);
         float2* r2 = reinterpret_cast<float2*>(r + po);
-        const float2* p2 = reinterpret_cast<const float2*>(p + po);
         const float2* a2 = reinterpret_cast<const float2*>(Ap + po);
         float2* v2 = reinterpret_cast<float2*>(v + po);
-        float xv[2][3], rv[2][3], pv[2][3], av[2][3];
+        float rv[2][3], av[2][3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            const float2 tx = x2[a], tr = r2[a], tp = p2[a], ta = a2[a];
-            xv[0][a] = tx.x;
-            xv[1][a] = tx.y;
+            const float2 tr = r2[a], ta = a2[a];
             rv[0][a] = tr.x;
             rv[1][a] = tr.y;
-            pv[0][a] = tp.x;
-            pv[1][a] = tp.y;
             av[0][a] = ta.x;
             av[1][a] = ta.y;
         }
@@ -355,7 +349,6 @@ __global__ void __launch_bounds__(VB) k_amg_update(PairGeom G, int it_host, int 
             const float al = l ? al1 : al0;
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-                xv[l][a] += al * pv[l][a];
                 rv[l][a] -= in ? al * av[l][a] : 0.f;
                 rr[l] += (double)rv[l][a] * rv[l][a];
             }
@@ -369,7 +362,6 @@ __global__ void __launch_bounds__(VB) k_amg_update(PairGeom G, int it_host, int 
         }
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            x2[a] = make_float2(xv[0][a], xv[1][a]);
             r2[a] = make_float2(rv[0][a], rv[1][a]);
             v2[a] = make_float2(vv[0][a], vv[1][a]);
         }
@@ -418,24 +410,35 @@ __global__ void __launch_bounds__(VB) k_amg_update(PairGeom G, int it_host, int 
     if (threadIdx.x == 0) cnt[q.pr] = 0u;
 }
 
-// p = z + beta p for active systems; advances the device iteration counter.
+// x += alpha p with this iteration's alpha (also for a system frozen by this iteration's update: its alpha is zeroed
+// only by the next operator launch), then p = z + beta p for active systems; advances the device iteration counter.
 __global__ void __launch_bounds__(VB) k_amg_pupdate(PairGeom G, const float* __restrict__ zb, float* __restrict__ p,
-                                                    FcgScalars sc)
+                                                    float* __restrict__ xp, FcgScalars sc)
 {
     if (sc.itp && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) atomicAdd(sc.itp, 1);
     const PairQ q = pair_q(G);
     const int64_t i = (int64_t)blockIdx.x * VB + threadIdx.x;
     if (i >= G.N) return;
     const bool on0 = q.nl > 0 && sc.act[q.s0] != 0, on1 = q.nl > 1 && sc.act[q.s0 + 1] != 0;
-    if (!on0 && !on1) return;
+    const float a0 = q.nl > 0 ? (float)sc.alpha[q.s0] : 0.f, a1 = q.nl > 1 ? (float)sc.alpha[q.s0 + 1] : 0.f;
+    const bool mov = a0 != 0.f || a1 != 0.f;
+    if (!on0 && !on1 && !mov) return;
     const float b0 = on0 ? (float)sc.beta[q.s0] : 0.f, b1 = on1 ? (float)sc.beta[q.s0 + 1] : 0.f;
     const int64_t po = ((int64_t)q.pr * G.N + i) * 6;
     const float2* z2 = reinterpret_cast<const float2*>(zb + po);
     float2* p2 = reinterpret_cast<float2*>(p + po);
+    float2* x2 = reinterpret_cast<float2*>(xp + po);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const float2 zz = z2[a], pp = p2[a];
-        p2[a] = make_float2(on0 ? zz.x + b0 * pp.x : pp.x, on1 ? zz.y + b1 * pp.y : pp.y);
+        const float2 pp = p2[a];
+        if (mov) {
+            const float2 xx = x2[a];
+            x2[a] = make_float2(xx.x + a0 * pp.x, xx.y + a1 * pp.y);
+        }
+        if (on0 || on1) {
+            const float2 zz = z2[a];
+            p2[a] = make_float2(on0 ? zz.x + b0 * pp.x : pp.x, on1 ? zz.y + b1 * pp.y : pp.y);
+        }
     }
 }
 
@@ -1922,7 +1925,7 @@ int amg_pcg(lpm_amg* hp, const float* b, float* x, const lpm_cg_opts& o, int* it
     if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
     // z0 = M r0, p0 = z0, r0.z0 (iteration 0 of the beta step)
     if ((e = fine_cycle(h, sc, true, st)) != cudaSuccess) return (int)e;
-    k_amg_pupdate<<<pg, VB, 0, st>>>(G, h.Ap, h.p, sc);
+    k_amg_pupdate<<<pg, VB, 0, st>>>(G, h.Ap, h.p, h.xp, sc);
     if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
     unsigned nconv = 0;
     e = cudaMemcpyAsync(&nconv, h.sc.nconv, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
@@ -1949,11 +1952,11 @@ int amg_pcg(lpm_amg* hp, const float* b, float* x, const lpm_cg_opts& o, int* it
         cudaError_t ee = launch_sc_pair_mode(a, PM_DOT, s);
         timer.end();
         if (ee != cudaSuccess) return ee;
-        k_amg_update<<<dim3(gx, h.npair), VB, 0, s>>>(G, it, o.check, o.maxit, o.tol, h.fbox, h.fw, h.Ms, h.xp, h.r,
-                                                      h.p, h.Ap, h.v, sc, h.vpart, h.vcnt);
+        k_amg_update<<<dim3(gx, h.npair), VB, 0, s>>>(G, it, o.check, o.maxit, o.tol, h.fbox, h.fw, h.Ms, h.r, h.Ap,
+                                                      h.v, sc, h.vpart, h.vcnt);
         if ((ee = cudaGetLastError()) != cudaSuccess) return ee;
         if ((ee = fine_cycle(h, sc, true, s)) != cudaSuccess) return ee;
-        k_amg_pupdate<<<pg, VB, 0, s>>>(G, h.Ap, h.p, sc);
+        k_amg_pupdate<<<pg, VB, 0, s>>>(G, h.Ap, h.p, h.xp, sc);
         return cudaGetLastError();
     };
     GraphKey key;
