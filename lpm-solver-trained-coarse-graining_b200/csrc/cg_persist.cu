@@ -26,10 +26,8 @@
 // records LPM_ERR_TIMEOUT and returns, and the blocks waiting on it see the code and return too.
 #include <algorithm>
 #include <cmath>
-#include <cstring>
 #include <map>
 #include <mutex>
-#include <tuple>
 #include <type_traits>
 
 #include "lpm_cg.h"
