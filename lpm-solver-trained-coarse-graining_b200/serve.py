@@ -221,7 +221,8 @@ class Bucket:
             raise ValueError("request %s with %d loads does not fit bucket %s x %d" % (req.key, req.nloads, self.key,
                                                                                       self.R))
         if self.use_amg:
-            req.slot_map = amg_slots(req)
+            if req.slot_map is None:
+                req.slot_map = amg_slots(req)
             if req.slot_map is None:
                 raise ValueError("request %s has boundary masks outside the AMG bucket's load set" % (req.key,))
         R, d, N = self.R, self.d, self.N
@@ -359,8 +360,11 @@ class Server:
 
     def bucket_key(self, req):
         """The bucket of a request: its lattice size, plus "amg" for 3D requests on the standard boundary boxes."""
-        if self.amg3d and req.dim == 3 and amg_slots(req) is not None:
-            return req.key + ("amg",)
+        if self.amg3d and req.dim == 3:
+            if req.slot_map is None:
+                req.slot_map = amg_slots(req)   # kept for the bucket's admission
+            if req.slot_map is not None:
+                return req.key + ("amg",)
         return req.key
 
     def _slots_for(self, key):
