@@ -18,11 +18,11 @@
 // Tile: 16 x 16 sites, 256 threads; a warp covers rows ty and ty + 2 of 16 columns (the two half-warps then read
 // Tv rows 48 floats apart: no shared-memory bank conflicts).  The CTA marches in z over a chunk of planes; step z
 // computes the shell sums of plane z+1 (tile + 1-site ring) with the own terms of the tile (phase 1), then the
-// neighbour terms and the output of plane z (phase 2).  Shared memory, 187 KB (one CTA per SM):
-//   u      : 4 planes x 20 rows x 120 floats (sites x0-2 .. x0+17, pair layout)
+// neighbour terms and the output of plane z (phase 2).  Shared memory of the staged variant, 207 KB (one CTA per SM):
+//   u      : 5 planes x 20 rows x 120 floats (sites x0-2 .. x0+17, pair layout)
 //   Tv     : 2 planes x 18 slots x 18 rows x 24 sites (x0-4 .. x0+19)
 //   Kn     : 2 planes x 18 slots x 16 rows x 24 sites (x0 .. x0+23)
-//   (B, A) : 3 planes x 2 shells x 18 x 18 sites x float4 {B lane 0, B lane 1, A lane 0, A lane 1}
+//   (B, A) : 4 planes x 2 shells x 18 x 18 sites x float4 {B lane 0, B lane 1, A lane 0, A lane 1}
 // All global inputs arrive by TMA (no multicast), issued by one thread a plane ahead into rings guarded by
 // mbarriers.  Bonds that leave the box: in warps where every lane's site has all 18 bonds no masking is done;
 // otherwise dL of missing bonds is zeroed by selection, so whatever the coefficients of missing bonds hold is
@@ -64,15 +64,19 @@ constexpr size_t PU_SLOT = (size_t)PUH * PUW * 4;
 constexpr size_t PTV_SLOT = (size_t)18 * PSH * PTVW * 4;
 constexpr size_t PKN_SLOT = (size_t)18 * PY * PKNW * 4;
 constexpr size_t PBA_SLOT = (size_t)2 * PSPL * 16;
-// Two variants share the kernel.  Staged (LEAN = false): Tv double-buffered and Kn staged by TMA, 187 KB, one CTA
-// per SM.  Lean (LEAN = true): one Tv slot refilled right after phase 1 has read it, Kn of the own sites read from
-// global memory in phase 1 and Tv of the own sites from global memory (L2) in phase 2, 101 KB and at most 128
-// registers: two CTAs (16 warps) per SM.
-constexpr size_t POFF_TV = 4 * PU_SLOT;
+// Two variants share the kernel.  Staged (LEAN = false): Tv double-buffered and Kn staged by TMA, five u planes and
+// four (B, A) planes, so that one block barrier per z step suffices (a warp may start the next step's phase 1 while
+// others finish phase 2), 207 KB, one CTA per SM.  Lean (LEAN = true): one Tv slot refilled right after phase 1 has
+// read it, Kn of the own sites read from global memory in phase 1 and Tv of the own sites from global memory (L2) in
+// phase 2, four u and three (B, A) planes with two block barriers per step, 101 KB and at most 128 registers: two
+// CTAs (16 warps) per SM.
+__host__ __device__ constexpr int u_slots(bool lean) { return lean ? 4 : 5; }
+__host__ __device__ constexpr int ba_slots(bool lean) { return lean ? 3 : 4; }
 __host__ __device__ constexpr int tv_slots(bool lean) { return lean ? 1 : 2; }
-__host__ __device__ constexpr size_t off_kn(bool lean) { return POFF_TV + tv_slots(lean) * PTV_SLOT; }
+__host__ __device__ constexpr size_t off_tv(bool lean) { return u_slots(lean) * PU_SLOT; }
+__host__ __device__ constexpr size_t off_kn(bool lean) { return off_tv(lean) + tv_slots(lean) * PTV_SLOT; }
 __host__ __device__ constexpr size_t off_ba(bool lean) { return off_kn(lean) + (lean ? 0 : 2 * PKN_SLOT); }
-__host__ __device__ constexpr size_t pair_bytes(bool lean) { return off_ba(lean) + 3 * PBA_SLOT; }
+__host__ __device__ constexpr size_t pair_bytes(bool lean) { return off_ba(lean) + ba_slots(lean) * PBA_SLOT; }
 static_assert(PU_SLOT % 128 == 0 && PTV_SLOT % 128 == 0 && PKN_SLOT % 128 == 0 && PBA_SLOT % 128 == 0,
               "TMA destinations must stay 128-byte aligned");
 static_assert(pair_bytes(false) <= 227 * 1024, "shared memory budget");
@@ -119,13 +123,15 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
               const __grid_constant__ CUtensorMap tm_kn, PairArgs P)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(8) uint64_t bars[8];  // u: 0..3, Tv: 4..5, Kn: 6..7
+    constexpr int NUS = u_slots(LEAN), NBAS = ba_slots(LEAN);
+    constexpr int BTV = NUS, BKN = NUS + 2, NBAR = NUS + 4;  // mbarriers: u 0..NUS-1, Tv BTV.., Kn BKN..
+    __shared__ __align__(8) uint64_t bars[NBAR];
     __shared__ double red[32];
     __shared__ int abort_flag;
     __shared__ bool last_flag;
 
     float* su = reinterpret_cast<float*>(smem);
-    float* stv = reinterpret_cast<float*>(smem + POFF_TV);
+    float* stv = reinterpret_cast<float*>(smem + off_tv(LEAN));
     float* skn = reinterpret_cast<float*>(smem + off_kn(LEAN));
     float4* sba = reinterpret_cast<float4*>(smem + off_ba(LEAN));
 
@@ -171,7 +177,7 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
     }
 
     if (tid == 0) {
-        for (int b = 0; b < 8; ++b) mbar_init(&bars[b], 1);
+        for (int b = 0; b < NBAR; ++b) mbar_init(&bars[b], 1);
         fence_mbar_init();
         abort_flag = 0;
         if (saddr(smem) & 127u) {  // TMA destinations must be 128-byte aligned: refuse to run and report
@@ -181,7 +187,7 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
     }
     {
         const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int e = tid; e < 3 * 2 * PSPL; e += PNT) sba[e] = z4;
+        for (int e = tid; e < NBAS * 2 * PSPL; e += PNT) sba[e] = z4;
         // u slots standing for planes below 0 are never loaded; keep them finite
         const int nneg = zbeg - 2 < 0 ? 2 - zbeg : 0;
         for (int e = tid; e < nneg * (int)(PU_SLOT / 4); e += PNT) su[e] = 0.f;
@@ -200,38 +206,38 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
     };
     auto issue_u = [&](int p) {
         const int n = p - u0;
-        uint64_t* bar = &bars[n & 3];
+        uint64_t* bar = &bars[n % NUS];
         if (p < 0 || p >= nz) {
             mbar_arrive(bar);
             return;
         }
         mbar_expect_arrive(bar, (uint32_t)PU_SLOT);
-        tma_load4(su + (size_t)(n & 3) * (PU_SLOT / 4), &tm_u, bar, 6 * (x0 - 2), y0 - 2, p, pr);
-        note(n & 3, (n >> 2) & 1);
+        tma_load4(su + (size_t)(n % NUS) * (PU_SLOT / 4), &tm_u, bar, 6 * (x0 - 2), y0 - 2, p, pr);
+        note(n % NUS, (n / NUS) & 1);
     };
-    // Tv fill n: slot n % tv_slots, barrier 4 + slot, parity (n / tv_slots) & 1
+    // Tv fill n: slot n % tv_slots, barrier BTV + slot, parity (n / tv_slots) & 1
     constexpr int NTV = tv_slots(LEAN);
     auto issue_tv = [&](int p) {
         const int n = p - tv0;
-        uint64_t* bar = &bars[4 + n % NTV];
+        uint64_t* bar = &bars[BTV + n % NTV];
         if (p < 0 || p >= nz) {
             mbar_arrive(bar);
             return;
         }
         mbar_expect_arrive(bar, (uint32_t)PTV_SLOT);
         tma_load4(stv + (size_t)(n % NTV) * (PTV_SLOT / 4), &tm_tv, bar, x0 - 4, y0 - 1, p, 18 * set);
-        note(4 + n % NTV, (n / NTV) & 1);
+        note(BTV + n % NTV, (n / NTV) & 1);
     };
     auto issue_kn = [&](int p) {
         const int n = p - kn0;
-        uint64_t* bar = &bars[6 + (n & 1)];
+        uint64_t* bar = &bars[BKN + (n & 1)];
         if (p < 0 || p >= nz) {
             mbar_arrive(bar);
             return;
         }
         mbar_expect_arrive(bar, (uint32_t)PKN_SLOT);
         tma_load4(skn + (size_t)(n & 1) * (PKN_SLOT / 4), &tm_kn, bar, x0, y0, p, 18 * set);
-        note(6 + (n & 1), (n >> 1) & 1);
+        note(BKN + (n & 1), (n >> 1) & 1);
     };
     // Every thread waits (bounded) for the in-range fills it is about to read; an expired wait raises the abort
     // flag, which all threads test after the next block barrier.
@@ -244,16 +250,16 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
         }
     };
     auto wait_planes = [&](int pu, int ptv, int pkn) {
-        if (pu >= 0 && pu < nz && pu >= u0) wait_fill((pu - u0) & 3, ((pu - u0) >> 2) & 1);
-        if (ptv >= 0 && ptv < nz && ptv >= tv0) wait_fill(4 + (ptv - tv0) % NTV, ((ptv - tv0) / NTV) & 1);
+        if (pu >= 0 && pu < nz && pu >= u0) wait_fill((pu - u0) % NUS, ((pu - u0) / NUS) & 1);
+        if (ptv >= 0 && ptv < nz && ptv >= tv0) wait_fill(BTV + (ptv - tv0) % NTV, ((ptv - tv0) / NTV) & 1);
         if (!LEAN && pkn >= 0 && pkn < nz && pkn >= kn0 && pkn < zend)
-            wait_fill(6 + ((pkn - kn0) & 1), ((pkn - kn0) >> 1) & 1);
+            wait_fill(BKN + ((pkn - kn0) & 1), ((pkn - kn0) >> 1) & 1);
     };
 
-    auto u_slot = [&](int p) { return su + (size_t)((p - u0) & 3) * (PU_SLOT / 4); };
+    auto u_slot = [&](int p) { return su + (size_t)((p - u0) % NUS) * (PU_SLOT / 4); };
     auto tv_slot = [&](int p) { return stv + (size_t)((p - tv0) % NTV) * (PTV_SLOT / 4); };
     auto kn_slot = [&](int p) { return skn + (size_t)((p - kn0) & 1) * (PKN_SLOT / 4); };
-    auto ba_slot = [&](int p) { return sba + (size_t)(((p % 3) + 3) % 3) * (PBA_SLOT / 16); };
+    auto ba_slot = [&](int p) { return sba + (size_t)(((p % NBAS) + NBAS) % NBAS) * (PBA_SLOT / 16); };
     auto zero_ba = [&](int p) {
         float4* d = ba_slot(p);
         const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -578,11 +584,15 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
                     if (z + 2 <= zend) issue_tv(z + 2);
                 }
                 phase2(z);
-                __syncthreads();
+                // Lean: the next step's Tv fill and phase 1 reuse buffers phase 2 may still read.  Staged: the next
+                // step's fills go to the u slot of plane z - 1 and phase 1 writes the (B, A) slot of plane z + 2,
+                // neither of which this phase 2 reads, and every warp has left phase 2 of plane z - 1 before any
+                // passes this step's barrier: no second barrier.
+                if constexpr (LEAN) __syncthreads();
             }
         }
         if (!ok && tid == 0) {  // let the copies in flight land before the block's shared memory is released
-            for (int b = 0; b < 8; ++b)
+            for (int b = 0; b < NBAR; ++b)
                 if ((pend >> b) & 1u) mbar_wait(&bars[b], (ppar >> b) & 1u);
         }
     }
