@@ -57,13 +57,13 @@ PRECONDS = {"amg": "aggregation AMG, W(1,1) cycle, one hierarchy per specimen an
             "bj": "3x3 block Jacobi"}
 
 
-def workload_config(w, batch, n_gpus, precond="amg"):
+def workload_config(w, batch, n_gpus):
+    """The workload (identical in the GPU arm and the reference arm); how each arm solves it goes under "method"."""
     W = WORKLOADS[w]
     n, L = W["n"], len(W["loads"])
     return {"workload": W["label"], "lattice": [n] * 3, "specimens_per_gpu": batch, "rhs_per_specimen": L,
-            "systems_per_gpu": L * batch, "tol": TOL, "precision": "fp32 inner PCG + fp64 refinement",
-            "preconditioner": PRECONDS[precond], "l2": "inputs larger than L2 (%.0f MB of FP64 coefficients per GPU)"
-            % (batch * n ** 3 * 36 * 8 / 1e6), "parallelism": "dp%d (independent specimens per GPU)" % n_gpus}
+            "systems_per_gpu": L * batch, "tol": TOL, "l2": "inputs larger than L2 (%.0f MB of FP64 coefficients per "
+            "GPU)" % (batch * n ** 3 * 36 * 8 / 1e6), "parallelism": "dp%d (independent specimens per GPU)" % n_gpus}
 
 
 def make_specimen(w, seed, geom, micro):
@@ -181,62 +181,137 @@ def job_throughput(world, systems_per_rank, steps, ms):
 
 
 # ------------------------------------------------------------------------------------------------ CPU side
-def kmv_traffic(nsys):
-    """DRAM bytes per K.u launch for `nsys` systems of the 48^3 workload (6 per specimen), scaled from the ncu capture
-    of a 4-specimen launch (24 systems) summarised in profiles/: read + write bytes grow with the systems and sets."""
-    path = os.path.join(ROOT, "profiles", "k_sc_pair_48cube_batch4.md")
+def kmv_traffic(nsys, workload):
+    """DRAM bytes per K.u launch for `nsys` systems, from the ncu capture recorded in profiles/k_sc_pair_traffic.json
+    (dram__bytes_read.sum + dram__bytes_write.sum of one launch of the captured case, scaled by systems: the bytes of a
+    launch grow with its systems and coefficient sets, which keep the same ratio here).  None if not recorded."""
+    path = os.path.join(ROOT, "profiles", "k_sc_pair_traffic.json")
     if not os.path.exists(path):
-        return None
-    got = {}
-    for line in open(path):
-        for key in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
-            if line.startswith("| `%s`" % key):
-                val, unit = line.split("|")[2].split()
-                got[key] = float(val) * {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}[unit]
-    if len(got) != 2:
-        return None
-    return (got["dram__bytes_read.sum"] + got["dram__bytes_write.sum"]) / 24 * nsys
+        return None, None
+    rec = json.load(open(path))
+    cap = rec.get(workload)
+    if not cap:
+        return None, None
+    return (cap["dram_bytes_read"] + cap["dram_bytes_write"]) / cap["systems"] * nsys, \
+        "ncu dram bytes of one launch (%s, commit %s) scaled by systems" % (cap["case"], cap["commit"])
 
 
-def cpu_solve_sample(lat, Kn, Tv, free, ups, nsolve, maxit=20000):
-    """FP64 block-Jacobi PCG of the CPU oracle (the reference's lin3d._pcg restated in C, all host threads) on the
-    first `nsolve` load cases of specimen 0, at most `maxit` iterations each.  Returns (seconds, solves, threads,
-    iterations of the last solve)."""
+def cpu_solve_sample(lat, Kn, Tv, free, ups, picks, maxit=20000, threads=None):
+    """FP64 block-Jacobi PCG of the CPU oracle (the reference's lin3d._pcg / solve_pcg restated in C, OpenMP) on the
+    (specimen, load) pairs `picks`, at most `maxit` iterations each, with `threads` OpenMP threads (all host threads by
+    default).  Returns (seconds, solves, threads, iterations of the last solve)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    O.set_threads(os.cpu_count() or 1)
+    O.set_threads(threads or os.cpu_count() or 1)
     t0 = time.perf_counter()
     it = 0
-    for l in range(nsolve):
-        fixed = ~free[l]
-        _, info = O.solve_pcg(lat, Kn[0], Tv[0], fixed, ups[l], tol=TOL, maxit=maxit)
+    for j, l in picks:
+        _, info = O.solve_pcg(lat, Kn[j], Tv[j], ~free[l], ups[l], tol=TOL, maxit=maxit)
         it = info["iters"]
-    return time.perf_counter() - t0, nsolve, O.get_threads(), it
+    return time.perf_counter() - t0, len(picks), O.get_threads(), it
+
+
+def cpu_amg_sample(lat, Kn, Tv, free, ups, j, l):
+    """FP64 aggregation-AMG PCG of the reference's timing/t3d/amg3d.py (settings of timing/t3d/problems.py:19) as the
+    NumPy oracle restates it, one load case: geometry, numeric setup and PCG to 1e-8.  Returns (seconds, iterations)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import amg as OA
+    O.set_threads(os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    b = -O.sc_apply(lat, ups[l], Kn[j], Tv[j]) * free[l][:, None]
+    h = OA.Hierarchy(OA.Geometry(lat, free[l]), Kn[j], Tv[j])
+    _, it, _ = h.pcg(b, TOL)
+    return time.perf_counter() - t0, it
+
+
+def reference_picks(nspec, nload, k, per_step):
+    """(specimen, load) pairs of step k of the bounded CPU sample: consecutive pairs of the whole batch, wrapping."""
+    return [((k * per_step + q) // nload % nspec, (k * per_step + q) % nload) for q in range(per_step)]
 
 
 def run_reference(a):
+    """The reference arm: the reference's FP64 block-Jacobi PCG (coarse3d/lin3d.py:464-532, restated in C by the
+    oracle) on the host cores, all threads, on a bounded sample of the same workload per step (one solve of the next
+    (specimen, load) pair of the batch), same metric and config as the GPU arm."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    lat, Kn, Tv, free, ups = load_workload(a.workload, [0])
-    nsolve = 1
-    for _ in range(a.warmup):
-        cpu_solve_sample(lat, Kn, Tv, free, ups, nsolve)
+    B = a.batch
+    lat, Kn, Tv, free, ups = load_workload(a.workload, list(range(B)))
+    L = len(WORKLOADS[a.workload]["loads"])
+    per_step = 1
+    for k in range(a.warmup):
+        cpu_solve_sample(lat, Kn, Tv, free, ups, reference_picks(B, L, k, per_step))
     secs = []
-    for _ in range(a.steps):
-        s, n, thr, _ = cpu_solve_sample(lat, Kn, Tv, free, ups, nsolve)
+    thr = 1
+    for k in range(a.steps):
+        s, n, thr, _ = cpu_solve_sample(lat, Kn, Tv, free, ups, reference_picks(B, L, a.warmup + k, per_step))
         secs.append(s)
     tot = sum(secs)
-    value = a.steps * nsolve / tot
+    value = a.steps * per_step / tot
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": 1e3 * tot / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(a.workload, a.batch, a.gpus, a.precond),
+            "config": workload_config(a.workload, a.batch, a.gpus),
+            "method": "FP64 block-Jacobi PCG to rel. res. 1e-8 on the host cores (the C oracle restating "
+                      "coarse3d/lin3d.py:464-532, OpenMP)",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port",
-                             "sample": "%d load case(s) per step of specimen 0, FP64 block-Jacobi PCG to 1e-8 "
-                                       "(oracle restating coarse3d/lin3d.py:464-532)" % nsolve},
+                             "sample": "%d solve(s) per step: the next (specimen, load) pairs of the %d x %d batch, "
+                                       "FP64 block-Jacobi PCG to 1e-8" % (per_step, B, L)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def torch_sct_cg(lat, Kn, Tv, b, free, tol, check=10, maxit=50000):
+    """The reference's FP64 GPU CG, restated in plain PyTorch tensor ops as coarse3d/torch_lpm3d.py:36-140 runs it
+    (SCT.apply by gathers over the (N, 18) neighbour table with a zero ghost row, SCT.pcg with M = identity, a
+    per-system activity mask and a host check every `check` iterations).  A comparator only: nothing of the library
+    runs in it.  Kn, Tv (B, 1, N, 18), b (B, L, N, 3), free (L, N) float64 CUDA tensors.  Returns (x, iterations)."""
+    import torch
+    dev = b.device
+    N = lat.N
+    nbr = torch.as_tensor(np.where(lat.nbr >= 0, lat.nbr, N), device=dev)
+    valid = torch.as_tensor(lat.valid, device=dev, dtype=torch.float64)
+    ndir = torch.as_tensor(lat.ndir, device=dev, dtype=torch.float64)
+    sh = torch.as_tensor(np.asarray(lat.shell), device=dev)
+    slot = torch.arange(18, device=dev)
+    ghost = lambda t: torch.cat([t, torch.zeros_like(t[..., :1, :])], -2)
+
+    def apply(u):
+        dL = ((u[..., :, None, :] - ghost(u)[..., nbr, :]) * ndir).sum(-1) * valid
+        TdL = Tv * dL
+        S = torch.stack([dL[..., :6].sum(-1), dL[..., 6:].sum(-1)], -1)[..., sh]
+        TS = torch.stack([TdL[..., :6].sum(-1), TdL[..., 6:].sum(-1)], -1)[..., sh]
+        Sq = ghost(S)[..., nbr, slot]
+        TSq = ghost(TS)[..., nbr, slot]
+        F = (2 * Kn * dL + 0.5 * (TS + TSq) + 0.5 * Tv * (S + Sq)) * valid
+        return F @ ndir
+
+    fr = free[..., None]
+    x = torch.zeros_like(b)
+    r = b.clone()
+    bn = b.flatten(-2).norm(dim=-1)
+    bn = torch.where(bn > 0, bn, torch.ones_like(bn))
+    p = r.clone()
+    rz = (r * r).flatten(-2).sum(-1)
+    act = torch.ones_like(rz)
+    it = 0
+    for it in range(1, maxit + 1):
+        Ap = apply(p) * fr
+        pAp = (p * Ap).flatten(-2).sum(-1)
+        alpha = torch.where(pAp != 0, rz / pAp, torch.zeros_like(rz)) * act
+        x = x + alpha[..., None, None] * p
+        r = r - alpha[..., None, None] * Ap
+        if it % check == 0:
+            act = ((r.flatten(-2).norm(dim=-1) / bn) > tol).to(b.dtype)
+            if not bool(act.any()):
+                break
+        rz2 = (r * r).flatten(-2).sum(-1)
+        beta = torch.where(rz != 0, rz2 / rz, torch.zeros_like(rz))
+        rz = rz2
+        p = r + beta[..., None, None] * p
+    return x, it
 
 
 # ---------------------------------------------------------------------------------------------- serving stream
@@ -755,18 +830,28 @@ def main():
         u, info = step(Kn, Tv, free, ups)
     barrier()
 
+    from lpm_b200 import _lib
     sampler = ClockSampler(local)
     sampler.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # one event per step boundary (recorded between steps, outside every captured graph): the per-step times
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
+    cap0 = _lib.graph_stats()
     barrier()
     ev0.record()
     infos = []
-    for _ in range(a.steps):
+    for k in range(a.steps):
+        evs[k].record()
         u, info = step(Kn, Tv, free, ups)
         infos.append(info)
+    evs[a.steps].record()
     ev1.record()
     barrier()
     clocks = sampler.stop()
+    cap1 = _lib.graph_stats()
+    step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(a.steps)]
+    graphs = {"captured_in_timed_region": cap1[0] - cap0[0], "cache_flushes_in_timed_region": cap1[2] - cap0[2],
+              "held_after": cap1[1]}
     # per-launch operator timings come from one more step outside the timed region (timing every launch with events
     # turns off the CUDA-graph replay of the iteration blocks)
     prof = core.new_prof()
@@ -791,13 +876,12 @@ def main():
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
     achieved = alg_bytes / (full_ms / 1e3) / 1e9 if prof[3] > 0 else None
-    traffic = kmv_traffic(nsys) if a.workload == "spheres48" else None
+    traffic, traffic_src = kmv_traffic(nsys, a.workload)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                 "kernel": "k_sc_pair: pair-packed FP32 SC K.u with the p.Ap epilogue (all %d systems, %d coefficient "
                           "sets) in the inner PCG" % (nsys, B),
-                "traffic_source": "ncu dram bytes of a 4-specimen launch (profiles/k_sc_pair_48cube_batch4.md) scaled "
-                                  "by systems",
+                "traffic_source": traffic_src,
                 "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": full_ms, "avg_launch_ms_all": all_ms,
                 "launches_profiled": int(prof[1]), "peak_source": peak_src,
                 "timing_source": "CUDA events around every operator launch of one extra step outside the timed region"}
@@ -857,7 +941,6 @@ def main():
 
     # ---- comparator: plain FP64 GPU CG on the same batch with this library's fastest FP64 path (packed
     # coefficients, TMA-fed fused operator, same engine), packing included; accuracy vs FP64 PCG to 1e-12
-    from lpm_b200 import _lib
     b = -core.kmv(dl, ups, Kn, Tv) * free[None, :, :, None]
     fp64_cg = None
     if not a.no_fp64:
@@ -884,13 +967,41 @@ def main():
                 "u_rel_l2_per_load": [float(v) for v in du[0].cpu()], "stress_rel_l2_per_load":
                     [float(v) for v in ds[0].cpu()]}
 
+    # ---- comparator: the reference's own FP64 GPU CG algorithm (SCT.pcg with M = identity, plain PyTorch tensor
+    # ops) on a sample of the batch, timed with CUDA events on the same GPU
+    torch_cg = None
+    if not a.no_fp64 and a.workload == "spheres48":
+        nb = min(B, 4)
+        torch.cuda.synchronize(dev)
+        ev0.record()
+        _, it_t = torch_sct_cg(lat, Kn[:nb], Tv[:nb], b[:nb], free, TOL)
+        ev1.record()
+        torch.cuda.synchronize(dev)
+        torch_cg = {"solves_per_s": nb * Lc / (ev0.elapsed_time(ev1) / 1e3), "iterations": it_t,
+                    "sample": "%d specimens x %d loads" % (nb, Lc),
+                    "path": "the algorithm of coarse3d/torch_lpm3d.py:36-140 (SCT.apply by tensor gathers, SCT.pcg "
+                            "with M = identity, check every 10 iterations) restated in plain PyTorch"}
+
     cpu = None
+    cpu_extra = None
     if rank == 0 and world == 1 and not a.no_cpu:
         if a.workload == "spheres48":
-            secs, n, thr, _ = cpu_solve_sample(lat, Kn_h, Tv_h, free_h, ups_h, 2)
+            picks = [(0, 0), (0, 1)]
+            secs, n, thr, _ = cpu_solve_sample(lat, Kn_h, Tv_h, free_h, ups_h, picks)
             cpu = {"value": n / secs, "unit": UNIT, "cores": thr, "kind": "port",
                    "sample": "2 load cases (k_xx, k_yy) of specimen 0, FP64 block-Jacobi PCG to 1e-8 by the C oracle "
                              "(restating coarse3d/lin3d.py:464-532), %.1f s" % secs}
+            # the reference's thread protocol (timing/t3d/bench3d.py:167-171): all cores, 6 threads, 1 thread; and its
+            # strongest CPU solver, the aggregation-AMG PCG (timing/t3d/problems.py:112-132), on one load case
+            cpu_extra = {"bj_pcg_threads": {}}
+            for t in (6, 1):
+                s_t, n_t, thr_t, _ = cpu_solve_sample(lat, Kn_h, Tv_h, free_h, ups_h, [(0, 0)], threads=t)
+                cpu_extra["bj_pcg_threads"][str(thr_t)] = n_t / s_t
+            cpu_extra["bj_pcg_threads"][str(thr)] = n / secs
+            s_a, it_a = cpu_amg_sample(lat, Kn_h, Tv_h, free_h, ups_h, 0, 0)
+            cpu_extra["amg_pcg"] = {"solves_per_s": 1.0 / s_a, "iterations": it_a, "cores": thr,
+                                    "path": "NumPy restatement of timing/t3d/amg3d.py (setup + PCG, load k_xx of "
+                                            "specimen 0)"}
         else:
             # a full CPU solve of this size takes tens of minutes: time 30 PCG iterations of load 0 and scale by the
             # iteration count the same FP64 PCG needs on the GPU
@@ -898,7 +1009,7 @@ def main():
             _, i0 = core.cg(dl, Kn[0:1, 0], Tv[0:1, 0], b[0:1, 0], Minv=M0, free=free[0:1], tol=TOL, maxit=20000,
                             check=1, poll=50)
             need = int(i0.iters[0])
-            secs, n, thr, done = cpu_solve_sample(lat, Kn_h, Tv_h, free_h, ups_h, 1, maxit=30)
+            secs, n, thr, done = cpu_solve_sample(lat, Kn_h, Tv_h, free_h, ups_h, [(0, 0)], maxit=30)
             cpu = {"value": 1.0 / (secs / max(done, 1) * need), "unit": UNIT, "cores": thr, "kind": "port",
                    "sample": "30 FP64 block-Jacobi PCG iterations of load k_xx by the C oracle (restating "
                              "coarse3d/lin3d.py:464-532), %.1f s, scaled to the %d iterations the same PCG needs "
@@ -921,15 +1032,20 @@ def main():
             "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64", "data": "synthetic (seeded %s microstructures, shapes of the %d^3 config)"
             % ("spheres" if a.workload == "spheres48" else "prolate-ellipsoid", WORKLOADS[a.workload]["n"]),
-            "config": dict(workload_config(a.workload, B, world, a.precond), inner_tol=a.inner_tol,
-                           operator_tiles={"zchunk": tiles[0], "variant": ["staged", "lean"][tiles[1]]},
-                           amg_levels=[[list(g) for g in amgb.grids(k)[0]] for k in range(len(amgb.boxes))]
-                           if amgb is not None else None),
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "config": workload_config(a.workload, B, world),
+            "method": {"precision": "fp32 inner PCG + fp64 refinement", "preconditioner": PRECONDS[a.precond],
+                       "inner_tol": a.inner_tol,
+                       "operator_tiles": {"zchunk": tiles[0], "variant": ["staged", "lean"][tiles[1]]},
+                       "amg_levels": [[list(g) for g in amgb.grids(k)[0]] for k in range(len(amgb.boxes))]
+                       if amgb is not None else None},
+            "roofline": roofline, "cpu_baseline": cpu, "cpu_comparators": cpu_extra, "e2e": e2e,
             "clocks": clocks, "gpu_launches": gpu_launches, "all_converged": bool(ok),
             "inner_iters_mean": float(iters.mean()), "outer_steps": [i.outer for i in infos][:1],
+            "step_ms": [round(v, 3) for v in step_ms], "graphs": graphs,
             "fp64_gpu_cg": fp64_cg,
             "speedup_vs_fp64_gpu_cg": value / world / fp64_cg["solves_per_s"] if fp64_cg else None,
+            "reference_gpu_cg": torch_cg,
+            "speedup_vs_reference_gpu_cg": value / world / torch_cg["solves_per_s"] if torch_cg else None,
             "accuracy": accuracy}
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -93,6 +93,9 @@ typedef struct lpm_ir_opts {
 
 int lpm_abi_version(void);
 const char* lpm_status_string(int code);
+/* Diagnostics of the CUDA-graph cache behind the CG engines' iteration blocks: graphs captured so far, graphs held,
+ * and flushes of the bounded cache (process-wide).  No counterpart in the reference (it has no CUDA graphs). */
+void lpm_graph_stats(int64_t* captures, int64_t* entries, int64_t* flushes);
 
 /* ------------------------------------------------------------------------------------------------ coefficients */
 /* Pack (nset, n, slots) FP64 coefficients into the (nset, slots, n) layout in FP32 or FP64.
@@ -162,6 +165,20 @@ int lpm_cg_batched_f32(const lpm_lattice* lat, const float* Kn, const float* Tv,
  * freezing (same iteration counts up to the rounding of its reductions) and runs one cooperative kernel per solve:
  * three team barriers per iteration, each wait bounded in time (LPM_ERR_TIMEOUT on expiry). */
 int lpm_cg_persistent_fits(const lpm_lattice* lat, const lpm_batch* batch);
+
+/* ------------------------------------------------------------------------------------- assembled matrices */
+/* Workspace bytes of lpm_csr_pcg_f64 for an n x n matrix. */
+int64_t lpm_csr_workspace_bytes(int64_t n);
+
+/* K_ff x_f = b_f for an assembled sparse K (CSR: rowptr (n+1) int64, col int32, val FP64, device arrays) with the free
+ * set as a per-row mask (uint8, 1 = free; NULL = all free), by Jacobi-preconditioned CG in FP64 from x = 0, stopping
+ * when |r| <= tol |b| (tested every iteration).  x (n) receives the free part (zero on fixed rows); b is read on free
+ * rows only.  Replaces the SuperLU factorisation and solve of coarse2d/lin2d.py:166-180 (solve_disp), called from
+ * coarse2d/cg.py:64-76 for the 2D fine references.  opts: tol, maxit and poll are used (prof non-NULL turns off the
+ * graph replay).  iters / relres / status: DEVICE arrays of one element. */
+int lpm_csr_pcg_f64(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val, const uint8_t* mask,
+                    const double* b, double* x, const lpm_cg_opts* opts, void* workspace, size_t workspace_bytes,
+                    int32_t* iters, double* relres, int32_t* status, void* stream);
 
 /* ------------------------------------------------------------------------------- mixed-precision refinement */
 int64_t lpm_ir_workspace_bytes(const lpm_lattice* lat, const lpm_batch* batch, int32_t precond);
@@ -303,6 +320,13 @@ int lpm_tune_kmv_set(const lpm_lattice* lat, const lpm_batch* batch, int32_t zch
  * sites (n) int64 = site of each particle; nbr (n, slots) int64 out. */
 int lpm_build_nbr(int32_t dim, int32_t nx, int32_t ny, int32_t nz, int64_t n, const int64_t* site_of,
                   const int64_t* sites, int64_t* nbr, void* stream);
+
+/* Bond tables of specimens with voids on the full box (nx*ny*nz sites, all kept in the numbering): solid (nspec, n)
+ * uint8 (1 = solid); nbr (nspec, n, slots) int32 out, slot k of site i = its grid neighbour q if both i and q are
+ * solid, else -1.  This is the per-specimen bond validity gvalid & solid_i & solid_q of cement3d/torch_v1.py:37-45
+ * (SCTV.set_mask); each table is the nbr of an lpm_lattice for that specimen's operator calls. */
+int lpm_solid_nbr(int32_t dim, int32_t nx, int32_t ny, int32_t nz, int32_t nspec, const uint8_t* solid, int32_t* nbr,
+                  void* stream);
 
 #ifdef __cplusplus
 }

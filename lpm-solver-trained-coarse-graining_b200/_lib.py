@@ -47,6 +47,7 @@ class AmgOpts(ctypes.Structure):
 _SIGS = {
     "lpm_abi_version": ([], ctypes.c_int),
     "lpm_status_string": ([ctypes.c_int], ctypes.c_char_p),
+    "lpm_graph_stats": ([_P(_c_i64), _P(_c_i64), _P(_c_i64)], None),
     "lpm_pack_coef_f32": ([_c_p, _c_p, _c_i64, _c_i32, _c_i32, _c_p], ctypes.c_int),
     "lpm_pack_coef_f64": ([_c_p, _c_p, _c_i64, _c_i32, _c_i32, _c_p], ctypes.c_int),
     "lpm_kmv_scratch_bytes": ([_P(Lattice), _c_i32, _c_i32], _c_i64),
@@ -62,6 +63,9 @@ _SIGS = {
                             _c_p, _c_sz, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
     "lpm_cg_batched_f32": ([_P(Lattice), _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p, _c_p, _c_p, _c_i32, _P(CgOpts),
                             _c_p, _c_sz, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
+    "lpm_csr_workspace_bytes": ([_c_i64], _c_i64),
+    "lpm_csr_pcg_f64": ([_c_i64, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _P(CgOpts), _c_p, _c_sz, _c_p, _c_p, _c_p,
+                         _c_p], ctypes.c_int),
     "lpm_ir_workspace_bytes": ([_P(Lattice), _P(Batch), _c_i32], _c_i64),
     "lpm_ir_batched": ([_P(Lattice), _c_p, _c_p, _c_i32, _c_p, _c_p, _c_p, _P(Batch), _c_p, _c_p, _c_p, _P(IrOpts),
                         _c_p, _c_sz, _c_p, _c_p, _c_p, _P(_c_i32), _c_p], ctypes.c_int),
@@ -73,6 +77,7 @@ _SIGS = {
     "lpm_stress_f64": ([_P(Lattice), _c_p, _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_d, _c_p, _c_p, _c_sz, _c_p],
                        ctypes.c_int),
     "lpm_energy_f64": ([_P(Lattice), _c_p, _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p], ctypes.c_int),
+    "lpm_solid_nbr": ([_c_i32, _c_i32, _c_i32, _c_i32, _c_i32, _c_p, _c_p, _c_p], ctypes.c_int),
     "lpm_build_nbr": ([_c_i32, _c_i32, _c_i32, _c_i32, _c_i64, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
     "lpm_energy_vjp_f64": ([_P(Lattice), _c_p, _c_p, _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p, _c_p, _c_i32, _c_p,
                             _c_sz, _c_p], ctypes.c_int),
@@ -118,6 +123,13 @@ def load():
             fn.restype = res
         _lib = lib
     return _lib
+
+
+def graph_stats():
+    """(captures, graphs held, cache flushes) of the library's CUDA-graph cache, process-wide."""
+    c, e, f = _c_i64(0), _c_i64(0), _c_i64(0)
+    load().lpm_graph_stats(ctypes.byref(c), ctypes.byref(e), ctypes.byref(f))
+    return int(c.value), int(e.value), int(f.value)
 
 
 def exported_symbols():

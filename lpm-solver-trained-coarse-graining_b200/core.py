@@ -22,7 +22,9 @@ class DeviceLattice:
     Full boxes use implicit neighbours; lattices with inactive sites carry an int32 neighbour table on the device.
     """
 
-    def __init__(self, lat, device="cuda"):
+    def __init__(self, lat, device="cuda", nbr=None):
+        """nbr: optional (N, NN) int32 CUDA tensor of bonds that replaces the geometric ones (-1 = no bond), e.g. one
+        specimen's table from solid_tables(); the lattice then runs on the table kernels."""
         self.lat = lat
         self.device = torch.device(device)
         if self.device.type != "cuda":
@@ -33,7 +35,11 @@ class DeviceLattice:
         self.NN = lat.NN
         nz = lat.nz if lat.dim == 3 else 1
         self.nbr = None
-        if not lat.full:
+        if nbr is not None:
+            if tuple(nbr.shape) != (lat.N, lat.NN) or nbr.dtype != torch.int32 or not nbr.is_cuda:
+                raise ValueError("bond table must be a CUDA int32 tensor of shape (%d, %d)" % (lat.N, lat.NN))
+            self.nbr = nbr.contiguous()
+        elif not lat.full:
             self.nbr = torch.as_tensor(np.ascontiguousarray(lat.nbr, dtype=np.int32), device=self.device)
         self.c = L.Lattice(lat.dim, lat.nx, lat.ny, nz, lat.N, None if self.nbr is None else self.nbr.data_ptr())
         self.l0 = torch.as_tensor(np.asarray(lat.l0, float), device=self.device, dtype=_F64)
@@ -393,6 +399,23 @@ def post_vjp(dl, which, u, G, Kn, Tv):
                                     L.stream_ptr(uf.device))
     L.check(rc, "lpm_%s_vjp_f64" % which)
     return du.reshape(u.shape), gK, gT
+
+
+def solid_tables(lat, solid):
+    """Per-specimen bond tables (B, N, NN) int32 of the full box `lat` under solid masks (B, N) (bool CUDA tensor):
+    a bond exists iff it is geometric and both ends are solid (cement3d/torch_v1.py:37-45)."""
+    if not lat.full:
+        raise ValueError("solid masks apply to the full box (void particles stay in the numbering)")
+    L.require_cuda(solid)
+    B = solid.shape[0]
+    if tuple(solid.shape) != (B, lat.N):
+        raise ValueError("solid mask must be (B, %d)" % lat.N)
+    sm = solid.to(torch.uint8).contiguous()
+    out = torch.empty((B, lat.N, lat.NN), dtype=torch.int32, device=solid.device)
+    nz = lat.nz if lat.dim == 3 else 1
+    L.check(L.load().lpm_solid_nbr(lat.dim, lat.nx, lat.ny, nz, B, L.ptr(sm), L.ptr(out),
+                                   L.stream_ptr(solid.device)), "lpm_solid_nbr")
+    return out
 
 
 def build_nbr(lat, device="cuda"):

@@ -6,6 +6,7 @@
 #include "lpm_cg.h"
 #include "lpm_tma.h"
 #include "lpm_kernels.h"
+#include "lpm_graph.h"
 
 using namespace lpm;
 
@@ -156,6 +157,15 @@ int cg_impl(const lpm_lattice* lat, const T* Kn, const T* Tv, int32_t layout, co
 extern "C" {
 
 int lpm_abi_version(void) { return LPM_ABI_VERSION; }
+
+void lpm_graph_stats(int64_t* captures, int64_t* entries, int64_t* flushes)
+{
+    long long c = 0, e = 0, f = 0;
+    lpm::graph_stats(&c, &e, &f);
+    if (captures) *captures = c;
+    if (entries) *entries = e;
+    if (flushes) *flushes = f;
+}
 
 const char* lpm_status_string(int code)
 {
@@ -503,6 +513,15 @@ int lpm_tune_kmv_set(const lpm_lattice* lat, const lpm_batch* batch, int32_t zch
     const int npp = (bt.rhs_per_set + 1) / 2, nset = (bt.nsys + bt.rhs_per_set - 1) / bt.rhs_per_set;
     pair_zchunk_record(L.nx, L.ny, L.nz, nset * npp, zchunk, variant);
     return LPM_OK;
+}
+
+int lpm_solid_nbr(int32_t dim, int32_t nx, int32_t ny, int32_t nz, int32_t nspec, const uint8_t* solid, int32_t* nbr,
+                  void* stream)
+{
+    if ((dim != 2 && dim != 3) || nx < 1 || ny < 1 || nz < 1 || (dim == 2 && nz != 1) || nspec < 1 || nspec > 65535 ||
+        !solid || !nbr || (int64_t)nx * ny * nz > INT32_MAX)
+        return LPM_ERR_ARG;
+    return ret(launch_solid_nbr(dim, nx, ny, nz, nspec, solid, nbr, S(stream)));
 }
 
 int lpm_build_nbr(int32_t dim, int32_t nx, int32_t ny, int32_t nz, int64_t n, const int64_t* site_of,

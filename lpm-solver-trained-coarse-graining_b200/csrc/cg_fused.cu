@@ -846,7 +846,16 @@ int cg_solve_fused(const Lattice& L, const T* Kn, const T* Tv, const Batch& bt, 
 namespace {
 std::mutex g_graph_mu;
 std::map<GraphKey, cudaGraphExec_t>* g_graphs = new std::map<GraphKey, cudaGraphExec_t>();  // never destroyed
+long long g_graph_captures = 0, g_graph_flushes = 0;
 }  // namespace
+
+void graph_stats(long long* captures, long long* entries, long long* flushes)
+{
+    std::lock_guard<std::mutex> g(g_graph_mu);
+    if (captures) *captures = g_graph_captures;
+    if (entries) *entries = (long long)g_graphs->size();
+    if (flushes) *flushes = g_graph_flushes;
+}
 
 cudaGraphExec_t graph_find(const GraphKey& k)
 {
@@ -861,8 +870,10 @@ void graph_put(const GraphKey& k, cudaGraphExec_t e)
     if (g_graphs->size() >= 64) {  // bounded: drop everything (entries are cheap to capture again)
         for (auto& kv : *g_graphs) cudaGraphExecDestroy(kv.second);
         g_graphs->clear();
+        ++g_graph_flushes;
     }
     (*g_graphs)[k] = e;
+    ++g_graph_captures;
 }
 
 cudaStream_t graph_capture_stream()

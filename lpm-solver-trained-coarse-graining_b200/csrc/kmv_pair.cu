@@ -58,6 +58,12 @@ constexpr int PSW = PX + 2, PSH = PY + 2, PSPL = PSW * PSH;  // tile + 1-site ri
 constexpr int PTVW = 24;           // Tv sites per row (x0-4 .. x0+19)
 constexpr int PKNW = 24;           // Kn sites per row (x0 .. x0+23)
 constexpr int PNRING = PSPL - PNT;
+// Threads per CTA.  Lean: the 256 tile threads also take the 68 ring sites (threads 0..67).  Staged: three more warps
+// own the ring sites (threads 256..323), so the tile warps carry no ring work and phase 1 costs every warp about the
+// same; an idle lane of the last ring warp issues the TMA fills, off the tile warps' path.
+constexpr int PRING_THREADS = 96;
+__host__ __device__ constexpr int pair_threads(bool lean) { return lean ? PNT : PNT + PRING_THREADS; }
+static_assert(PNRING <= PRING_THREADS, "ring warps cover the ring");
 constexpr unsigned FULL18 = 0x3FFFFu;
 
 constexpr size_t PU_SLOT = (size_t)PUH * PUW * 4;
@@ -118,7 +124,7 @@ __host__ __device__ constexpr SlotGeo slot_geo(int k)
 __device__ __forceinline__ pair_t ld2(const float* p) { return *reinterpret_cast<const pair_t*>(p); }
 
 template <int MODE, bool LEAN>
-__global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
+__global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
     k_sc_pair(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ CUtensorMap tm_tv,
               const __grid_constant__ CUtensorMap tm_kn, PairArgs P)
 {
@@ -127,7 +133,7 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
     constexpr int BTV = NUS, BKN = NUS + 2, NBAR = NUS + 4;  // mbarriers: u 0..NUS-1, Tv BTV.., Kn BKN..
     __shared__ __align__(8) uint64_t bars[NBAR];
     __shared__ double red[32];
-    __shared__ int abort_flag;
+    __shared__ int abort_flag;  // set before the first block barrier only (shared-memory alignment check)
     __shared__ bool last_flag;
 
     float* su = reinterpret_cast<float*>(smem);
@@ -135,8 +141,12 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
     float* skn = reinterpret_cast<float*>(smem + off_kn(LEAN));
     float4* sba = reinterpret_cast<float4*>(smem + off_ba(LEAN));
 
+    constexpr int NTH = pair_threads(LEAN);
     const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31;
+    const bool tile_thr = tid < PNT;  // owns a site of the tile (all threads of the lean variant)
     const int tx = lane & 15, ty = ((wid >> 1) << 2) + (wid & 1) + ((lane >> 4) << 1);
+    // the thread that issues the TMA fills and tracks them for the drain on abort
+    const bool producer = tid == (LEAN ? 0 : NTH - 1);
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const int ntx = (nx + PX - 1) / PX, nty = (ny + PY - 1) / PY;
     const int tile = blockIdx.x % (ntx * nty), zc = blockIdx.x / (ntx * nty);
@@ -187,10 +197,10 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
     }
     {
         const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int e = tid; e < NBAS * 2 * PSPL; e += PNT) sba[e] = z4;
+        for (int e = tid; e < NBAS * 2 * PSPL; e += NTH) sba[e] = z4;
         // u slots standing for planes below 0 are never loaded; keep them finite
         const int nneg = zbeg - 2 < 0 ? 2 - zbeg : 0;
-        for (int e = tid; e < nneg * (int)(PU_SLOT / 4); e += PNT) su[e] = 0.f;
+        for (int e = tid; e < nneg * (int)(PU_SLOT / 4); e += NTH) su[e] = 0.f;
     }
     __syncthreads();
     if (abort_flag) any_on = false;
@@ -239,13 +249,16 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
         tma_load4(skn + (size_t)(n & 1) * (PKN_SLOT / 4), &tm_kn, bar, x0, y0, p, 18 * set);
         note(BKN + (n & 1), (n >> 1) & 1);
     };
-    // Every thread waits (bounded) for the in-range fills it is about to read; an expired wait raises the abort
-    // flag, which all threads test after the next block barrier.
+    // Every thread waits (bounded) for the in-range fills it is about to read; an expired wait sets the thread's own
+    // `lost` flag, and the next block barrier ORs the flags of all threads (__syncthreads_or), so every thread takes
+    // the same abort decision at the same barrier.  A shared flag would not do: a fast warp could raise it for step
+    // z+1 before a slow warp has read it after step z's barrier, and the two would then wait at different barriers.
+    bool lost = false;
     auto wait_fill = [&](int b, int parity) {
         if (!mbar_wait(&bars[b], (uint32_t)parity)) {
-            abort_flag = 1;
+            lost = true;
             if (P.err) atomicExch(P.err, 1);
-        } else if (tid == 0) {
+        } else if (producer) {
             pend &= ~(1u << b);
         }
     };
@@ -263,7 +276,7 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
     auto zero_ba = [&](int p) {
         float4* d = ba_slot(p);
         const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int e = tid; e < 2 * PSPL; e += PNT) d[e] = z4;
+        for (int e = tid; e < 2 * PSPL; e += NTH) d[e] = z4;
     };
 
     // ---------------------------------------------------------------------------------------------- phase 1
@@ -389,22 +402,23 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
     };
 
     const int gx = x0 + tx, gy = y0 + ty;
-    const bool own_xy = gx < nx && gy < ny;
+    const bool own_xy = tile_thr && gx < nx && gy < ny;
     const unsigned own_mxy = xy_mask(gx, gy);
-    const bool has_item = tid < PNRING;
+    const int rit = LEAN ? tid : tid - PNT;  // ring item of this thread
+    const bool has_item = rit >= 0 && rit < PNRING;
     int rqx = 0, rqy = 0;
-    if (tid < PSW) {
-        rqx = tid;
+    if (rit < PSW) {
+        rqx = rit;
         rqy = 0;
-    } else if (tid < 2 * PSW) {
-        rqx = tid - PSW;
+    } else if (rit < 2 * PSW) {
+        rqx = rit - PSW;
         rqy = PSH - 1;
-    } else if (tid < 2 * PSW + PY) {
+    } else if (rit < 2 * PSW + PY) {
         rqx = 0;
-        rqy = tid - 2 * PSW + 1;
+        rqy = rit - 2 * PSW + 1;
     } else {
         rqx = PSW - 1;
-        rqy = tid - 2 * PSW - PY + 1;
+        rqy = rit - 2 * PSW - PY + 1;
     }
     const int rX = x0 - 1 + rqx, rY = y0 - 1 + rqy;
     const bool ring_in = has_item && rX >= 0 && rX < nx && rY >= 0 && rY < ny;
@@ -523,7 +537,7 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
     // that ends the phase 1 reading its single slot.
     bool ok = true;
     if (any_on) {
-        if (tid == 0) {
+        if (producer) {
             for (int p = zbeg - 2; p <= zbeg + 1; ++p) issue_u(p);
             issue_tv(zbeg - 1);
             if constexpr (!LEAN) {
@@ -536,10 +550,9 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
         wait_planes(zbeg - 1, zbeg - 1, -1);
         wait_planes(zbeg, -1, -1);
         phase1(zbeg - 1, false);
-        __syncthreads();
-        ok = !abort_flag;
+        ok = !__syncthreads_or(lost);
         if (ok) {
-            if (tid == 0) {
+            if (producer) {
                 fence_proxy_async();
                 if (zbeg + 2 <= zend + 1) issue_u(zbeg + 2);
                 if constexpr (LEAN)
@@ -549,9 +562,8 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
             }
             wait_planes(zbeg + 1, zbeg, zbeg);
             phase1(zbeg, true);
-            __syncthreads();
-            ok = !abort_flag;
-            if (LEAN && ok && tid == 0) {
+            ok = !__syncthreads_or(lost);
+            if (LEAN && ok && producer) {
                 fence_proxy_async();
                 if (zbeg + 1 <= zend) issue_tv(zbeg + 1);
             }
@@ -564,7 +576,7 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
 #pragma unroll
                     for (int k = 0; k < 18; ++k) tv_cur[k] = tv_next[k];
                 }
-                if (tid == 0) {
+                if (producer) {
                     fence_proxy_async();
                     if (z + 3 <= zend + 1) issue_u(z + 3);
                     if constexpr (!LEAN) {
@@ -574,12 +586,11 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
                 }
                 wait_planes(z + 2, z + 1, z + 1);
                 phase1(z + 1, z + 1 < zend);
-                __syncthreads();
-                if (abort_flag) {
+                if (__syncthreads_or(lost)) {  // uniform: every thread leaves the loop at this barrier
                     ok = false;
                     break;
                 }
-                if (LEAN && tid == 0) {  // the Tv slot is free: fill it with the plane of the next phase 1
+                if (LEAN && producer) {  // the Tv slot is free: fill it with the plane of the next phase 1
                     fence_proxy_async();
                     if (z + 2 <= zend) issue_tv(z + 2);
                 }
@@ -591,7 +602,7 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
                 if constexpr (LEAN) __syncthreads();
             }
         }
-        if (!ok && tid == 0) {  // let the copies in flight land before the block's shared memory is released
+        if (!ok && producer) {  // let the copies in flight land before the block's shared memory is released
             for (int b = 0; b < NBAR; ++b)
                 if ((pend >> b) & 1u) mbar_wait(&bars[b], (ppar >> b) & 1u);
         }
@@ -613,7 +624,7 @@ __global__ void __launch_bounds__(PNT, LEAN ? 2 : 1)
             __syncthreads();
             if (last_flag) {
                 double acc = 0.0;
-                for (int b = tid; b < nblk; b += PNT) acc += __ldcg(P.part + (int64_t)s * nblk + b);
+                for (int b = tid; b < nblk; b += NTH) acc += __ldcg(P.part + (int64_t)s * nblk + b);
                 acc = block_sum(acc, red);
                 if (tid == 0) {
                     P.cnt[s] = 0u;
@@ -678,7 +689,7 @@ cudaError_t launch_pair(const PairArgs& a, cudaStream_t st)
         PairArgs b = a;
         b.pair0 = g0;
         const int ng = a.npair - g0 < 65535 ? a.npair - g0 : 65535;
-        k_sc_pair<MODE, LEAN><<<dim3(ntile * nzc, ng), PNT, pair_bytes(LEAN), st>>>(mu, mtv, mkn, b);
+        k_sc_pair<MODE, LEAN><<<dim3(ntile * nzc, ng), pair_threads(LEAN), pair_bytes(LEAN), st>>>(mu, mtv, mkn, b);
     }
     return cudaGetLastError();
 }

@@ -155,6 +155,13 @@ __global__ void __launch_bounds__(TX* TY, 1)
     constexpr uint32_t TV_BYTES = (uint32_t)(18 * SH * TVW * sizeof(T));
     constexpr uint32_t KN_BYTES = (uint32_t)(18 * TY * TX * sizeof(T));
     const int coef_plane0 = set * 18;  // 4th tensor coordinate of slot 0 of this set
+    // Thread 0 keeps the parity of the last fill issued on each barrier (bit b of `ppar`, and bit b of `pend` while
+    // it may still be in flight) so that an aborting block can let its copies land before it exits.
+    unsigned pend = 0, ppar = 0;
+    auto note = [&](int b, int parity) {
+        pend |= 1u << b;
+        ppar = (ppar & ~(1u << b)) | ((unsigned)parity << b);
+    };
     auto issue_u = [&](int p) {
         const int n = p - u0;
         uint64_t* bar = &bars[n & 3];
@@ -164,6 +171,7 @@ __global__ void __launch_bounds__(TX* TY, 1)
         }
         mbar_expect_arrive(bar, U_BYTES);
         tma_load4(su + (size_t)(n & 3) * (Lay::U_SLOT / sizeof(T)), &tm_u, bar, 3 * x0 - 8, y0 - 2, p, sbase);
+        note(n & 3, (n >> 2) & 1);
     };
     auto issue_tv = [&](int p) {
         const int n = p - tv0;
@@ -174,6 +182,7 @@ __global__ void __launch_bounds__(TX* TY, 1)
         }
         mbar_expect_arrive(bar, TV_BYTES);
         tma_load4(stv + (size_t)(n & 1) * (Lay::TV_SLOT / sizeof(T)), &tm_tv, bar, x0 - 4, y0 - 1, p, coef_plane0);
+        note(4 + (n & 1), (n >> 1) & 1);
     };
     auto issue_kn = [&](int p) {
         const int n = p - kn0;
@@ -184,25 +193,24 @@ __global__ void __launch_bounds__(TX* TY, 1)
         }
         mbar_expect_arrive(bar, KN_BYTES);
         tma_load4(skn + (size_t)(n & 1) * (Lay::KN_SLOT / sizeof(T)), &tm_kn, bar, x0, y0, p, coef_plane0);
+        note(6 + (n & 1), (n >> 1) & 1);
     };
     // Thread 0 waits (bounded) for the listed in-range fills, then the block synchronises; every thread then
-    // observes the completed phases itself (immediate) before reading.
+    // observes the completed phases itself (immediate) before reading.  The abort decision is the OR over the block
+    // at that barrier (__syncthreads_or), so all threads return at the same step: a shared flag written by thread 0
+    // could already hold the next step's expiry when a slow warp reads it.
     auto wait_planes = [&](int pu, int ptv, int pkn) -> bool {
         auto ok_u = [&](int p) { return p >= 0 && p < nz && p >= u0; };
         auto ok_tv = [&](int p) { return p >= 0 && p < nz && p >= tv0; };
         auto ok_kn = [&](int p) { return p >= 0 && p < nz && p >= kn0 && p < zend; };
+        bool good = true;
         if (tid == 0) {
-            bool good = true;
             if (ok_u(pu)) good = good && mbar_wait(&bars[(pu - u0) & 3], ((pu - u0) >> 2) & 1);
             if (ok_tv(ptv)) good = good && mbar_wait(&bars[4 + ((ptv - tv0) & 1)], ((ptv - tv0) >> 1) & 1);
             if (ok_kn(pkn)) good = good && mbar_wait(&bars[6 + ((pkn - kn0) & 1)], ((pkn - kn0) >> 1) & 1);
-            if (!good) {
-                abort_flag = 1;
-                if (P.err) atomicExch(P.err, 1);
-            }
+            if (!good && P.err) atomicExch(P.err, 1);
         }
-        __syncthreads();
-        if (abort_flag) return false;
+        if (__syncthreads_or(!good)) return false;
         if (ok_u(pu)) mbar_wait(&bars[(pu - u0) & 3], ((pu - u0) >> 2) & 1);
         if (ok_tv(ptv)) mbar_wait(&bars[4 + ((ptv - tv0) & 1)], ((ptv - tv0) >> 1) & 1);
         if (ok_kn(pkn)) mbar_wait(&bars[6 + ((pkn - kn0) & 1)], ((pkn - kn0) >> 1) & 1);
@@ -497,6 +505,10 @@ __global__ void __launch_bounds__(TX* TY, 1)
                 phase2(z);
                 __syncthreads();
             }
+        }
+        if (!ok && tid == 0) {  // let the copies in flight land (bounded) before the block's shared memory is released
+            for (int b = 0; b < 8; ++b)
+                if ((pend >> b) & 1u) mbar_wait(&bars[b], (ppar >> b) & 1u);
         }
     }
 

@@ -69,6 +69,10 @@ cudaError_t launch_post_vjp(const Lattice& L, int which, const double* u, const 
                             const double* Tv, const CoefLayout& cl, const Batch& bt, const double* l0, double V,
                             double* du, double* gK, double* gT, double* scratch, int acc, cudaStream_t st);
 
+// Per-specimen bond tables (nspec, nx*ny*nz, NN) int32 of a full box with per-specimen solid masks (nspec, n) uint8.
+cudaError_t launch_solid_nbr(int dim, int nx, int ny, int nz, int nspec, const uint8_t* solid, int32_t* nbr,
+                             cudaStream_t st);
+
 // Neighbour table (n, NN) int64 of a masked box, same values as the reference's LatticeGeom.nbr.
 cudaError_t launch_build_nbr(int dim, int nx, int ny, int nz, int64_t n, const int64_t* site_of, const int64_t* sites,
                              int64_t* nbr, cudaStream_t st);

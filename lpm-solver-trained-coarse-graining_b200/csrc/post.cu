@@ -221,6 +221,32 @@ __global__ void k_build_nbr(int nx, int ny, int nz, int64_t n, const int64_t* __
     }
 }
 
+// Bond table of one specimen with voids on the full box: slot k of site i exists iff the geometric neighbour q is
+// inside the box and both i and q are solid (cement3d/torch_v1.py:37-45, valid = gvalid & solid_i & solid_q).
+template <int DIM>
+__global__ void k_solid_nbr(int nx, int ny, int nz, const uint8_t* __restrict__ solid, int32_t* __restrict__ nbr)
+{
+    using S = Slots<DIM>;
+    const int64_t n = (int64_t)nx * ny * nz;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t b = blockIdx.y;
+    const uint8_t* sb = solid + b * n;
+    int32_t* o = nbr + (b * n + i) * S::NN;
+    const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((int64_t)nx * ny));
+    const bool si = sb[i] != 0;
+#pragma unroll
+    for (int k = 0; k < S::NN; ++k) {
+        const int qx = x + S::dx(k), qy = y + S::dy(k), qz = z + S::dz(k);
+        int32_t q = -1;
+        if (si && qx >= 0 && qx < nx && qy >= 0 && qy < ny && qz >= 0 && qz < nz) {
+            const int64_t qi = ((int64_t)qz * ny + qy) * nx + qx;
+            if (sb[qi]) q = (int32_t)qi;
+        }
+        o[k] = q;
+    }
+}
+
 template <int DIM, class NB, typename F>
 cudaError_t per_system(NB, const Lattice& L, int nsys, cudaStream_t st, F&& launch)
 {
@@ -336,6 +362,19 @@ cudaError_t launch_pack(const double* src, T* dst, int64_t N, int NN, int nset, 
 
 template cudaError_t launch_pack<float>(const double*, float*, int64_t, int, int, cudaStream_t);
 template cudaError_t launch_pack<double>(const double*, double*, int64_t, int, int, cudaStream_t);
+
+cudaError_t launch_solid_nbr(int dim, int nx, int ny, int nz, int nspec, const uint8_t* solid, int32_t* nbr,
+                             cudaStream_t st)
+{
+    const int64_t n = (int64_t)nx * ny * nz;
+    const unsigned g = (unsigned)((n + 255) / 256);
+    if (g == 0 || nspec < 1) return cudaSuccess;
+    if (dim == 3)
+        k_solid_nbr<3><<<dim3(g, nspec), 256, 0, st>>>(nx, ny, nz, solid, nbr);
+    else
+        k_solid_nbr<2><<<dim3(g, nspec), 256, 0, st>>>(nx, ny, 1, solid, nbr);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_build_nbr(int dim, int nx, int ny, int nz, int64_t n, const int64_t* site_of, const int64_t* sites,
                              int64_t* nbr, cudaStream_t st)

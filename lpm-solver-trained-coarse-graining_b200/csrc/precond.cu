@@ -86,8 +86,13 @@ __global__ void __launch_bounds__(256) k_block_jacobi(NB nb, int nx, int ny, int
         M[2] = -D[1][0] / det;
         M[3] = D[0][0] / det;
     }
+    // A particle without bonds (a void of a specimen with voids) has D = 0: its block is never used on a free DOF,
+    // so store zero rather than 0/0, which would reach the engines' masked products as NaN * 0.
+    bool finite = true;
 #pragma unroll
-    for (int a = 0; a < DIM * DIM; ++a) Minv[o + a] = (T)M[a];
+    for (int a = 0; a < DIM * DIM; ++a) finite = finite && isfinite(M[a]);
+#pragma unroll
+    for (int a = 0; a < DIM * DIM; ++a) Minv[o + a] = finite ? (T)M[a] : T(0);
 }
 
 template <typename T, int DIM, class NB>

@@ -96,9 +96,9 @@ class LatticeOperator:
     SC lattice: code-force operator (coarse3d/torch_lpm3d.py:63-83); square lattice: exact-Hessian operator
     (timing/t2d/solver2d.py:269-305, coarse2d/torch_lpm.py:173-191)."""
 
-    def __init__(self, lat, device="cuda", dtype=_F64):
+    def __init__(self, lat, device="cuda", dtype=_F64, dl=None):
         self.lat, self.dev, self.dt = lat, torch.device(device), dtype
-        self.dl = core.DeviceLattice(lat, device)
+        self.dl = core.DeviceLattice(lat, device) if dl is None else dl
         self.N = lat.N
         self.ndir = torch.as_tensor(lat.ndir, device=self.dev, dtype=dtype)
         self.valid = torch.as_tensor(lat.valid, device=self.dev, dtype=dtype)
@@ -156,7 +156,7 @@ class LatticeOperator:
         nsys = int(np.prod(lead)) if lead else 1
         rps = nsys // Kc.shape[0]
         layout = _lib.LAYOUT_REF
-        if self.lat.full and self.d == 3:      # full SC boxes run on the packed (SoA) layout, the fused operator path
+        if self.dl.nbr is None and self.d == 3:   # full SC boxes run on the packed (SoA) layout, the fused operator
             Kc, Tc, layout = core.pack(Kc, self.dt), core.pack(Tc, self.dt), _lib.LAYOUT_SOA
         x, info = core.cg(self.dl, Kc, Tc, b.reshape(nsys, self.N, self.d),
                           x=None if x0 is None else x0.expand(tuple(lead) + (self.N, self.d)).reshape(nsys, self.N, self.d),
@@ -164,6 +164,10 @@ class LatticeOperator:
                           maxit=maxit, check=check, layout=layout, rhs_per_set=rps)
         x = x.reshape(tuple(lead) + (self.N, self.d))
         return x, info
+
+    def bond_grad(self, u, lam, Kn, Tv):
+        """Per-slot d(lam . K(Kn, Tv) u)/d(Kn, Tv), summed over the systems sharing each coefficient set."""
+        return core.bond_grad(self.dl, u, lam, Kn, Tv)
 
     def pcg(self, b, Kn, Tv, M, free, tol=1e-10, maxit=20000, x0=None, check=10):
         """Solve K_ff x = b for all systems (coarse3d/torch_lpm3d.py:109-140).  Returns (x, iterations, max rel)."""
@@ -253,7 +257,7 @@ class LinSolve(torch.autograd.Function):
         with torch.no_grad():
             lam, info = op._solve_sets(g * free[..., None], Kn, Tv, free, ctx.tol, 20000, 10)
             info.raise_on_breakdown()
-            gK, gT = core.bond_grad(op.dl, u, lam, Kn, Tv)
+            gK, gT = op.bond_grad(u, lam, Kn, Tv)
             lead = u.shape[:-2]
             dK = -_sum_to(gK, Kn, lead).to(Kn.dtype)
             dT = -_sum_to(gT, Tv, lead).to(Tv.dtype)

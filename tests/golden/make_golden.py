@@ -1,8 +1,9 @@
 """Generates the golden fixtures of tests/golden/ by running the reference itself (FP64, CPU).
 
-Run in a container that holds the reference checkout (default /root/reference, or $LPM_REFERENCE):
+Run where the reference checkout is available, with LPM_REFERENCE set to its root directory:
 
-    python tests/golden/make_golden.py            # all parts, each in a fresh interpreter
+    LPM_REFERENCE=<reference checkout> python tests/golden/make_golden.py          # all parts, fresh interpreters
+    LPM_REFERENCE=<reference checkout> python tests/golden/make_golden.py cfg3     # one part
 
 The reference is imported read-only: Numba's cache goes to a temporary directory, and the two modules that create
 folders inside the reference tree at import time (timing/t2d/a2common.py, timing/t3d/common.py) are replaced by stubs.
@@ -14,6 +15,13 @@ Parts:
          torch_lpm dense-assembly gradient of lam^T K u and of the CoarseT.run losses (as coarse2d/check_gradient.py)
   amg    aggregation AMG of timing/t3d/amg3d.py with the settings of timing/t3d/problems.py (geometry, levels, rho,
          one cycle, PCG iterations; 14^3 and the 48^3 bench specimen) and geom3d.interface_cells
+  sctv   the per-specimen void operator of cement3d/torch_v1.py (SCTV, CoarseTV): apply, stress, energy and block
+         diagonals under two specimens' solid masks, and a differentiable CoarseTV.run (9 loads) with its loss gradient
+  cfg3   the differentiable 2D coarse solve of the benchmark's third configuration at nc = 32 and 48 (the sizes the
+         reference's dense torch_lpm path handles): GRF fine field -> Voigt cells -> two-end-mean bonds (coarse2d/
+         micro.py, coarse2d/cg.py:201-234), lognormal(0.2) factors per undirected bond rounded to FP32, loads lr_tx,
+         tb_ty, tb_sx, loss = sum over loads of the MSE of u against a seeded target, and its gradient w.r.t. the log
+         bond stiffness theta from torch_lpm.CoarseT.run (dense assembly + Cholesky, torch autograd)
 """
 import os
 import subprocess
@@ -21,7 +29,7 @@ import sys
 import tempfile
 import types
 
-REF = os.environ.get("LPM_REFERENCE", "/root/reference")
+REF = os.environ.get("LPM_REFERENCE", "")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -438,9 +446,117 @@ def part_amg():
     print("golden_amg.npz:", len(out), "arrays")
 
 
-PARTS = {"sc": part_sc, "sq": part_sq, "grad": part_grad, "amg": part_amg}
+def part_cfg3():
+    """Dense-Cholesky gradient of the reference's 2D coarse model on the third benchmark configuration's inputs, at
+    the coarse sizes its dense path reaches (nc = 32 from a 64^2 fine field, nc = 48 from 96^2; s = 2)."""
+    _env()
+    sys.path.insert(0, os.path.join(REF, "coarse2d"))
+    import numpy as np
+    import torch
+    import cg as CG
+    import lin2d as L2
+    import micro as MI
+    import torch_lpm as T2
+    torch.set_default_dtype(torch.float64)
+    out = {}
+    loads = ["lr_tx", "tb_ty", "tb_sx"]
+    for nc in (32, 48):
+        s = 2
+        nf = nc * s
+        ph = MI.grf_two_phase(nf, nf, 6.0, 0.30, 3)
+        E = np.where(ph == 1, 10.0, 1.0)
+        Cpix = L2.iso_C(E, 0.25, plane="stress")
+        m = T2.CoarseT(nc, nc, s, 1.0, device="cpu", loads=loads)
+        lat = m.lat
+        cp = CG.cell_params_from_C6(CG.voigt_cells(Cpix, nf, nf, s))
+        K0, T0 = CG.bond_params_from_cells(lat, cp)
+        rng = np.random.default_rng(11)
+        q = np.where(lat.valid, lat.nbr, 0)
+        opp = np.repeat(lat.opp[None, :], lat.N, 0)
+
+        def lognormal_sym(rg):
+            z = rg.standard_normal((lat.N, 8))
+            z = np.where(np.arange(8)[None, :] % 2 == 0, z, z[q, opp])      # one factor per undirected bond
+            return np.exp(0.2 * z)
+        f0 = lognormal_sym(rng).astype(np.float32).astype(np.float64)
+        ft = lognormal_sym(rng)
+        with torch.no_grad():
+            tgt = m.run(torch.tensor(K0 * ft)[None], torch.tensor(T0)[None])
+        tgt = {ld: v["u"] for ld, v in tgt.items()}
+        Kb = torch.tensor(K0 * f0)[None]
+        Tb = torch.tensor(T0)[None]
+        qt, ot = torch.as_tensor(q), torch.as_tensor(opp)
+        valid = torch.as_tensor(lat.valid, dtype=torch.float64)
+        th = torch.zeros((1, lat.N, 8), requires_grad=True)
+        Kn = Kb * torch.exp(0.5 * (th + th[:, qt, ot])) * valid
+        o = m.run(Kn, Tb)
+        L = sum(((o[ld]["u"] - tgt[ld]) ** 2).mean() for ld in loads)
+        L.backward()
+        pre = "n%d_" % nc
+        out.update({pre + "ph": ph, pre + "K0": K0, pre + "T0": T0, pre + "Kb": Kb.numpy()[0], pre + "loss": float(L),
+                    pre + "gth": th.grad.numpy()[0]})
+        for ld in loads:
+            out[pre + "tgt_" + ld] = tgt[ld].numpy()[0]
+            out[pre + "u_" + ld] = o[ld]["u"].detach().numpy()[0]
+        print("nc", nc, "loss", float(L))
+    np.savez_compressed(os.path.join(HERE, "golden_cfg3.npz"), **out)
+    print("golden_cfg3.npz:", len(out), "arrays")
+
+
+def part_sctv():
+    """cement3d/torch_v1.py on a 6^3 coarse grid (s = 2) with two specimens whose solid masks remove ~20% of the
+    cells: the operator's outputs under the masks and the gradient of a loss through CoarseTV.run (LinSolve)."""
+    _env()
+    sys.path.insert(0, os.path.join(REF, "coarse3d"))
+    sys.path.insert(0, os.path.join(REF, "cement3d"))
+    import numpy as np
+    import torch
+    import torch_v1 as TV
+    torch.set_default_dtype(torch.float64)
+    out = {}
+    nc, s, B = 6, 2, 2
+    cm = TV.CoarseTV(nc, s, device="cpu")
+    lat = cm.lat
+    N = lat.N
+    rng = np.random.default_rng(31)
+    solid = rng.random((B, N)) > 0.2
+    Kn = np.zeros((B, N, 18))
+    Tv = np.zeros((B, N, 18))
+    for b in range(B):
+        for i in range(N):
+            for k in range(0, 18, 2):
+                q = lat.nbr[i, k]
+                if q >= 0:
+                    Kn[b, i, k] = Kn[b, q, k ^ 1] = rng.uniform(0.8, 1.2)
+                    Tv[b, i, k] = Tv[b, q, k ^ 1] = rng.uniform(-0.03, 0.03)
+    op = cm.op
+    st = torch.as_tensor(solid)
+    op.set_mask(st)
+    u = rng.standard_normal((B, 2, N, 3))
+    Kt, Tt = torch.tensor(Kn)[:, None], torch.tensor(Tv)[:, None]
+    out.update(solid=solid, Kn=Kn, Tv=Tv, u=u, valid=op.vb.numpy()[:, 0],
+               Ku=op.apply(torch.tensor(u), Kt, Tt).numpy(), sig=op.stress(torch.tensor(u), Kt, Tt).numpy(),
+               w=op.energy(torch.tensor(u), Kt, Tt).numpy(), D=op.block_diag(Kt, Tt).numpy())
+    # differentiable CoarseTV.run: loss = sum of squares of u and stresses against fixed weights
+    Kg = torch.tensor(Kn, requires_grad=True)
+    Tg = torch.tensor(Tv, requires_grad=True)
+    r = cm.run(Kg, Tg, cell=st, tol=1e-12)
+    Wu = rng.standard_normal(tuple(r["u"].shape))
+    Ws = rng.standard_normal(tuple(r["sig"].shape))
+    L = (r["u"] * torch.tensor(Wu)).sum() * 1e3 + (r["sig"] * torch.tensor(Ws)).sum() * 1e3
+    L.backward()
+    out.update(run_u=r["u"].detach().numpy(), run_sig=r["sig"].detach().numpy(), run_w=r["w"].detach().numpy(),
+               run_F=r["F"].detach().numpy(), Wu=Wu, Ws=Ws, loss=float(L.detach()), gKn=Kg.grad.numpy(),
+               gTv=Tg.grad.numpy())
+    np.savez_compressed(os.path.join(HERE, "golden_sctv.npz"), **out)
+    print("golden_sctv.npz:", len(out), "arrays")
+
+
+PARTS = {"sc": part_sc, "sq": part_sq, "grad": part_grad, "amg": part_amg, "cfg3": part_cfg3, "sctv": part_sctv}
 
 if __name__ == "__main__":
+    if not REF or not os.path.isdir(REF):
+        sys.exit("set LPM_REFERENCE to the root of the reference checkout")
     if len(sys.argv) > 1 and sys.argv[1] in PARTS:
         PARTS[sys.argv[1]]()
     else:

@@ -69,3 +69,23 @@ def test_generators(gsc, gsq):
     assert np.array_equal(micro.ellipsoids(16, 16, 16, 0.3, 3.0, np.random.default_rng(8), aspect=(3.0, 3.0),
                                            rjit=0.0)[0], gsc["gen_ellip"])
     assert np.array_equal(micro.grf3(12, 12, 12, 2.0, 0.3, np.random.default_rng(9))[0], gsc["gen_grf3"])
+
+
+def test_cfg3_inputs_match_reference():
+    """The third configuration's coarse-parameter pipeline (GRF fine field -> Voigt cells -> two-end-mean bonds,
+    coarse2d/micro.py:13-20 and coarse2d/cg.py:201-234) reproduces the reference's arrays at nc = 32 and 48."""
+    from lpm_b200 import micro
+    from conftest import GOLDEN
+    import os
+    with np.load(os.path.join(GOLDEN, "golden_cfg3.npz")) as d:
+        g = {k: d[k] for k in d.files}
+    for nc in (32, 48):
+        pre = "n%d_" % nc
+        nf = 2 * nc
+        ph = micro.grf_two_phase(nf, nf, 6.0, 0.30, 3)
+        assert np.array_equal(ph, g[pre + "ph"])
+        Cpix = G.iso_C2d(np.where(ph == 1, 10.0, 1.0), 0.25, plane="stress")
+        lat = G.SquareLattice(nc, nc, 2.0)
+        cp = G.cell_params_from_C6(G.voigt_cells2d(Cpix, nf, nf, 2))
+        K0, T0 = G.bond_params_from_cells2d(lat, cp)
+        assert relmax(K0, g[pre + "K0"]) < 1e-15 and relmax(T0, g[pre + "T0"]) < 1e-15

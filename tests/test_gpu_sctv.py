@@ -1,0 +1,108 @@
+"""Per-specimen voids (torch_v1.SCTV / CoarseTV / FineRefTV, the drop-in for cement3d/torch_v1.py) against the
+reference's own outputs (tests/golden/golden_sctv.npz, made by running cement3d/torch_v1.py on the CPU) and, for a
+voided 48^3 specimen, against the CPU oracle's FP64 PCG on the same bond tables.
+
+Bars: operator outputs 1e-13 (FP64) and 3e-6 (FP32); solves to 1e-12 and their gradients 1e-8 / 1e-7; the mixed
+solve 1e-6 relative displacement."""
+import os
+import types
+
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from conftest import GOLDEN, relmax
+from lpm_b200 import core
+from lpm_b200 import geom as G
+from lpm_b200 import micro as M
+from lpm_b200 import torch_v1 as TV
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda")
+
+
+@pytest.fixture(scope="module")
+def gv():
+    with np.load(os.path.join(GOLDEN, "golden_sctv.npz")) as d:
+        return {k: d[k] for k in d.files}
+
+
+def T(a, grad=False, dt=torch.float64):
+    return torch.tensor(np.asarray(a), device=DEV, dtype=dt, requires_grad=grad)
+
+
+def test_solid_tables_match_reference_validity(gv):
+    cm = TV.CoarseTV(6, 2, device=DEV)
+    tabs = core.solid_tables(cm.lat, torch.as_tensor(gv["solid"], device=DEV))
+    assert np.array_equal((tabs >= 0).cpu().numpy(), gv["valid"])
+    cm.op.set_mask(torch.as_tensor(gv["solid"], device=DEV))
+    assert np.array_equal(cm.op.vb[:, 0].cpu().numpy(), gv["valid"])
+
+
+def test_sctv_operator_outputs(gv):
+    cm = TV.CoarseTV(6, 2, device=DEV)
+    op = cm.op
+    op.set_mask(torch.as_tensor(gv["solid"], device=DEV))
+    u, Kn, Tv = T(gv["u"]), T(gv["Kn"])[:, None], T(gv["Tv"])[:, None]
+    assert relmax(op.apply(u, Kn, Tv).cpu().numpy(), gv["Ku"]) < 1e-13
+    assert relmax(op.stress(u, Kn, Tv).cpu().numpy(), gv["sig"]) < 1e-13
+    assert relmax(op.energy(u, Kn, Tv).cpu().numpy(), gv["w"]) < 1e-13
+    assert relmax(op.block_diag(Kn, Tv).cpu().numpy(), gv["D"]) < 1e-13
+    op32 = TV.SCTV(cm.lat, DEV, torch.float32)
+    op32.set_mask(torch.as_tensor(gv["solid"], device=DEV))
+    f32 = op32.apply(u.float(), Kn.float(), Tv.float()).double().cpu().numpy()
+    assert relmax(f32, gv["Ku"]) < 3e-6
+
+
+def test_sctv_no_mask_is_the_plain_operator(gv):
+    cm = TV.CoarseTV(6, 2, device=DEV)
+    u, Kn, Tv = T(gv["u"]), T(gv["Kn"])[:, None], T(gv["Tv"])[:, None]
+    cm.op.set_mask(None)
+    a = cm.op.apply(u, Kn, Tv)
+    b = cm.op.base.apply(u, Kn, Tv)
+    assert torch.equal(a, b)
+
+
+def test_coarsetv_run_and_gradient(gv):
+    cm = TV.CoarseTV(6, 2, device=DEV)
+    Kg, Tg = T(gv["Kn"], True), T(gv["Tv"], True)
+    r = cm.run(Kg, Tg, cell=torch.as_tensor(gv["solid"], device=DEV), tol=1e-12)
+    for k in ("u", "sig", "w", "F"):
+        assert relmax(r[k].detach().cpu().numpy(), gv["run_" + k]) < 1e-8, k
+    L = (r["u"] * T(gv["Wu"])).sum() * 1e3 + (r["sig"] * T(gv["Ws"])).sum() * 1e3
+    assert abs(float(L) - float(gv["loss"])) < 1e-8 * max(1.0, abs(float(gv["loss"])))
+    L.backward()
+    assert relmax(Kg.grad.cpu().numpy(), gv["gKn"]) < 1e-7
+    assert relmax(Tg.grad.cpu().numpy(), gv["gTv"]) < 1e-7
+
+
+def test_voided_48cube_mixed_solve_vs_oracle():
+    """A 48^3 specimen with random spherical pores (20% of the volume) under KUBC k_xx and k_xy: the mixed-precision
+    solve to 1e-8 against the oracle's FP64 block-Jacobi PCG to 1e-12 on the same bond table."""
+    n = 48
+    lat = G.LatticeGeom(n, n, n, 1.0)
+    pores, _ = M.spheres(n, n, n, 0.20, 3.0, np.random.default_rng(4), rjit=0.0)
+    solid = pores == 0
+    # a solid particle whose neighbours are all pores has no bonds (a singular row): count it as a pore
+    deg = (core.solid_tables(lat, torch.as_tensor(solid[None], device=DEV))[0] >= 0).sum(1).cpu().numpy()
+    solid &= deg > 0
+    C = G.iso_C(np.ones(lat.N), 0.2)
+    Kn, Tv = G.bond_params_two_end_mean(lat, G.sc_params_from_C(C, 0.5))
+    fr = TV.FineRefTV(n, 1, device=DEV, loads=["k_xx", "k_xy"], precision="mixed")
+    sd = torch.as_tensor(solid[None], device=DEV)
+    fr.op.set_mask(sd)
+    valid = fr.op.vb[0, 0].cpu().numpy()
+    Kv, Tvv = Kn * valid, Tv * valid
+    free = (fr.bc.free[None] * sd.double()[:, None])
+    up = fr.bc.up[None] * sd.double()[:, None, :, None]
+    u, info = fr.op.solve_mixed(T(Kv)[None, None], T(Tvv)[None, None], up, free, tol=1e-8)
+    assert (info.status == 0).all() and (info.relres <= 1e-8).all()
+    tab = core.solid_tables(lat, sd)[0].cpu().numpy().astype(np.int64)
+    olat = types.SimpleNamespace(N=lat.N, nbr=tab, ndir=lat.ndir, l0=lat.l0, V=lat.V)
+    for l in range(2):
+        fixed = ~(free[0, l].cpu().numpy() > 0)
+        uo, _ = O.solve_pcg(olat, Kv, Tvv, fixed, up[0, l].cpu().numpy(), tol=1e-12)
+        ug = u[0, l].cpu().numpy()
+        assert np.linalg.norm(ug - uo) / np.linalg.norm(uo) < 1e-6, l
+        assert np.abs(ug[~solid]).max() == 0.0

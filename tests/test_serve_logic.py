@@ -171,3 +171,13 @@ def test_amg_bucket_routing_and_slots():
         assert serve.bucket_bytes(key, 2, 9) > serve.bucket_bytes(key[:4], 2, 9)
     finally:
         srv.close()
+
+
+def test_reference_sample_walks_the_batch():
+    """The reference arm's bounded sample takes consecutive (specimen, load) pairs of the whole batch, wrapping."""
+    import bench
+    assert bench.reference_picks(16, 6, 0, 1) == [(0, 0)]
+    assert bench.reference_picks(16, 6, 7, 1) == [(1, 1)]
+    seen = {bench.reference_picks(16, 6, k, 1)[0] for k in range(96)}
+    assert len(seen) == 96
+    assert bench.reference_picks(2, 3, 2, 2) == [(1, 1), (1, 2)]
