@@ -166,6 +166,18 @@ int lpm_cg_batched_f32(const lpm_lattice* lat, const float* Kn, const float* Tv,
  * three team barriers per iteration, each wait bounded in time (LPM_ERR_TIMEOUT on expiry). */
 int lpm_cg_persistent_fits(const lpm_lattice* lat, const lpm_batch* batch);
 
+/* Bound of one team-barrier wait of the persistent engine, in ns (process-wide, default 2e9); returns the previous
+ * bound.  A wait that exceeds it records LPM_ERR_TIMEOUT, the kernel's blocks return and the solve reports that code.
+ * 0 makes every wait that does not find its barrier passed at once expire: the way a test exercises the expiry path
+ * without hanging or faulting a GPU.  No counterpart in the reference (it has no device-side waits). */
+uint64_t lpm_set_wait_limit_ns(uint64_t ns);
+
+/* Bound of the TMA-fed operators' data waits, in mbarrier polls (process-wide, default 4194304); returns the previous
+ * bound.  An expired wait makes the kernel record the error, let the copies it issued land (with the default bound)
+ * and stop computing; the CG engines then return LPM_ERR_TIMEOUT.  0 makes every data wait expire at once: the way a
+ * test exercises the abort path without hanging or faulting a GPU.  No counterpart in the reference. */
+uint32_t lpm_set_tma_wait_polls(uint32_t polls);
+
 /* ------------------------------------------------------------------------------------- assembled matrices */
 /* Workspace bytes of lpm_csr_pcg_f64 for an n x n matrix. */
 int64_t lpm_csr_workspace_bytes(int64_t n);

@@ -48,6 +48,8 @@ _SIGS = {
     "lpm_abi_version": ([], ctypes.c_int),
     "lpm_status_string": ([ctypes.c_int], ctypes.c_char_p),
     "lpm_graph_stats": ([_P(_c_i64), _P(_c_i64), _P(_c_i64)], None),
+    "lpm_set_wait_limit_ns": ([ctypes.c_uint64], ctypes.c_uint64),
+    "lpm_set_tma_wait_polls": ([ctypes.c_uint32], ctypes.c_uint32),
     "lpm_pack_coef_f32": ([_c_p, _c_p, _c_i64, _c_i32, _c_i32, _c_p], ctypes.c_int),
     "lpm_pack_coef_f64": ([_c_p, _c_p, _c_i64, _c_i32, _c_i32, _c_p], ctypes.c_int),
     "lpm_kmv_scratch_bytes": ([_P(Lattice), _c_i32, _c_i32], _c_i64),

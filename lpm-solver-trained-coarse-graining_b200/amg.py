@@ -196,14 +196,19 @@ class AmgBatch:
                                          L.ptr(st), L.stream_ptr(dev)), "lpm_amg_pcg_f32")
         return x, core.SolveInfo(it.cpu().numpy(), rel.cpu().numpy(), st.cpu().numpy())
 
-    def ir(self, Kn64, Tv64, b, tol=1e-8, inner_tol=1e-3, maxit=20000, max_outer=20, check=1, poll=10, prof=None):
+    def ir(self, Kn64, Tv64, b, tol=1e-8, inner_tol=1e-3, maxit=20000, max_outer=20, check=1, poll=10, prof=None,
+           packed=False):
         """Mixed-precision solve with the AMG-PCG inner solver: Kn64/Tv64 FP64 coefficient sets (nset, N, 18) in the
-        reference layout, b (nsys, N, 3) FP64 zero on fixed DOFs.  Returns (x, SolveInfo)."""
+        reference layout (packed=True: already packed to (nset, 18, N) by core.pack), b (nsys, N, 3) FP64 zero on
+        fixed DOFs.  Returns (x, SolveInfo)."""
         dl = self.dl
         bf = b.reshape(self.nsys, dl.N, 3).to(torch.float64).contiguous()
         # FP64 residuals on the TMA operator: packed (nset, 18, N) coefficients
-        Kc = core.pack(Kn64.reshape(-1, dl.N, dl.NN), torch.float64)
-        Tc = core.pack(Tv64.reshape(-1, dl.N, dl.NN), torch.float64)
+        if packed:
+            Kc, Tc = Kn64.contiguous(), Tv64.contiguous()
+        else:
+            Kc = core.pack(Kn64.reshape(-1, dl.N, dl.NN), torch.float64)
+            Tc = core.pack(Tv64.reshape(-1, dl.N, dl.NN), torch.float64)
         xf = torch.zeros_like(bf)
         lib = L.load()
         b_ = core._batch(self.nsys, self.rps, self.nmask)

@@ -158,6 +158,10 @@ extern "C" {
 
 int lpm_abi_version(void) { return LPM_ABI_VERSION; }
 
+uint64_t lpm_set_wait_limit_ns(uint64_t ns) { return (uint64_t)persist_wait_limit((unsigned long long)ns); }
+
+uint32_t lpm_set_tma_wait_polls(uint32_t polls) { return tma_set_wait_polls(polls); }
+
 void lpm_graph_stats(int64_t* captures, int64_t* entries, int64_t* flushes)
 {
     long long c = 0, e = 0, f = 0;

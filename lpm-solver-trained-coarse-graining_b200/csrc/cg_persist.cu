@@ -25,6 +25,7 @@
 // time (blocks of ordinary kernels only delay a launch).  Every barrier wait is bounded in time: on expiry a block
 // records LPM_ERR_TIMEOUT and returns, and the blocks waiting on it see the code and return too.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <map>
 #include <mutex>
@@ -42,7 +43,8 @@ using namespace stencil;
 
 constexpr int PB = 256;        // threads per block
 constexpr int MAXST = 16;      // systems per team
-constexpr unsigned long long WAIT_NS = 2000000000ull;  // bound of one barrier wait (2 s)
+constexpr unsigned long long WAIT_NS = 2000000000ull;  // default bound of one barrier wait (2 s)
+std::atomic<unsigned long long> g_wait_ns{WAIT_NS};     // current bound (lpm_set_wait_limit_ns)
 
 template <typename T>
 struct PersistArgs {
@@ -59,6 +61,7 @@ struct PersistArgs {
     double* part;   // (4, nsys, B): p'.Ap, r.z, r.r, b.b per block
     unsigned* bar;  // (nteam) arrival counters, zero at launch
     int* err;
+    unsigned long long wait_ns;  // bound of one team-barrier wait
     int* iters;
     double* relres;
     int* status;
@@ -83,7 +86,8 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p)
 
 // Team barrier number `n` (1, 2, ...): every block adds one arrival; the barrier is passed when the counter reaches
 // n * B.  Returns false when the wait expired or another block of the grid reported an error.
-__device__ __forceinline__ bool team_sync(unsigned* ctr, unsigned n, int B, int* err, int* s_abort)
+__device__ __forceinline__ bool team_sync(unsigned* ctr, unsigned n, int B, int* err, int* s_abort,
+                                          unsigned long long wait_ns)
 {
     __syncthreads();
     if (B > 1 && threadIdx.x == 0) {
@@ -97,7 +101,7 @@ __device__ __forceinline__ bool team_sync(unsigned* ctr, unsigned n, int B, int*
                 *s_abort = 1;
                 break;
             }
-            if (global_ns() - t0 > WAIT_NS) {
+            if (global_ns() - t0 >= wait_ns) {  // wait_ns = 0: expire unless the barrier is passed at once
                 atomicCAS(err, 0, LPM_ERR_TIMEOUT);
                 *s_abort = 1;
                 break;
@@ -227,7 +231,7 @@ __global__ void __launch_bounds__(PB) k_cg_persist(NB nb, PersistArgs<T> a)
         put_partial(v[1], 1, s);
         put_partial(v[2], 2, s);
     }
-    if (!team_sync(ctr, ++nbar, a.B, a.err, &s_abort)) return;
+    if (!team_sync(ctr, ++nbar, a.B, a.err, &s_abort, a.wait_ns)) return;
     team_totals(a.part, 3, nsys, a.B, team, a.nteam, nst, nullptr, s_t[0]);
     team_totals(a.part, 1, nsys, a.B, team, a.nteam, nst, nullptr, s_t[1]);
     team_totals(a.part, 2, nsys, a.B, team, a.nteam, nst, nullptr, s_t[2]);
@@ -327,7 +331,7 @@ __global__ void __launch_bounds__(PB) k_cg_persist(NB nb, PersistArgs<T> a)
                     for (int c = 0; c < 4; ++c) o[c] = o4[c];
                 }
             }
-            if (!team_sync(ctr, ++nbar, a.B, a.err, &s_abort)) return;
+            if (!team_sync(ctr, ++nbar, a.B, a.err, &s_abort, a.wait_ns)) return;
 
             // ------------------------------------------------------------------------------------- B: Ap, p'.Ap
             for (int js = 0; js < nst; ++js) {
@@ -364,7 +368,7 @@ __global__ void __launch_bounds__(PB) k_cg_persist(NB nb, PersistArgs<T> a)
                 put_partial(dot, 0, s);
             }
         }
-        if (!team_sync(ctr, ++nbar, a.B, a.err, &s_abort)) return;
+        if (!team_sync(ctr, ++nbar, a.B, a.err, &s_abort, a.wait_ns)) return;
         team_totals(a.part, 0, nsys, a.B, team, a.nteam, nst, s_act, s_t[0]);
         __syncthreads();
         if (threadIdx.x < nst && s_act[threadIdx.x]) {
@@ -412,7 +416,7 @@ __global__ void __launch_bounds__(PB) k_cg_persist(NB nb, PersistArgs<T> a)
             put_partial(v[0], 1, s);
             put_partial(v[1], 2, s);
         }
-        if (!team_sync(ctr, ++nbar, a.B, a.err, &s_abort)) return;
+        if (!team_sync(ctr, ++nbar, a.B, a.err, &s_abort, a.wait_ns)) return;
         team_totals(a.part, 1, nsys, a.B, team, a.nteam, nst, s_act, s_t[1]);
         team_totals(a.part, 2, nsys, a.B, team, a.nteam, nst, s_act, s_t[2]);
         __syncthreads();
@@ -598,6 +602,7 @@ int run_persist(NB nb, const Lattice& L, const T* Kn, const T* Tv, const CoefLay
     a.maxit = o.maxit;
     a.precheck = o.precheck;
     a.tol = o.tol;
+    a.wait_ns = g_wait_ns.load();
     cudaError_t e = cudaMemsetAsync(a.bar, 0, sizeof(unsigned) * bt.nsys, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(a.err, 0, sizeof(int), st);
     if (e != cudaSuccess) return (int)e;
@@ -681,6 +686,8 @@ int cg_solve_persist(const Lattice& L, const T* Kn, const T* Tv, const CoefLayou
     return dispatch_prec<T, 2>(GridNb<2>{L.nx, L.ny, 1}, L, Kn, Tv, cl, bt, Minv, mask, b, x, x_is_zero, o, ws,
                                ws_bytes, iters, relres, status, st);
 }
+
+unsigned long long persist_wait_limit(unsigned long long ns) { return g_wait_ns.exchange(ns); }
 
 template int cg_solve_persist<float>(const Lattice&, const float*, const float*, const CoefLayout&, const Batch&,
                                      const float*, const uint8_t*, const float*, float*, int, const lpm_cg_opts&,

@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
     // z+1 before a slow warp has read it after step z's barrier, and the two would then wait at different barriers.
     bool lost = false;
     auto wait_fill = [&](int b, int parity) {
-        if (!mbar_wait(&bars[b], (uint32_t)parity)) {
+        if (!mbar_wait(&bars[b], (uint32_t)parity, P.wait_polls)) {
             lost = true;
             if (P.err) atomicExch(P.err, 1);
         } else if (producer) {
@@ -688,6 +688,7 @@ cudaError_t launch_pair(const PairArgs& a, cudaStream_t st)
     for (int g0 = 0; g0 < a.npair; g0 += 65535) {
         PairArgs b = a;
         b.pair0 = g0;
+        b.wait_polls = tma_wait_polls();
         const int ng = a.npair - g0 < 65535 ? a.npair - g0 : 65535;
         k_sc_pair<MODE, LEAN><<<dim3(ntile * nzc, ng), pair_threads(LEAN), pair_bytes(LEAN), st>>>(mu, mtv, mkn, b);
     }

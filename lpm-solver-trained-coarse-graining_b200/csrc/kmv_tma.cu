@@ -23,6 +23,8 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <atomic>
+
 #include <mutex>
 #include <type_traits>
 
@@ -205,9 +207,10 @@ __global__ void __launch_bounds__(TX* TY, 1)
         auto ok_kn = [&](int p) { return p >= 0 && p < nz && p >= kn0 && p < zend; };
         bool good = true;
         if (tid == 0) {
-            if (ok_u(pu)) good = good && mbar_wait(&bars[(pu - u0) & 3], ((pu - u0) >> 2) & 1);
-            if (ok_tv(ptv)) good = good && mbar_wait(&bars[4 + ((ptv - tv0) & 1)], ((ptv - tv0) >> 1) & 1);
-            if (ok_kn(pkn)) good = good && mbar_wait(&bars[6 + ((pkn - kn0) & 1)], ((pkn - kn0) >> 1) & 1);
+            const unsigned lim = P.wait_polls;
+            if (ok_u(pu)) good = good && mbar_wait(&bars[(pu - u0) & 3], ((pu - u0) >> 2) & 1, lim);
+            if (ok_tv(ptv)) good = good && mbar_wait(&bars[4 + ((ptv - tv0) & 1)], ((ptv - tv0) >> 1) & 1, lim);
+            if (ok_kn(pkn)) good = good && mbar_wait(&bars[6 + ((pkn - kn0) & 1)], ((pkn - kn0) >> 1) & 1, lim);
             if (!good && P.err) atomicExch(P.err, 1);
         }
         if (__syncthreads_or(!good)) return false;
@@ -583,6 +586,7 @@ cudaError_t launch_one(const TmaArgs<T>& a, int ngt, int nzc, cudaStream_t st)
     const int ntile = ((a.nx + TX - 1) / TX) * ((a.ny + TY - 1) / TY);
     for (int g0 = 0; g0 < ngt; g0 += 65535) {
         TmaArgs<T> b = a;
+        b.wait_polls = tma_wait_polls();
         b.grp0 = g0;
         const int ng = ngt - g0 < 65535 ? ngt - g0 : 65535;
         k_sc_tma<T, NR, TY, EPI><<<dim3(ntile * nzc, ng), dim3(TX, TY), Lay::BYTES, st>>>(mu, mtv, mkn, b);
@@ -623,6 +627,13 @@ bool tma_aligned(const void* a, const void* b, const void* c)
 {
     return ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b) | reinterpret_cast<uintptr_t>(c)) & 15u) == 0;
 }
+
+namespace {
+std::atomic<unsigned> g_wait_polls{ptx::kWaitLimit};
+}  // namespace
+
+unsigned tma_wait_polls() { return g_wait_polls.load(std::memory_order_relaxed); }
+unsigned tma_set_wait_polls(unsigned polls) { return g_wait_polls.exchange(polls); }
 
 bool tma_supported(int nx, int elem_bytes)
 {

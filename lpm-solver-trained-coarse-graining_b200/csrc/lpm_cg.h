@@ -97,6 +97,8 @@ int cg_solve(const Lattice& L, const T* Kn, const T* Tv, const CoefLayout& cl, c
 
 // Persistent engine (cg_persist.cu): one cooperative launch per solve.  persist_fits: the batch has a team shape on
 // this device; persist_auto: LPM_ENGINE_AUTO picks it (small batches).  cg_solve routes to it by opts.engine.
+// Sets the bound of one team-barrier wait of the persistent engine (ns, process-wide); returns the previous bound.
+unsigned long long persist_wait_limit(unsigned long long ns);
 bool persist_fits(const Lattice& L, const Batch& bt);
 bool persist_auto(const Lattice& L, const Batch& bt);
 size_t persist_workspace_bytes(const Lattice& L, const Batch& bt, int elem_bytes);

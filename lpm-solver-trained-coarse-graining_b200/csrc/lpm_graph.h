@@ -15,8 +15,14 @@ namespace lpm {
 struct GraphKey {
     std::array<const void*, 10> ptr{};
     std::array<long long, 16> val{};
-    bool operator<(const GraphKey& o) const { return ptr != o.ptr ? ptr < o.ptr : val < o.val; }
+    long long waits = 0;  // the wait bounds baked into the captured launches (filled in by run_iteration_block)
+    bool operator<(const GraphKey& o) const
+    {
+        return ptr != o.ptr ? ptr < o.ptr : (val != o.val ? val < o.val : waits < o.waits);
+    }
 };
+
+unsigned tma_wait_polls();  // current poll bound of the TMA operators' data waits (kmv_tma.cu)
 
 cudaGraphExec_t graph_find(const GraphKey& k);
 void graph_put(const GraphKey& k, cudaGraphExec_t e);
@@ -36,7 +42,10 @@ cudaError_t run_iteration_block(bool use_graph, const GraphKey& key, int it, int
         }
         return cudaSuccess;
     }
-    cudaGraphExec_t ge = graph_find(key);
+    // a captured launch keeps the wait bound it was captured with: graphs of different bounds are different graphs
+    GraphKey k = key;
+    k.waits = (long long)tma_wait_polls();
+    cudaGraphExec_t ge = graph_find(k);
     if (!ge) {
         cudaStream_t cs = graph_capture_stream();
         if (!cs) return cudaErrorNotReady;
@@ -53,7 +62,7 @@ cudaError_t run_iteration_block(bool use_graph, const GraphKey& key, int it, int
         e = cudaGraphInstantiate(&ge, g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return e;
-        graph_put(key, ge);
+        graph_put(k, ge);
     }
     return cudaGraphLaunch(ge, st);
 }

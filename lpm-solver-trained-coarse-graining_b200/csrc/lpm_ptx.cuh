@@ -38,10 +38,10 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity)
     return ok != 0;
 }
 
-// Bounded wait for the phase of `bar` with the given parity; false on expiry.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+// Bounded wait for the phase of `bar` with the given parity (at most `limit` polls); false on expiry.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned limit = kWaitLimit)
 {
-    for (unsigned n = 0; n < kWaitLimit; ++n)
+    for (unsigned n = 0; n < limit; ++n)
         if (mbar_test(bar, parity)) return true;
     return false;
 }

@@ -27,10 +27,17 @@ struct TmaArgs {
     int has_sc;
     int it;
     int* err;             // set to 1 if an mbarrier wait expired
+    unsigned wait_polls;  // poll bound of the data waits (set by the launcher from tma_wait_polls())
 };
 
 // Tiled 4D tensor map over FP32 (elem_bytes 4) or FP64 data, no swizzle, zero fill out of bounds; false when the
 // driver entry point is missing or the encoding is rejected.
+// Poll bound of the TMA operators' data waits (process-wide; default ptx::kWaitLimit).  Setting it returns the
+// previous bound; 0 makes every data wait expire at once, so the kernels take their abort path (record the error,
+// let the copies they issued land with the full bound, stop computing).
+unsigned tma_wait_polls();
+unsigned tma_set_wait_polls(unsigned polls);
+
 bool make_tensor_map4(CUtensorMap* m, int elem_bytes, const void* base, const uint64_t dims[4],
                       const uint64_t strides_bytes[3], const uint32_t box[4]);
 bool tma_supported(int nx, int elem_bytes);
@@ -65,6 +72,7 @@ struct PairArgs {
     int has_sc;
     int it;
     int* err;
+    unsigned wait_polls;  // poll bound of the data waits (set by the launcher from tma_wait_polls())
     // AMG smoother epilogues (PM_RESID, PM_SMOOTH, PM_SMOOTH_DOT)
     const float* rhs;  // pair layout: the right-hand side of the smoothing step
     const float* Ms;   // (nset, 9, N) block-Jacobi inverse

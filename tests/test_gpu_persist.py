@@ -150,3 +150,25 @@ def test_persistent_masked_lattice():
     assert (ia.status == 0).all() and (ip.status == 0).all()
     assert close_iters(ia, ip)
     assert relmax(xp, xa) < 1e-8
+
+
+def test_team_barrier_expiry_reports_timeout_and_leaves_the_gpu_usable():
+    """With the wait bound at 0 every team-barrier wait that does not find its barrier passed at once expires: the
+    solve returns LPM_ERR_TIMEOUT (the kernel's blocks record the code and return; nothing hangs or faults), and the
+    next solve with the default bound on the same GPU gives the launched engine's answer."""
+    lat, Kn, Tv, fixed, up = grf2d(128, [0])
+    dl = core.DeviceLattice(lat)
+    free = T(~fixed)
+    b = -core.kmv(dl, T(up), T(Kn), T(Tv)) * free
+    lib = L.load()
+    prev = lib.lpm_set_wait_limit_ns(0)
+    try:
+        with pytest.raises(L.LPMError, match=r"code -5"):
+            core.cg(dl, T(Kn), T(Tv), b, free=free, tol=1e-10, maxit=20000, check=1, engine=PE)
+    finally:
+        assert lib.lpm_set_wait_limit_ns(prev) == 0
+    assert prev == 2000000000
+    torch.cuda.synchronize()
+    xa, ia, xp, ip = both(dl, T(Kn), T(Tv), b, free=free, tol=1e-10, maxit=20000, check=1)
+    assert (ip.status == 0).all() and close_iters(ia, ip)
+    assert relmax(xp, xa) < 1e-8
