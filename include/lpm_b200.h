@@ -326,6 +326,22 @@ int lpm_autotune_kmv(const lpm_lattice* lat, const lpm_batch* batch, const float
  * (1..nz, at most nz/8 chunks) and variant (0 or 1, as above).  No reference counterpart. */
 int lpm_tune_kmv_set(const lpm_lattice* lat, const lpm_batch* batch, int32_t zchunk, int32_t variant);
 
+/* --------------------------------------------------------------------------------------- parameter assembly */
+/* Symmetric scatter of per-bond values to a (nspec, n, 18) parameter array (coarse3d/train3d.py:77-97, Scatter):
+ * out[b, p_j, k_j] = out[b, q_j, k_j ^ 1] = vals[b, j] for the nb bonds of one group (q_j = -1: no second end).
+ * out must hold the values of earlier groups (or zeros); later writes win, as index_put does. */
+int lpm_bond_scatter_f64(int32_t nspec, int64_t n, int64_t nb, const int32_t* p, const int32_t* k, const int32_t* q,
+                         const double* vals, double* out, void* stream);
+/* Its adjoint: g[b, j] = G[b, p_j, k_j] + G[b, q_j, k_j ^ 1] (the autograd pass of Scatter for bonds written once). */
+int lpm_bond_gather_sym_f64(int32_t nspec, int64_t n, int64_t nb, const int32_t* p, const int32_t* k,
+                            const int32_t* q, const double* G, double* g, void* stream);
+/* Smallest eigenvalue lam (nspec, n) and its unit eigenvector vec (nspec, n, 6 or 12) of every (particle, shell) group
+ * bond Hessian of the stability penalty (coarse3d/train3d.py:119-137, group_penalty): H = diag(kn) + (tv 1^T +
+ * 1 tv^T)/2 on the shell's in-box slots and 1e3 sc[b] on the diagonal of the others; Kn, Tv (nspec, n, 18) FP64 in the
+ * reference layout, full SC boxes only. */
+int lpm_group_eigmin_sc(const lpm_lattice* lat, int32_t nspec, const double* Kn, const double* Tv, const double* sc,
+                        int32_t shell, double* lam, double* vec, void* stream);
+
 /* ------------------------------------------------------------------------------------------------ geometry */
 /* Neighbour table of a (possibly masked) box, identical to LatticeGeom.nbr / Lattice2D.nbr
  * (coarse3d/geom3d.py:38-65, coarse2d/lin2d.py:32-74): site_of (nx*ny*nz) int64 = particle id or -1,

@@ -79,6 +79,9 @@ _SIGS = {
     "lpm_stress_f64": ([_P(Lattice), _c_p, _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_d, _c_p, _c_p, _c_sz, _c_p],
                        ctypes.c_int),
     "lpm_energy_f64": ([_P(Lattice), _c_p, _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p], ctypes.c_int),
+    "lpm_bond_scatter_f64": ([_c_i32, _c_i64, _c_i64, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
+    "lpm_bond_gather_sym_f64": ([_c_i32, _c_i64, _c_i64, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
+    "lpm_group_eigmin_sc": ([_P(Lattice), _c_i32, _c_p, _c_p, _c_p, _c_i32, _c_p, _c_p, _c_p], ctypes.c_int),
     "lpm_solid_nbr": ([_c_i32, _c_i32, _c_i32, _c_i32, _c_i32, _c_p, _c_p, _c_p], ctypes.c_int),
     "lpm_build_nbr": ([_c_i32, _c_i32, _c_i32, _c_i32, _c_i64, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
     "lpm_energy_vjp_f64": ([_P(Lattice), _c_p, _c_p, _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p, _c_p, _c_i32, _c_p,

@@ -1,0 +1,172 @@
+// Bond-parameter assembly upstream of the 3D solve (coarse3d/train3d.py):
+//
+//  * the symmetric scatter of per-group bond values to the (B, N, 18) parameter arrays (train3d.Scatter,
+//    train3d.py:77-97): value j of a group goes to slot k_j of particle p_j and to slot k_j ^ 1 of its neighbour q_j,
+//    and its adjoint, which sums the two slots of every bond;
+//  * the smallest eigenpair of every (particle, shell) group bond Hessian of the stability penalty
+//    (train3d.group_penalty, train3d.py:119-137):
+//        H = diag(kn) + (tv 1^T + 1 tv^T) / 2 on the valid slots of the shell, and 1e3 sc on the diagonal of the
+//        missing ones (sc = the sample's mean |Kn|),
+//    by cyclic Jacobi rotations on the 6 x 6 (shell 0) or 12 x 12 (shell 1) matrix held by one thread; the eigenvector
+//    gives the derivative of the eigenvalue (dlam/dH = v v^T for a simple eigenvalue).
+#include <cstdint>
+
+#include "../../include/lpm_b200.h"
+#include "lpm_kernels.h"
+
+namespace lpm {
+
+namespace {
+
+__global__ void k_bond_scatter(int64_t n, int64_t nb, const int32_t* __restrict__ p, const int32_t* __restrict__ k,
+                               const int32_t* __restrict__ q, const double* __restrict__ vals, double* __restrict__ out)
+{
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nb) return;
+    const int64_t b = blockIdx.y;
+    const double v = vals[b * nb + j];
+    double* o = out + b * n * 18;
+    o[(int64_t)p[j] * 18 + k[j]] = v;
+    if (q[j] >= 0) o[(int64_t)q[j] * 18 + (k[j] ^ 1)] = v;
+}
+
+__global__ void k_bond_gather_sym(int64_t n, int64_t nb, const int32_t* __restrict__ p, const int32_t* __restrict__ k,
+                                  const int32_t* __restrict__ q, const double* __restrict__ G, double* __restrict__ g)
+{
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nb) return;
+    const int64_t b = blockIdx.y;
+    const double* Gb = G + b * n * 18;
+    double v = Gb[(int64_t)p[j] * 18 + k[j]];
+    if (q[j] >= 0) v += Gb[(int64_t)q[j] * 18 + (k[j] ^ 1)];
+    g[b * nb + j] = v;
+}
+
+// Smallest eigenpair of the symmetric M x M matrix A (row-major, overwritten) by cyclic Jacobi; V receives the
+// eigenvectors as columns.
+template <int M>
+__device__ void jacobi_min(double (&A)[M][M], double (&V)[M][M], double& lam, double (&v)[M])
+{
+    for (int a = 0; a < M; ++a)
+        for (int b = 0; b < M; ++b) V[a][b] = a == b ? 1.0 : 0.0;
+    double scale = 0.0;
+    for (int a = 0; a < M; ++a)
+        for (int b = 0; b < M; ++b) scale += A[a][b] * A[a][b];
+    for (int sweep = 0; sweep < 40; ++sweep) {
+        double off = 0.0;
+        for (int a = 0; a < M; ++a)
+            for (int b = a + 1; b < M; ++b) off += A[a][b] * A[a][b];
+        if (off <= 1e-32 * scale) break;
+        for (int p = 0; p < M - 1; ++p) {
+            for (int r = p + 1; r < M; ++r) {
+                const double apr = A[p][r];
+                if (apr == 0.0) continue;
+                // rotation that zeroes A[p][r] (stable tangent form)
+                const double theta = (A[r][r] - A[p][p]) / (2.0 * apr);
+                const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+                for (int m = 0; m < M; ++m) {  // columns p, r
+                    const double amp = A[m][p], amr = A[m][r];
+                    A[m][p] = c * amp - s * amr;
+                    A[m][r] = s * amp + c * amr;
+                }
+                for (int m = 0; m < M; ++m) {  // rows p, r
+                    const double apm = A[p][m], arm = A[r][m];
+                    A[p][m] = c * apm - s * arm;
+                    A[r][m] = s * apm + c * arm;
+                }
+                for (int m = 0; m < M; ++m) {
+                    const double vmp = V[m][p], vmr = V[m][r];
+                    V[m][p] = c * vmp - s * vmr;
+                    V[m][r] = s * vmp + c * vmr;
+                }
+            }
+        }
+    }
+    int im = 0;
+    for (int a = 1; a < M; ++a)
+        if (A[a][a] < A[im][im]) im = a;
+    lam = A[im][im];
+    for (int a = 0; a < M; ++a) v[a] = V[a][im];
+}
+
+// One thread per (sample, particle): the group of `shell` (slots 0..5 or 6..17).  valid: implicit full box.
+template <int M>
+__global__ void __launch_bounds__(64) k_group_eig(int nx, int ny, int nz, int nspec, const double* __restrict__ Kn,
+                                                  const double* __restrict__ Tv, const double* __restrict__ sc,
+                                                  double* __restrict__ lam_out, double* __restrict__ vec_out)
+{
+    const int64_t N = (int64_t)nx * ny * nz;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N * nspec) return;
+    const int64_t b = t / N, i = t % N;
+    const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((int64_t)nx * ny));
+    const int k0 = M == 6 ? 0 : 6;
+    double kn[M], tv[M];
+    bool vv[M];
+    for (int a = 0; a < M; ++a) {
+        const int k = k0 + a;
+        const int qx = x + sc_dx(k), qy = y + sc_dy(k), qz = z + sc_dz(k);
+        vv[a] = qx >= 0 && qx < nx && qy >= 0 && qy < ny && qz >= 0 && qz < nz;
+        kn[a] = vv[a] ? Kn[(b * N + i) * 18 + k] : 0.0;
+        tv[a] = vv[a] ? Tv[(b * N + i) * 18 + k] : 0.0;
+    }
+    const double big = 1e3 * sc[b];
+    double A[M][M], V[M][M], v[M], lam;
+    for (int a = 0; a < M; ++a)
+        for (int c = 0; c < M; ++c) {
+            double h = (vv[a] && vv[c]) ? 0.5 * (tv[a] + tv[c]) : 0.0;
+            if (a == c) h += vv[a] ? kn[a] : big;
+            A[a][c] = h;
+        }
+    jacobi_min<M>(A, V, lam, v);
+    lam_out[t] = lam;
+    for (int a = 0; a < M; ++a) vec_out[t * M + a] = v[a];
+}
+
+}  // namespace
+
+}  // namespace lpm
+
+using namespace lpm;
+
+int lpm_bond_scatter_f64(int32_t nspec, int64_t n, int64_t nb, const int32_t* p, const int32_t* k, const int32_t* q,
+                         const double* vals, double* out, void* stream)
+{
+    if (nspec < 1 || nspec > 65535 || n < 1 || nb < 0 || (nb > 0 && (!p || !k || !q || !vals)) || !out)
+        return LPM_ERR_ARG;
+    if (nb == 0) return LPM_OK;
+    k_bond_scatter<<<dim3((unsigned)((nb + 255) / 256), nspec), 256, 0, (cudaStream_t)stream>>>(n, nb, p, k, q, vals,
+                                                                                                  out);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? LPM_OK : (int)e;
+}
+
+int lpm_bond_gather_sym_f64(int32_t nspec, int64_t n, int64_t nb, const int32_t* p, const int32_t* k,
+                            const int32_t* q, const double* G, double* g, void* stream)
+{
+    if (nspec < 1 || nspec > 65535 || n < 1 || nb < 0 || (nb > 0 && (!p || !k || !q || !g)) || !G) return LPM_ERR_ARG;
+    if (nb == 0) return LPM_OK;
+    k_bond_gather_sym<<<dim3((unsigned)((nb + 255) / 256), nspec), 256, 0, (cudaStream_t)stream>>>(n, nb, p, k, q, G,
+                                                                                                     g);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? LPM_OK : (int)e;
+}
+
+int lpm_group_eigmin_sc(const lpm_lattice* lat, int32_t nspec, const double* Kn, const double* Tv, const double* sc,
+                        int32_t shell, double* lam, double* vec, void* stream)
+{
+    if (!lat || lat->dim != 3 || lat->nbr || nspec < 1 || !Kn || !Tv || !sc || !lam || !vec ||
+        (shell != 0 && shell != 1))
+        return LPM_ERR_ARG;
+    if ((int64_t)lat->nx * lat->ny * lat->nz != lat->n) return LPM_ERR_ARG;
+    const int64_t tot = lat->n * nspec;
+    const unsigned g = (unsigned)((tot + 63) / 64);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (shell == 0)
+        k_group_eig<6><<<g, 64, 0, st>>>(lat->nx, lat->ny, lat->nz, nspec, Kn, Tv, sc, lam, vec);
+    else
+        k_group_eig<12><<<g, 64, 0, st>>>(lat->nx, lat->ny, lat->nz, nspec, Kn, Tv, sc, lam, vec);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? LPM_OK : (int)e;
+}

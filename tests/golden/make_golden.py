@@ -17,6 +17,8 @@ Parts:
          one cycle, PCG iterations; 14^3 and the 48^3 bench specimen) and geom3d.interface_cells
   sctv   the per-specimen void operator of cement3d/torch_v1.py (SCTV, CoarseTV): apply, stress, energy and block
          diagonals under two specimens' solid masks, and a differentiable CoarseTV.run (9 loads) with its loss gradient
+  asm    parameter assembly upstream of the 3D solve (coarse3d/train3d.py): the symmetric Scatter of per-group bond
+         values to (B, N, 18) and the group_penalty stability term, with their autograd gradients
   cfg3   the differentiable 2D coarse solve of the benchmark's third configuration at nc = 32 and 48 (the sizes the
          reference's dense torch_lpm path handles): GRF fine field -> Voigt cells -> two-end-mean bonds (coarse2d/
          micro.py, coarse2d/cg.py:201-234), lognormal(0.2) factors per undirected bond rounded to FP32, loads lr_tx,
@@ -552,7 +554,54 @@ def part_sctv():
     print("golden_sctv.npz:", len(out), "arrays")
 
 
-PARTS = {"sc": part_sc, "sq": part_sq, "grad": part_grad, "amg": part_amg, "cfg3": part_cfg3, "sctv": part_sctv}
+def part_asm():
+    """coarse3d/train3d.py Scatter and group_penalty on a 5^3 coarse model (s = 2), B = 2, two bond groups (axial and
+    diagonal forward bonds, every undirected bond once), values drawn so that some group Hessians fall below the
+    penalty threshold."""
+    _env()
+    sys.path.insert(0, os.path.join(REF, "coarse3d"))
+    import numpy as np
+    import torch
+    import torch_lpm3d as T
+    import train3d as TR
+    torch.set_default_dtype(torch.float64)
+    nc, s, B = 5, 2, 2
+    cm = T.CoarseT(nc, s, device="cpu")
+    lat = cm.lat
+    groups = []
+    for slots in (range(0, 6, 2), range(6, 18, 2)):
+        bonds = [np.stack([np.nonzero(lat.valid[:, k])[0], np.full(int(lat.valid[:, k].sum()), k)], 1) for k in slots]
+        groups.append(dict(bonds=np.concatenate(bonds)))
+    sc = TR.Scatter(nc, s, groups, device="cpu")
+    rng = np.random.default_rng(41)
+    vals, leaves = [], []
+    for g in groups:
+        nb = len(g["bonds"])
+        kn = torch.tensor(rng.uniform(0.02, 1.0, (B, nb)), requires_grad=True)
+        tv = torch.tensor(rng.uniform(-0.2, 0.1, (B, nb)), requires_grad=True)
+        vals.append((kn, tv))
+        leaves += [kn, tv]
+    Kn, Tv = sc(vals)
+    Wk = rng.standard_normal(tuple(Kn.shape))
+    Wt = rng.standard_normal(tuple(Tv.shape))
+    Ls = (Kn * torch.tensor(Wk)).sum() + (Tv * torch.tensor(Wt)).sum()
+    gs = torch.autograd.grad(Ls, leaves, retain_graph=True)
+    pen, lmin = TR.group_penalty(cm, Kn, Tv, frac=0.05)
+    gp = torch.autograd.grad(pen.sum(), leaves)
+    out = dict(Kn=Kn.detach().numpy(), Tv=Tv.detach().numpy(), Wk=Wk, Wt=Wt, pen=pen.detach().numpy(),
+               lmin=float(lmin))
+    for i, g in enumerate(groups):
+        out["bonds%d" % i] = g["bonds"]
+        out["kn%d" % i] = vals[i][0].detach().numpy()
+        out["tv%d" % i] = vals[i][1].detach().numpy()
+        out["gs_kn%d" % i], out["gs_tv%d" % i] = gs[2 * i].numpy(), gs[2 * i + 1].numpy()
+        out["gp_kn%d" % i], out["gp_tv%d" % i] = gp[2 * i].numpy(), gp[2 * i + 1].numpy()
+    print("penalty", pen.detach().numpy(), "lmin", float(lmin))
+    np.savez_compressed(os.path.join(HERE, "golden_asm.npz"), **out)
+    print("golden_asm.npz:", len(out), "arrays")
+
+
+PARTS = {"asm": part_asm, "sc": part_sc, "sq": part_sq, "grad": part_grad, "amg": part_amg, "cfg3": part_cfg3, "sctv": part_sctv}
 
 if __name__ == "__main__":
     if not REF or not os.path.isdir(REF):
