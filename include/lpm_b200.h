@@ -121,12 +121,15 @@ int lpm_kmv_sq_f32(const lpm_lattice* lat, const float* u, const float* Kn, cons
 /* Size of the device array behind lpm_kmv_f64_static: 32 MiB on every GPU that loads the library, held until exit. */
 #define LPM_KMV_STATIC_SCRATCH_BYTES (32u * 1024u * 1024u)
 
-/* FP64 out = K u exactly as lpm_kmv_sc_f64 (lat->dim == 3) or lpm_kmv_sq_f64 (lat->dim == 2), but with no scratch
+/* FP64 out = K u, the same operator as lpm_kmv_sc_f64 (lat->dim == 3) or lpm_kmv_sq_f64 (lat->dim == 2) and equal to
+ * it within rounding (this entry always runs the two-pass kernels; full SC boxes in the packed layout go through the
+ * single-pass TMA operator there), but with no scratch
  * argument and no device allocation: for callers that cannot allocate device memory or pass a buffer (an FFI host
  * that only forwards device pointers it was given, a fixed memory budget, a path where a cudaMalloc would stall).
  * No counterpart in the reference.  Limit: 4 * nsys * n doubles must fit LPM_KMV_STATIC_SCRATCH_BYTES (nsys * n <=
  * 1,048,576, e.g. nine systems of a 48^3 box), else LPM_ERR_WORKSPACE.  The first call on a device looks up the
- * array's device address with that device current, so make it before any stream capture.  Every call on a device
+ * array's device address with that device current, so make it before any stream capture; the cached address does
+ * not survive a cudaDeviceReset of that device.  Every call on a device
  * shares the array: calls whose work overlaps on the GPU race and must be serialised by the caller. */
 int lpm_kmv_f64_static(const lpm_lattice* lat, const double* u, const double* Kn, const double* Tv,
                        int32_t coef_layout, const lpm_batch* batch, double* out, void* stream);

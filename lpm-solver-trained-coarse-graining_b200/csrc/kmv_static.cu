@@ -11,12 +11,15 @@
 // library holds it for the life of the process.  Host code cannot use its name as a device address (on the host the
 // name refers to a host-side shadow), so on the first call on each device, with that device current, the device
 // address is looked up with cudaGetSymbolAddress and cached; that first call should therefore come before any stream
-// capture.  All calls on a device share the one array: two calls whose work overlaps on that GPU (different streams,
+// capture.  The cached address belongs to the device context it was looked up in: after a cudaDeviceReset (which
+// ends that context) it is stale, so a process that resets a device must not call this entry point on it again.
+// All calls on a device share the one array: two calls whose work overlaps on that GPU (different streams,
 // or several host threads) race on it and must be serialised by the caller.  Pass 1 overwrites every entry that pass 2
 // later reads, so the array needs no clearing between calls.  No call allocates or frees device memory.
 #include <mutex>
 
 #include "../../include/lpm_b200.h"
+#include "lpm_abi.h"
 #include "lpm_kernels.h"
 
 namespace {
@@ -54,22 +57,17 @@ extern "C" int lpm_kmv_f64_static(const lpm_lattice* lat, const double* u, const
                                   int32_t coef_layout, const lpm_batch* batch, double* out, void* stream)
 {
     using namespace lpm;
-    if (!lat || !batch || !u || !Kn || !Tv || !out) return LPM_ERR_ARG;
-    if (lat->dim != 2 && lat->dim != 3) return LPM_ERR_ARG;
-    if (lat->nx < 1 || lat->ny < 1 || lat->nz < 1 || lat->n < 1 || (lat->dim == 2 && lat->nz != 1)) return LPM_ERR_ARG;
-    if (!lat->nbr && lat->n != (int64_t)lat->nx * lat->ny * lat->nz) return LPM_ERR_ARG;
-    if (batch->nsys < 1 || batch->rhs_per_set < 1 || batch->nmask < 1) return LPM_ERR_ARG;
-    if (coef_layout != LPM_LAYOUT_REF && coef_layout != LPM_LAYOUT_SOA) return LPM_ERR_ARG;
+    if (!u || !Kn || !Tv || !out) return LPM_ERR_ARG;
+    Lattice L;
+    Batch bt;
+    CoefLayout cl;
+    int rc = to_lattice(lat, L);
+    if (rc || (rc = to_batch(batch, bt)) || (rc = to_layout(coef_layout, L, cl))) return rc;
     // 4 shell sums per particle and system must fit the static array
-    const double need = 4.0 * (double)batch->nsys * (double)lat->n;
+    const double need = 4.0 * (double)bt.nsys * (double)L.N;
     if (need > (double)kStaticDoubles) return LPM_ERR_WORKSPACE;
     double* scratch = nullptr;
-    int rc = static_scratch(&scratch);
-    if (rc != LPM_OK) return rc;
-    Lattice L{lat->dim, lat->nx, lat->ny, lat->nz, lat->n, lat->nbr};
-    const int NN = lat->dim == 3 ? 18 : 8;
-    CoefLayout cl{lat->n * NN, coef_layout == LPM_LAYOUT_REF ? 1 : lat->n, coef_layout == LPM_LAYOUT_REF ? NN : 1};
-    Batch bt{batch->nsys, batch->rhs_per_set, batch->nmask};
+    if ((rc = static_scratch(&scratch)) != LPM_OK) return rc;
     const cudaError_t e =
         launch_kmv<double>(L, u, Kn, Tv, cl, bt, out, scratch, nullptr, static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? LPM_OK : (int)e;
