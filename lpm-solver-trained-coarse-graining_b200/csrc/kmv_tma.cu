@@ -70,9 +70,14 @@ __host__ __device__ constexpr unsigned dir_mask(int axis, int sgn)
     return m;
 }
 
+// Three extra warps (rows TY .. TY+2 of the block) take the halo-ring sites, so the tile warps carry none and the
+// block barrier after phase 1 waits for no straggling ring work.
+constexpr int RY = 3, RT = TX * RY;
+
 template <typename T, int NR, int TY>
 struct Layout {
-    static constexpr int NT = TX * TY;
+    static constexpr int NT = TX * TY;          // tile threads
+    static constexpr int NTH = TX * (TY + RY);  // all threads
     static constexpr int UH = TY + 4;
     static constexpr int SW = TX + 2, SH = TY + 2, SPL = SW * SH;
     static constexpr int NRING = SPL - NT;
@@ -88,13 +93,13 @@ struct Layout {
 };
 
 template <typename T, int NR, int TY, bool EPI>
-__global__ void __launch_bounds__(TX* TY, 1)
+__global__ void __launch_bounds__(TX*(TY + RY), 1)
     k_sc_tma(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ CUtensorMap tm_tv,
              const __grid_constant__ CUtensorMap tm_kn, TmaArgs<T> P)
 {
     using Lay = Layout<T, NR, TY>;
     using V2 = typename T2<T>::type;
-    constexpr int NT = Lay::NT, UH = Lay::UH, SW = Lay::SW, SH = Lay::SH, SPL = Lay::SPL;
+    constexpr int NT = Lay::NT, NTH = Lay::NTH, UH = Lay::UH, SW = Lay::SW, SH = Lay::SH, SPL = Lay::SPL;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t bars[8];  // u: 0..3, Tv: 4..5, Kn: 6..7
     __shared__ double red[32];
@@ -141,11 +146,11 @@ __global__ void __launch_bounds__(TX* TY, 1)
     {
         V2 zz;
         zz.x = zz.y = T(0);
-        for (int e = tid; e < 3 * NR * 2 * SPL; e += NT) sst[e] = zz;
+        for (int e = tid; e < 3 * NR * 2 * SPL; e += NTH) sst[e] = zz;
         // u slots that will stand for planes below 0 are never loaded; they must read as finite values (zero),
         // because invalid bonds are removed by multiplying with 0
         const int nneg = zc * P.zchunk - 2 < 0 ? 2 - zc * P.zchunk : 0;  // planes zbeg-2 .. -1
-        for (int e = tid; e < nneg * (int)(Lay::U_SLOT / sizeof(T)); e += NT) su[e] = T(0);
+        for (int e = tid; e < nneg * (int)(Lay::U_SLOT / sizeof(T)); e += NTH) su[e] = T(0);
     }
     __syncthreads();
     if (abort_flag) any_on = false;
@@ -237,7 +242,7 @@ __global__ void __launch_bounds__(TX* TY, 1)
         V2* dst = st_slot(zp);
         V2 zz;
         zz.x = zz.y = T(0);
-        for (int e = tid; e < NR * 2 * SPL; e += NT) dst[e] = zz;
+        for (int e = tid; e < NR * 2 * SPL; e += NTH) dst[e] = zz;
     };
 
     // shell sums (and own terms) of system j at site (qx, qy) of plane zp, given the site's Tv and validity
@@ -314,21 +319,20 @@ __global__ void __launch_bounds__(TX* TY, 1)
     };
 
     const int gx = x0 + tx, gy = y0 + ty;
-    const bool own_xy = gx < nx && gy < ny;
+    const bool own_xy = ty < TY && gx < nx && gy < ny;
     const unsigned own_mxy = xy_mask(gx, gy);
-    // halo-ring work items of this thread: item e = tid + it * NT (it < NIT) is ring site e % NRING of system
-    // e / NRING; NIT = 1 unless the ring sites of all NR systems outnumber the block's threads (FP64, two systems).
-    // With one item it is resolved once; with more, each z step resolves them again (fewer live registers).
+    // halo-ring work items of the ring threads (tid >= NT): item e = (tid - NT) + it * RT (it < NIT) is ring site
+    // e % NRING of system e / NRING; the first is resolved once, later ones in every z step (fewer live registers).
     constexpr int NITEM = Lay::NRING * NR;
-    constexpr int NIT = (NITEM + Lay::NT - 1) / Lay::NT;
+    constexpr int NIT = (NITEM + RT - 1) / RT;
     struct RingItem {
         int rj, rqx, rqy;
         bool in;
         unsigned mxy;
     };
     auto ring_item = [&](int it) {
-        const int e = tid + it * Lay::NT;
-        const bool has_item = e < NITEM;
+        const int e = (tid - NT) + it * RT;
+        const bool has_item = tid >= NT && e < NITEM;
         const int rs = has_item ? e % Lay::NRING : 0, rj = has_item ? e / Lay::NRING : 0;
         int rqx, rqy;
         if (rs < SW) {
@@ -531,7 +535,7 @@ __global__ void __launch_bounds__(TX* TY, 1)
             __syncthreads();
             if (last_flag) {
                 double acc = 0.0;
-                for (int b = tid; b < nblk; b += NT) acc += __ldcg(P.part + (int64_t)s * nblk + b);
+                for (int b = tid; b < nblk; b += NTH) acc += __ldcg(P.part + (int64_t)s * nblk + b);
                 acc = block_sum(acc, red);
                 if (tid == 0) {
                     P.cnt[s] = 0u;
@@ -589,7 +593,7 @@ cudaError_t launch_one(const TmaArgs<T>& a, int ngt, int nzc, cudaStream_t st)
         b.wait_polls = tma_wait_polls();
         b.grp0 = g0;
         const int ng = ngt - g0 < 65535 ? ngt - g0 : 65535;
-        k_sc_tma<T, NR, TY, EPI><<<dim3(ntile * nzc, ng), dim3(TX, TY), Lay::BYTES, st>>>(mu, mtv, mkn, b);
+        k_sc_tma<T, NR, TY, EPI><<<dim3(ntile * nzc, ng), dim3(TX, TY + RY), Lay::BYTES, st>>>(mu, mtv, mkn, b);
     }
     return cudaGetLastError();
 }
