@@ -94,7 +94,8 @@ typedef struct lpm_ir_opts {
 int lpm_abi_version(void);
 const char* lpm_status_string(int code);
 /* Diagnostics of the CUDA-graph cache behind the CG engines' iteration blocks: graphs captured so far, graphs held,
- * and flushes of the bounded cache (process-wide).  No counterpart in the reference (it has no CUDA graphs). */
+ * and evictions from the bounded (least-recently-used) cache, process-wide.  No counterpart in the reference (it has
+ * no CUDA graphs). */
 void lpm_graph_stats(int64_t* captures, int64_t* entries, int64_t* flushes);
 
 /* ------------------------------------------------------------------------------------------------ coefficients */

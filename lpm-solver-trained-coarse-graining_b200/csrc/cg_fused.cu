@@ -844,8 +844,16 @@ int cg_solve_fused(const Lattice& L, const T* Kn, const T* Tv, const Batch& bt, 
 
 // ----------------------------------------------------------------------------------------- graph cache
 namespace {
+// Graph cache: key -> (executable graph, last use).  Bounded; when full, the least recently used entry is destroyed
+// (a key only recurs while its buffers stay allocated, so old entries are the ones least likely to come back).
+constexpr size_t kGraphCap = 256;
+struct GraphEntry {
+    cudaGraphExec_t exec;
+    unsigned long long used;
+};
 std::mutex g_graph_mu;
-std::map<GraphKey, cudaGraphExec_t>* g_graphs = new std::map<GraphKey, cudaGraphExec_t>();  // never destroyed
+std::map<GraphKey, GraphEntry>* g_graphs = new std::map<GraphKey, GraphEntry>();  // never destroyed
+unsigned long long g_graph_clock = 0;
 long long g_graph_captures = 0, g_graph_flushes = 0;
 }  // namespace
 
@@ -861,18 +869,23 @@ cudaGraphExec_t graph_find(const GraphKey& k)
 {
     std::lock_guard<std::mutex> g(g_graph_mu);
     auto it = g_graphs->find(k);
-    return it == g_graphs->end() ? nullptr : it->second;
+    if (it == g_graphs->end()) return nullptr;
+    it->second.used = ++g_graph_clock;
+    return it->second.exec;
 }
 
 void graph_put(const GraphKey& k, cudaGraphExec_t e)
 {
     std::lock_guard<std::mutex> g(g_graph_mu);
-    if (g_graphs->size() >= 64) {  // bounded: drop everything (entries are cheap to capture again)
-        for (auto& kv : *g_graphs) cudaGraphExecDestroy(kv.second);
-        g_graphs->clear();
+    if (g_graphs->size() >= kGraphCap) {  // evict the least recently used graph
+        auto lru = g_graphs->begin();
+        for (auto it = g_graphs->begin(); it != g_graphs->end(); ++it)
+            if (it->second.used < lru->second.used) lru = it;
+        cudaGraphExecDestroy(lru->second.exec);
+        g_graphs->erase(lru);
         ++g_graph_flushes;
     }
-    (*g_graphs)[k] = e;
+    (*g_graphs)[k] = GraphEntry{e, ++g_graph_clock};
     ++g_graph_captures;
 }
 

@@ -27,7 +27,7 @@ unsigned tma_wait_polls();  // current poll bound of the TMA operators' data wai
 cudaGraphExec_t graph_find(const GraphKey& k);
 void graph_put(const GraphKey& k, cudaGraphExec_t e);
 cudaStream_t graph_capture_stream();
-// Captures so far, graphs held now and flushes of the bounded cache (process-wide counters).
+// Captures so far, graphs held now and evictions from the bounded cache (process-wide counters).
 void graph_stats(long long* captures, long long* entries, long long* flushes);
 
 // Runs `block` iterations starting at iteration `it`: replays (capturing on first use) the graph of `key` when
