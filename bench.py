@@ -775,6 +775,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--precond", default="amg", choices=sorted(PRECONDS),
                     help="inner PCG preconditioner of the 3D workloads (default: AMG)")
+    ap.add_argument("--tiles", default=None, help="pin the FP32 operator's z-chunk and variant, e.g. 48,staged "
+                    "(default: autotune)")
     ap.add_argument("--inner-tol", type=float, default=None,
                     help="inner FP32 solve tolerance (default 1e-4 with AMG, 1e-3 with block Jacobi)")
     a = ap.parse_args()
@@ -817,9 +819,15 @@ def main():
     ups = torch.as_tensor(ups_h, device=dev)[None].expand(B, -1, -1, -1).contiguous()   # (B, 6, N, 3)
     nsys = B * Lc
 
-    # tile tuning of the FP32 operator for this batch shape (the library records it for later launches)
-    tiles = core.autotune(dl, core.pack(Kn[:, 0], torch.float32), core.pack(Tv[:, 0], torch.float32), nsys, Lc,
-                          with_variant=True)
+    # tile tuning of the FP32 operator for this batch shape (the library records it for later launches); --tiles
+    # pins them instead (a profiling aid: the same kernel configuration at a smaller batch)
+    if a.tiles:
+        zc, var = a.tiles.split(",")
+        tiles = (int(zc), {"staged": 0, "lean": 1}[var])
+        core.tune_set(dl, nsys, Lc, *tiles)
+    else:
+        tiles = core.autotune(dl, core.pack(Kn[:, 0], torch.float32), core.pack(Tv[:, 0], torch.float32), nsys, Lc,
+                              with_variant=True)
 
     amgb = None
     if a.precond == "amg":

@@ -159,7 +159,7 @@ def test_team_barrier_expiry_reports_timeout_and_leaves_the_gpu_usable():
     lat, Kn, Tv, fixed, up = grf2d(128, [0])
     dl = core.DeviceLattice(lat)
     free = T(~fixed)
-    b = -core.kmv(dl, T(up), T(Kn), T(Tv)) * free
+    b = -core.kmv(dl, T(up)[None], T(Kn), T(Tv)) * free
     lib = L.load()
     prev = lib.lpm_set_wait_limit_ns(0)
     try:

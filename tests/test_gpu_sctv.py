@@ -10,6 +10,7 @@ import types
 import numpy as np
 import pytest
 import torch
+from scipy import ndimage
 
 import oracle as O
 from conftest import GOLDEN, relmax
@@ -83,10 +84,13 @@ def test_voided_48cube_mixed_solve_vs_oracle():
     n = 48
     lat = G.LatticeGeom(n, n, n, 1.0)
     pores, _ = M.spheres(n, n, n, 0.20, 3.0, np.random.default_rng(4), rjit=0.0)
-    solid = pores == 0
-    # a solid particle whose neighbours are all pores has no bonds (a singular row): count it as a pore
-    deg = (core.solid_tables(lat, torch.as_tensor(solid[None], device=DEV))[0] >= 0).sum(1).cpu().numpy()
-    solid &= deg > 0
+    # keep the solid's largest bond-connected cluster (face and edge neighbours, the 18 SC bonds): a solid pocket cut
+    # off by pores would float (rigid-body modes, K_ff singular), in the reference as here
+    st = np.ones((3, 3, 3), bool)
+    st[::2, ::2, ::2] = False
+    lab, nlab = ndimage.label((pores == 0).reshape(n, n, n), structure=st)
+    big = np.argmax(np.bincount(lab.ravel())[1:]) + 1
+    solid = (lab == big).ravel()
     C = G.iso_C(np.ones(lat.N), 0.2)
     Kn, Tv = G.bond_params_two_end_mean(lat, G.sc_params_from_C(C, 0.5))
     fr = TV.FineRefTV(n, 1, device=DEV, loads=["k_xx", "k_xy"], precision="mixed")
