@@ -90,6 +90,11 @@ __device__ void jacobi_min(double (&A)[M][M], double (&V)[M][M], double& lam, do
     for (int a = 0; a < M; ++a) v[a] = V[a][im];
 }
 
+// Grid offsets of the 18 slots (the order of coarse3d/geom3d.py:16-19), for loops over slots with a runtime index.
+__constant__ int c_off[18][3] = {{1, 0, 0},  {-1, 0, 0}, {0, 1, 0},  {0, -1, 0}, {0, 0, 1},   {0, 0, -1},
+                                 {1, 1, 0},  {-1, -1, 0}, {1, -1, 0}, {-1, 1, 0}, {1, 0, 1},  {-1, 0, -1},
+                                 {1, 0, -1}, {-1, 0, 1}, {0, 1, 1},  {0, -1, -1}, {0, 1, -1}, {0, -1, 1}};
+
 // One thread per (sample, particle): the group of `shell` (slots 0..5 or 6..17).  valid: implicit full box.
 template <int M>
 __global__ void __launch_bounds__(64) k_group_eig(int nx, int ny, int nz, int nspec, const double* __restrict__ Kn,
@@ -104,9 +109,10 @@ __global__ void __launch_bounds__(64) k_group_eig(int nx, int ny, int nz, int ns
     const int k0 = M == 6 ? 0 : 6;
     double kn[M], tv[M];
     bool vv[M];
+#pragma unroll
     for (int a = 0; a < M; ++a) {
         const int k = k0 + a;
-        const int qx = x + sc_dx(k), qy = y + sc_dy(k), qz = z + sc_dz(k);
+        const int qx = x + c_off[k][0], qy = y + c_off[k][1], qz = z + c_off[k][2];
         vv[a] = qx >= 0 && qx < nx && qy >= 0 && qy < ny && qz >= 0 && qz < nz;
         kn[a] = vv[a] ? Kn[(b * N + i) * 18 + k] : 0.0;
         tv[a] = vv[a] ? Tv[(b * N + i) * 18 + k] : 0.0;
