@@ -42,92 +42,89 @@ __global__ void k_bond_gather_sym(int64_t n, int64_t nb, const int32_t* __restri
     g[b * nb + j] = v;
 }
 
-// Smallest eigenpair of the symmetric M x M matrix A (row-major, overwritten) by cyclic Jacobi; V receives the
-// eigenvectors as columns.
+// Grid offsets of the 18 slots (the order of coarse3d/geom3d.py:16-19), for loops over slots with a runtime index.
+__constant__ int c_off[18][3] = {{1, 0, 0},  {-1, 0, 0}, {0, 1, 0},  {0, -1, 0}, {0, 0, 1},   {0, 0, -1},
+                                 {1, 1, 0},  {-1, -1, 0}, {1, -1, 0}, {-1, 1, 0}, {1, 0, 1},  {-1, 0, -1},
+                                 {1, 0, -1}, {-1, 0, 1}, {0, 1, 1},  {0, -1, -1}, {0, 1, -1}, {0, -1, 1}};
+
+constexpr int EG = 32;  // groups (threads) per block of the eigen kernel
+
+// One thread per (sample, particle): the group Hessian of `shell` (slots 0..5 or 6..17) of a full box, and its
+// smallest eigenpair by cyclic Jacobi rotations.  Each thread's matrix A and eigenvector matrix V live in shared
+// memory, element (a, c) of thread j at [(a * M + c) * EG + j], so the threads of a warp touch consecutive words.
 template <int M>
-__device__ void jacobi_min(double (&A)[M][M], double (&V)[M][M], double& lam, double (&v)[M])
+__global__ void __launch_bounds__(EG) k_group_eig(int nx, int ny, int nz, int nspec, const double* __restrict__ Kn,
+                                                  const double* __restrict__ Tv, const double* __restrict__ sc,
+                                                  double* __restrict__ lam_out, double* __restrict__ vec_out)
 {
-    for (int a = 0; a < M; ++a)
-        for (int b = 0; b < M; ++b) V[a][b] = a == b ? 1.0 : 0.0;
+    extern __shared__ double eig_smem[];
+    double* A = eig_smem + threadIdx.x;             // A(a, c) = A[(a * M + c) * EG]
+    double* V = eig_smem + M * M * EG + threadIdx.x;
+    auto at = [&](double* X, int a, int c) -> double& { return X[(a * M + c) * EG]; };
+
+    const int64_t N = (int64_t)nx * ny * nz;
+    const int64_t t = (int64_t)blockIdx.x * EG + threadIdx.x;
+    if (t >= N * nspec) return;
+    const int64_t b = t / N, i = t % N;
+    const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((int64_t)nx * ny));
+    const int k0 = M == 6 ? 0 : 6;
+    const double big = 1e3 * sc[b];
+    const double* kn = Kn + (b * N + i) * 18 + k0;
+    const double* tv = Tv + (b * N + i) * 18 + k0;
+    unsigned vmask = 0;
+    for (int a = 0; a < M; ++a) {
+        const int k = k0 + a;
+        const int qx = x + c_off[k][0], qy = y + c_off[k][1], qz = z + c_off[k][2];
+        if (qx >= 0 && qx < nx && qy >= 0 && qy < ny && qz >= 0 && qz < nz) vmask |= 1u << a;
+    }
     double scale = 0.0;
-    for (int a = 0; a < M; ++a)
-        for (int b = 0; b < M; ++b) scale += A[a][b] * A[a][b];
+    for (int a = 0; a < M; ++a) {
+        const bool va = (vmask >> a) & 1u;
+        for (int c = 0; c < M; ++c) {
+            const bool vc = (vmask >> c) & 1u;
+            double h = (va && vc) ? 0.5 * (tv[a] + tv[c]) : 0.0;
+            if (a == c) h += va ? kn[a] : big;
+            at(A, a, c) = h;
+            at(V, a, c) = a == c ? 1.0 : 0.0;
+            scale += h * h;
+        }
+    }
     for (int sweep = 0; sweep < 40; ++sweep) {
         double off = 0.0;
         for (int a = 0; a < M; ++a)
-            for (int b = a + 1; b < M; ++b) off += A[a][b] * A[a][b];
+            for (int c = a + 1; c < M; ++c) off += at(A, a, c) * at(A, a, c);
         if (off <= 1e-32 * scale) break;
         for (int p = 0; p < M - 1; ++p) {
             for (int r = p + 1; r < M; ++r) {
-                const double apr = A[p][r];
+                const double apr = at(A, p, r);
                 if (apr == 0.0) continue;
-                // rotation that zeroes A[p][r] (stable tangent form)
-                const double theta = (A[r][r] - A[p][p]) / (2.0 * apr);
-                const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-                const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+                // the rotation in the (p, r) plane that zeroes A(p, r), tangent in its stable form
+                const double theta = (at(A, r, r) - at(A, p, p)) / (2.0 * apr);
+                const double tn = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double cs = 1.0 / sqrt(tn * tn + 1.0), sn = tn * cs;
                 for (int m = 0; m < M; ++m) {  // columns p, r
-                    const double amp = A[m][p], amr = A[m][r];
-                    A[m][p] = c * amp - s * amr;
-                    A[m][r] = s * amp + c * amr;
+                    const double amp = at(A, m, p), amr = at(A, m, r);
+                    at(A, m, p) = cs * amp - sn * amr;
+                    at(A, m, r) = sn * amp + cs * amr;
                 }
                 for (int m = 0; m < M; ++m) {  // rows p, r
-                    const double apm = A[p][m], arm = A[r][m];
-                    A[p][m] = c * apm - s * arm;
-                    A[r][m] = s * apm + c * arm;
+                    const double apm = at(A, p, m), arm = at(A, r, m);
+                    at(A, p, m) = cs * apm - sn * arm;
+                    at(A, r, m) = sn * apm + cs * arm;
                 }
                 for (int m = 0; m < M; ++m) {
-                    const double vmp = V[m][p], vmr = V[m][r];
-                    V[m][p] = c * vmp - s * vmr;
-                    V[m][r] = s * vmp + c * vmr;
+                    const double vmp = at(V, m, p), vmr = at(V, m, r);
+                    at(V, m, p) = cs * vmp - sn * vmr;
+                    at(V, m, r) = sn * vmp + cs * vmr;
                 }
             }
         }
     }
     int im = 0;
     for (int a = 1; a < M; ++a)
-        if (A[a][a] < A[im][im]) im = a;
-    lam = A[im][im];
-    for (int a = 0; a < M; ++a) v[a] = V[a][im];
-}
-
-// Grid offsets of the 18 slots (the order of coarse3d/geom3d.py:16-19), for loops over slots with a runtime index.
-__constant__ int c_off[18][3] = {{1, 0, 0},  {-1, 0, 0}, {0, 1, 0},  {0, -1, 0}, {0, 0, 1},   {0, 0, -1},
-                                 {1, 1, 0},  {-1, -1, 0}, {1, -1, 0}, {-1, 1, 0}, {1, 0, 1},  {-1, 0, -1},
-                                 {1, 0, -1}, {-1, 0, 1}, {0, 1, 1},  {0, -1, -1}, {0, 1, -1}, {0, -1, 1}};
-
-// One thread per (sample, particle): the group of `shell` (slots 0..5 or 6..17).  valid: implicit full box.
-template <int M>
-__global__ void __launch_bounds__(64) k_group_eig(int nx, int ny, int nz, int nspec, const double* __restrict__ Kn,
-                                                  const double* __restrict__ Tv, const double* __restrict__ sc,
-                                                  double* __restrict__ lam_out, double* __restrict__ vec_out)
-{
-    const int64_t N = (int64_t)nx * ny * nz;
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= N * nspec) return;
-    const int64_t b = t / N, i = t % N;
-    const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((int64_t)nx * ny));
-    const int k0 = M == 6 ? 0 : 6;
-    double kn[M], tv[M];
-    bool vv[M];
-#pragma unroll
-    for (int a = 0; a < M; ++a) {
-        const int k = k0 + a;
-        const int qx = x + c_off[k][0], qy = y + c_off[k][1], qz = z + c_off[k][2];
-        vv[a] = qx >= 0 && qx < nx && qy >= 0 && qy < ny && qz >= 0 && qz < nz;
-        kn[a] = vv[a] ? Kn[(b * N + i) * 18 + k] : 0.0;
-        tv[a] = vv[a] ? Tv[(b * N + i) * 18 + k] : 0.0;
-    }
-    const double big = 1e3 * sc[b];
-    double A[M][M], V[M][M], v[M], lam;
-    for (int a = 0; a < M; ++a)
-        for (int c = 0; c < M; ++c) {
-            double h = (vv[a] && vv[c]) ? 0.5 * (tv[a] + tv[c]) : 0.0;
-            if (a == c) h += vv[a] ? kn[a] : big;
-            A[a][c] = h;
-        }
-    jacobi_min<M>(A, V, lam, v);
-    lam_out[t] = lam;
-    for (int a = 0; a < M; ++a) vec_out[t * M + a] = v[a];
+        if (at(A, a, a) < at(A, im, im)) im = a;
+    lam_out[t] = at(A, im, im);
+    for (int a = 0; a < M; ++a) vec_out[t * M + a] = at(V, a, im);
 }
 
 }  // namespace
@@ -167,12 +164,25 @@ int lpm_group_eigmin_sc(const lpm_lattice* lat, int32_t nspec, const double* Kn,
         return LPM_ERR_ARG;
     if ((int64_t)lat->nx * lat->ny * lat->nz != lat->n) return LPM_ERR_ARG;
     const int64_t tot = lat->n * nspec;
-    const unsigned g = (unsigned)((tot + 63) / 64);
+    const unsigned g = (unsigned)((tot + EG - 1) / EG);
     cudaStream_t st = (cudaStream_t)stream;
-    if (shell == 0)
-        k_group_eig<6><<<g, 64, 0, st>>>(lat->nx, lat->ny, lat->nz, nspec, Kn, Tv, sc, lam, vec);
-    else
-        k_group_eig<12><<<g, 64, 0, st>>>(lat->nx, lat->ny, lat->nz, nspec, Kn, Tv, sc, lam, vec);
+    if (shell == 0) {
+        k_group_eig<6><<<g, EG, 2 * 36 * EG * sizeof(double), st>>>(lat->nx, lat->ny, lat->nz, nspec, Kn, Tv, sc, lam,
+                                                                      vec);
+    } else {
+        constexpr int bytes = 2 * 144 * EG * sizeof(double);  // 73,728 B: above the 48 KB default, opted in once
+        static unsigned long long attr_set = 0;  // devices on which the opt-in was made
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return (int)e;
+        if (dev < 0 || dev >= 64) return LPM_ERR_UNSUPPORTED;
+        if (!((attr_set >> dev) & 1ull)) {
+            e = cudaFuncSetAttribute(k_group_eig<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            if (e != cudaSuccess) return (int)e;
+            attr_set |= 1ull << dev;
+        }
+        k_group_eig<12><<<g, EG, bytes, st>>>(lat->nx, lat->ny, lat->nz, nspec, Kn, Tv, sc, lam, vec);
+    }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? LPM_OK : (int)e;
 }

@@ -273,11 +273,6 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
     auto tv_slot = [&](int p) { return stv + (size_t)((p - tv0) % NTV) * (PTV_SLOT / 4); };
     auto kn_slot = [&](int p) { return skn + (size_t)((p - kn0) & 1) * (PKN_SLOT / 4); };
     auto ba_slot = [&](int p) { return sba + (size_t)(((p % NBAS) + NBAS) % NBAS) * (PBA_SLOT / 16); };
-    auto zero_ba = [&](int p) {
-        float4* d = ba_slot(p);
-        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int e = tid; e < 2 * PSPL; e += NTH) d[e] = z4;
-    };
 
     // ---------------------------------------------------------------------------------------------- phase 1
     // Shell sums of the site (qx, qy) (ring coordinates, 0 = x0-1 / y0-1) of plane zp for both lanes, stored as
@@ -288,13 +283,11 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
 #pragma unroll
     for (int k = 0; k < 18; ++k) tv_next[k] = 0.f;
 
-    auto site = [&](auto own_tag, auto mask_tag, int qx, int qy, int zp, unsigned vm, const float* tvs,
-                    const float* kns, int64_t kst) {
+    // pm, p0, pp: the u slots of planes zp-1, zp, zp+1; bsl: the (B, A) slot of plane zp.
+    auto site = [&](auto own_tag, auto mask_tag, int qx, int qy, const float* pm, const float* p0, const float* pp,
+                    float4* bsl, unsigned vm, const float* tvs, const float* kns, int64_t kst) {
         constexpr bool OWN = decltype(own_tag)::value;
         constexpr bool MASKED = decltype(mask_tag)::value;
-        const float* pm = u_slot(zp - 1);
-        const float* p0 = u_slot(zp);
-        const float* pp = u_slot(zp + 1);
         const int ci = (qy + 1) * PUW + 6 * (qx + 1);
         const pair_t ui[3] = {ld2(p0 + ci), ld2(p0 + ci + 2), ld2(p0 + ci + 4)};
         const pair_t cpl[3] = {add2(ui[0], ui[1]), add2(ui[0], ui[2]), add2(ui[1], ui[2])};
@@ -361,7 +354,7 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
         const pair_t h = dup(0.5f), q = dup(0.25f);
         const pair_t B0 = mul2(h, sub2(Sp0, Sm0)), A0 = mul2(h, sub2(Tp0, Tm0));
         const pair_t B1 = mul2(q, sub2(Sp1, Sm1)), A1 = mul2(q, sub2(Tp1, Tm1));
-        float4* dst = ba_slot(zp) + qy * PSW + qx;
+        float4* dst = bsl + qy * PSW + qx;
         float b0l, b0h, a0l, a0h, b1l, b1h, a1l, a1h;
         unpk(B0, b0l, b0h);
         unpk(A0, a0l, a0h);
@@ -426,16 +419,20 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
 
     using T_ = std::true_type;
     using F_ = std::false_type;
-    auto phase1 = [&](int zp, bool own) {
+    // Phase 1 of plane zp: pm, p0, pp are its u slots (planes zp-1, zp, zp+1), tvsl / knsl its Tv / Kn slots and bsl
+    // its (B, A) slot.
+    auto phase1 = [&](int zp, bool own, const float* pm, const float* p0, const float* pp, const float* tvsl,
+                      const float* knsl, float4* bsl) {
         if (zp < 0 || zp >= nz) {
-            zero_ba(zp);
+            const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int e = tid; e < 2 * PSPL; e += NTH) bsl[e] = z4;
             return;
         }
         const unsigned zm = z_mask(zp);
         const unsigned vm = own_mxy & zm;
         const bool uni = __all_sync(0xffffffffu, !own_xy || vm == FULL18);
         if (own_xy) {
-            const float* tvs = tv_slot(zp) + (ty + 1) * PTVW + tx + 4;
+            const float* tvs = tvsl + (ty + 1) * PTVW + tx + 4;
             if (own) {
                 const float* kns;
                 int64_t kst;
@@ -443,28 +440,28 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
                     kns = P.Kn + (int64_t)18 * set * P.N + ((int64_t)zp * ny + gy) * nx + gx;
                     kst = P.N;
                 } else {
-                    kns = kn_slot(zp) + ty * PKNW + tx;
+                    kns = knsl + ty * PKNW + tx;
                     kst = PY * PKNW;
                 }
                 if (uni)
-                    site(T_{}, F_{}, tx + 1, ty + 1, zp, vm, tvs, kns, kst);
+                    site(T_{}, F_{}, tx + 1, ty + 1, pm, p0, pp, bsl, vm, tvs, kns, kst);
                 else
-                    site(T_{}, T_{}, tx + 1, ty + 1, zp, vm, tvs, kns, kst);
+                    site(T_{}, T_{}, tx + 1, ty + 1, pm, p0, pp, bsl, vm, tvs, kns, kst);
             } else {
                 if (uni)
-                    site(F_{}, F_{}, tx + 1, ty + 1, zp, vm, tvs, nullptr, 0);
+                    site(F_{}, F_{}, tx + 1, ty + 1, pm, p0, pp, bsl, vm, tvs, nullptr, 0);
                 else
-                    site(F_{}, T_{}, tx + 1, ty + 1, zp, vm, tvs, nullptr, 0);
+                    site(F_{}, T_{}, tx + 1, ty + 1, pm, p0, pp, bsl, vm, tvs, nullptr, 0);
             }
         }
         const unsigned rvm = ring_mxy & zm;
         const bool runi = __all_sync(0xffffffffu, !ring_in || rvm == FULL18);
         if (ring_in) {
-            const float* tvs = tv_slot(zp) + rqy * PTVW + rqx + 3;
+            const float* tvs = tvsl + rqy * PTVW + rqx + 3;
             if (runi)
-                site(F_{}, F_{}, rqx, rqy, zp, rvm, tvs, nullptr, 0);
+                site(F_{}, F_{}, rqx, rqy, pm, p0, pp, bsl, rvm, tvs, nullptr, 0);
             else
-                site(F_{}, T_{}, rqx, rqy, zp, rvm, tvs, nullptr, 0);
+                site(F_{}, T_{}, rqx, rqy, pm, p0, pp, bsl, rvm, tvs, nullptr, 0);
         }
     };
 
@@ -472,12 +469,10 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
     pair_t own_cur[3] = {0ull, 0ull, 0ull};
     float tv_cur[18];
     pair_t dotp = 0ull;
-    auto phase2 = [&](int z) {
+    // Phase 2 of plane z: bm, b0, bp are the (B, A) slots of planes z-1, z, z+1 and uz the u slot of plane z.
+    auto phase2 = [&](int z, const float4* bm, const float4* b0, const float4* bp, const float* uz) {
         if (!own_xy) return;
         const int64_t i = ((int64_t)z * ny + gy) * nx + gx;
-        const float4* bm = ba_slot(z - 1);
-        const float4* b0 = ba_slot(z);
-        const float4* bp = ba_slot(z + 1);
         const int c0 = (ty + 1) * PSW + (tx + 1);
         pair_t f[3] = {own_cur[0], own_cur[1], own_cur[2]};
         const float* tvg = P.Tv + (int64_t)18 * set * P.N + i;
@@ -497,7 +492,7 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
             o[1] = f[1];
             o[2] = f[2];
             if constexpr (EPI) {
-                const float* pu = u_slot(z) + (ty + 2) * PUW + 6 * (tx + 2);
+                const float* pu = uz + (ty + 2) * PUW + 6 * (tx + 2);
                 dotp = fma2(ld2(pu), f[0], dotp);
                 dotp = fma2(ld2(pu + 2), f[1], dotp);
                 dotp = fma2(ld2(pu + 4), f[2], dotp);
@@ -519,7 +514,7 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
                 float m9[9];
 #pragma unroll
                 for (int e = 0; e < 9; ++e) m9[e] = __ldg(ms + (int64_t)e * P.N);
-                const float* pu = u_slot(z) + (ty + 2) * PUW + 6 * (tx + 2);
+                const float* pu = uz + (ty + 2) * PUW + 6 * (tx + 2);
                 const float c0 = in0 ? w0 : 0.f, c1 = in1 ? w1 : 0.f;
 #pragma unroll
                 for (int a = 0; a < 3; ++a) {
@@ -549,7 +544,8 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
         wait_planes(zbeg - 2, -1, -1);
         wait_planes(zbeg - 1, zbeg - 1, -1);
         wait_planes(zbeg, -1, -1);
-        phase1(zbeg - 1, false);
+        phase1(zbeg - 1, false, u_slot(zbeg - 2), u_slot(zbeg - 1), u_slot(zbeg), tv_slot(zbeg - 1), nullptr,
+               ba_slot(zbeg - 1));
         ok = !__syncthreads_or(lost);
         if (ok) {
             if (producer) {
@@ -561,7 +557,8 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
                     issue_tv(zbeg + 1);
             }
             wait_planes(zbeg + 1, zbeg, zbeg);
-            phase1(zbeg, true);
+            phase1(zbeg, true, u_slot(zbeg - 1), u_slot(zbeg), u_slot(zbeg + 1), tv_slot(zbeg), kn_slot(zbeg),
+                   ba_slot(zbeg));
             ok = !__syncthreads_or(lost);
             if (LEAN && ok && producer) {
                 fence_proxy_async();
@@ -569,7 +566,23 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
             }
         }
         if (ok) {
-            for (int z = zbeg; z < zend; ++z) {
+            // Slot indices of the z loop, the same for every thread and advanced once per step instead of being
+            // recomputed by division at every use.  With s = z - zbeg: the u fill of plane p is number p - (zbeg-2),
+            // so plane z-1 sits in slot (s+1) % NUS, and the fill of plane z+2 that this step waits for is number
+            // s+4 (parity ((s+4) / NUS) & 1); the Tv fill of plane z+1 is number s+2, the Kn fill number s+1; the
+            // (B, A) of plane p sits in slot p mod NBAS.
+            auto wrapu = [](int v) { return v >= NUS ? v - NUS : v; };
+            auto wrapb = [](int v) { return v >= NBAS ? v - NBAS : v; };
+            int iu = 1 % NUS;                               // u slot of plane z-1
+            int pu2 = (4 / NUS) & 1;                        // parity of the u fill of plane z+2
+            int ib = (((zbeg - 1) % NBAS) + NBAS) % NBAS;   // (B, A) slot of plane z-1
+#pragma unroll 2
+            for (int z = zbeg, s = 0; z < zend; ++z, ++s) {
+                const int iu0 = wrapu(iu + 1), iu1 = wrapu(iu0 + 1), iu2 = wrapu(iu1 + 1);
+                const int ib0 = wrapb(ib + 1), ib1 = wrapb(ib0 + 1);
+                const int itv = NTV == 2 ? (s & 1) : 0, ptv = NTV == 2 ? (((s + 2) >> 1) & 1) : (s & 1);
+                const int ikn = (s + 1) & 1, pkn = ((s + 1) >> 1) & 1;
+                const float* uz = su + (size_t)iu0 * (PU_SLOT / 4);
 #pragma unroll
                 for (int a = 0; a < 3; ++a) own_cur[a] = own_next[a];
                 if constexpr (!LEAN) {
@@ -584,8 +597,12 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
                         if (z + 2 < zend) issue_kn(z + 2);
                     }
                 }
-                wait_planes(z + 2, z + 1, z + 1);
-                phase1(z + 1, z + 1 < zend);
+                if (z + 2 < nz) wait_fill(iu2, pu2);
+                if (z + 1 < nz) wait_fill(BTV + itv, ptv);
+                if (!LEAN && z + 1 < zend) wait_fill(BKN + ikn, pkn);
+                phase1(z + 1, z + 1 < zend, uz, su + (size_t)iu1 * (PU_SLOT / 4), su + (size_t)iu2 * (PU_SLOT / 4),
+                       stv + (size_t)itv * (PTV_SLOT / 4), skn + (size_t)ikn * (PKN_SLOT / 4),
+                       sba + (size_t)ib1 * (PBA_SLOT / 16));
                 if (__syncthreads_or(lost)) {  // uniform: every thread leaves the loop at this barrier
                     ok = false;
                     break;
@@ -594,12 +611,16 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
                     fence_proxy_async();
                     if (z + 2 <= zend) issue_tv(z + 2);
                 }
-                phase2(z);
+                phase2(z, sba + (size_t)ib * (PBA_SLOT / 16), sba + (size_t)ib0 * (PBA_SLOT / 16),
+                       sba + (size_t)ib1 * (PBA_SLOT / 16), uz);
                 // Lean: the next step's Tv fill and phase 1 reuse buffers phase 2 may still read.  Staged: the next
                 // step's fills go to the u slot of plane z - 1 and phase 1 writes the (B, A) slot of plane z + 2,
                 // neither of which this phase 2 reads, and every warp has left phase 2 of plane z - 1 before any
                 // passes this step's barrier: no second barrier.
                 if constexpr (LEAN) __syncthreads();
+                iu = iu0;
+                ib = ib0;
+                if (wrapu(iu2 + 1) == 0) pu2 ^= 1;  // the next step waits for fill s+5
             }
         }
         if (!ok && producer) {  // let the copies in flight land before the block's shared memory is released
