@@ -288,7 +288,8 @@ int lpm_amg_create(const lpm_lattice* lat, const lpm_batch* batch, const int32_t
                    const int32_t* box_of_mask, const lpm_amg_opts* opts, lpm_amg** out);
 void lpm_amg_destroy(lpm_amg* amg);
 /* Numeric setup for the batch's coefficient sets (replaces amg3d.AMG3D.__init__, timing/t3d/amg3d.py:522-570):
- * Kn32/Tv32 packed FP32 (nset, 18, n), kept by reference until the next setup; Minv32 the FP32 block-Jacobi inverse
+ * Kn32/Tv32 packed FP32 (nset, 18, n), copied into the handle (so the caller's arrays are free after the call, and
+ * graphs of the handle's solves stay valid across setups); Minv32 the FP32 block-Jacobi inverse
  * (nset, n, 3, 3) of lpm_block_jacobi_f32.  Synchronises the stream. */
 int lpm_amg_setup(lpm_amg* amg, const float* Kn32, const float* Tv32, const float* Minv32, void* stream);
 /* rho of the finest level per (set, box estimate): (nset * nb) values, nb = nbox with rho0_per_box else 1.  set_rho0

@@ -102,7 +102,6 @@ class AmgBatch:
     def setup(self, K32, T32, M32, rho0=None):
         """Numeric hierarchies: K32/T32 packed FP32 (nset, 18, N), M32 FP32 block-Jacobi inverse (nset, N, 3, 3).
         rho0 (optional, per set) replaces the finest-level estimate (amg3d.AMG3D's rho0)."""
-        self._keep = (K32, T32)                 # the handle reads them until the next setup
         st = L.stream_ptr(self.dl.device)
         L.check(L.load().lpm_amg_setup(self._h, L.ptr(K32), L.ptr(T32), L.ptr(M32.contiguous()), st),
                 "lpm_amg_setup")

@@ -1418,7 +1418,8 @@ struct lpm_amg {
     float *pw_x = nullptr, *pw_y = nullptr;
     int *it_scr = nullptr, *st_scr = nullptr;
     double* rel_scr = nullptr;
-    const float *Kn = nullptr, *Tv = nullptr;
+    const float *Kn = nullptr, *Tv = nullptr;  // the handle's own copy of the packed FP32 coefficients
+    float *Kn_own = nullptr, *Tv_own = nullptr;
     int zchunk = 1, variant = 0, zchunk_probe = 1, zchunk_pow = 1;
     int nblk_pow = 1;
     void* mem = nullptr;
@@ -1464,6 +1465,8 @@ void carve_amg(lpm_amg& h, Carver2& c)
     h.pgrp = c.take<int>((size_t)3 * h.nset);
     h.fw = c.take<float>(h.nsys);
     h.Ms = c.take<float>((size_t)h.nset * 9 * N);
+    h.Kn_own = c.take<float>((size_t)h.nset * 18 * N);
+    h.Tv_own = c.take<float>((size_t)h.nset * 18 * N);
     // finest-level vectors; the probing and power-iteration setup reuses the same memory
     const size_t pv = (size_t)N * 6;
     const size_t solve = (size_t)5 * h.npair * pv;
@@ -1763,11 +1766,17 @@ cudaError_t fine_cycle(const lpm_amg& h, const FcgScalars& sc, bool dot, cudaStr
 int amg_setup(lpm_amg& h, const float* Kn, const float* Tv, const float* Minv, cudaStream_t st)
 {
     const int64_t N = h.L.N;
-    h.Kn = Kn;
-    h.Tv = Tv;
+    // The cycle's operator reads the handle's own copy of the coefficients: every buffer a captured iteration block
+    // touches then stays at the same address from one setup to the next, so the graphs of the solve are reused
+    // across setups (a new numeric setup only rewrites device memory those graphs read).
     h.ready = false;
-    cudaError_t e = cudaMemsetAsync(h.err, 0, sizeof(int), st);
+    const size_t cb = sizeof(float) * (size_t)h.nset * 18 * N;
+    cudaError_t e = cudaMemcpyAsync(h.Kn_own, Kn, cb, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.Tv_own, Tv, cb, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h.err, 0, sizeof(int), st);
     if (e != cudaSuccess) return (int)e;
+    h.Kn = h.Kn_own;
+    h.Tv = h.Tv_own;
     k_repack_ms<<<grid2(N, VB, h.nset), VB, 0, st>>>(Minv, h.Ms, N);
     PairArgs base = pair_base(h);
     // ---- rho of the finest level: systems (set, k-th box), k < nb0
@@ -1961,8 +1970,7 @@ int amg_pcg(lpm_amg* hp, const float* b, float* x, const lpm_cg_opts& o, int* it
     };
     GraphKey key;
     key.ptr = {hp, b, x, o.tol_sys, h.Kn, h.Tv, iters, relres, status, nullptr};
-    key.val = {3, (long long)h.id, (long long)h.gen, o.poll, o.check, o.maxit, h.zchunk, h.variant, 0, 0, 0, 0, 0, 0,
-               0, 0};
+    key.val = {3, (long long)h.id, 0, o.poll, o.check, o.maxit, h.zchunk, h.variant, 0, 0, 0, 0, 0, 0, 0, 0};
     double tolv = o.tol;
     std::memcpy(&key.val[8], &tolv, sizeof(double));
     int it = 1, rc = LPM_OK;
