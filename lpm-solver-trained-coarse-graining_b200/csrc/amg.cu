@@ -29,6 +29,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "lpm_amg.h"
@@ -695,6 +696,344 @@ __global__ void __launch_bounds__(VB) k_probe_gen(BoxDev B, int a, int nx, int n
     for (int ax = 0; ax < 3; ++ax) o[ax] = make_float2(val[0][ax], val[1][ax]);
 }
 
+// ------------------------------------------------------------------------------- direct level-1 Galerkin product
+// A1 = P^T K_ff P from the bond coefficients, the product timing/t3d/amg3d.py:151-198 (_galerkin0 on _krow) forms,
+// without probe vectors.  One block per (aggregate J, coefficient set) computes the column block J: the fields
+// U_m = P_J e_m (mode m of J, zero off J) are rigid on J, so a bond stretch dL_ik = n_k.(U_i - U_q) vanishes unless
+// the bond crosses J's surface, and then it is n_k.P_J(i) (i in J) or -n_k.P_J(q) (q in J).  Hence
+//   (1) the shell sums S^c, TS^c of the six fields are nonzero only on J +- 1: they go to a shared table;
+//   (2) f_p = (K U_m)_p (lin3d.py:126-149: F_pk = 2 Kn dL + (TS_p^c + TS_q^c)/2 + Tv (S_p^c + S_q^c)/2,
+//       f_p = sum_k F_pk n_k) is nonzero only on J +- 2; it is formed for the box's sites there;
+//   (3) A1[I, J](r, m) = sum_{p in I} P_I(p)[:, r] . f_p[:, m] for the (up to 27) aggregates I next to J.  P_I(p) is
+//       affine in the site's offset d from I's centre, so this needs only the moments sum f and sum d f over I's
+//       sites, accumulated in FP64 in a fixed order: the result does not depend on scheduling.
+// Every (I, J) pair of neighbours is written by exactly one block.  Missing bonds (leaving the lattice) contribute
+// nothing, as in the operator; sites off the box have U = 0 but keep their shell sums (K_ff is K restricted to free
+// rows and columns, not the operator of a smaller lattice).  Requires aggregates at most GD_WMAX sites wide and at
+// least 2 wide where an axis has several (so J +- 2 meets only J's neighbours; the AMG takes a >= 3): a = 3 gives
+// widths 3..5.
+constexpr int GD_T = 256;
+constexpr int GD_WMAX = 5;
+constexpr int GD_SW = 28;  // floats per site of the shell-sum table: [c][S 0..5, TS 6..11], padded (float4 phases)
+
+// Slots whose offset along `axis` is `sgn` (-1, 0, +1), as a bit mask over the 18 slots.
+__host__ __device__ constexpr unsigned gd_dir(int axis, int sgn)
+{
+    unsigned m = 0;
+    for (int k = 0; k < 18; ++k) {
+        const int d = axis == 0 ? sc_dx(k) : axis == 1 ? sc_dy(k) : sc_dz(k);
+        if (d == sgn) m |= 1u << k;
+    }
+    return m;
+}
+
+// Slots k of site p whose neighbour p + o_k lies in the box [lo, hi] (inclusive).
+__device__ __forceinline__ unsigned gd_range(const int p[3], const int lo[3], const int hi[3])
+{
+    constexpr unsigned M[3][3] = {{gd_dir(0, -1), gd_dir(0, 0), gd_dir(0, 1)},
+                                  {gd_dir(1, -1), gd_dir(1, 0), gd_dir(1, 1)},
+                                  {gd_dir(2, -1), gd_dir(2, 0), gd_dir(2, 1)}};
+    unsigned m = 0x3FFFFu;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax)
+#pragma unroll
+        for (int d = -1; d <= 1; ++d)
+            if (p[ax] + d < lo[ax] || p[ax] + d > hi[ax]) m &= ~M[ax][d + 1];
+    return m;
+}
+
+struct GalJ {
+    int lo[3], hi[3];  // J's sites (inclusive)
+    float c[3];        // J's centre
+    float isn, i3, i4, i5;
+};
+
+// dL of slot k for the six fields of J across a bond crossing J's surface; d: offset of the bond's end in J from J's
+// centre, s = -w when p is in J (dL = n.P_J(p), n_k = -w o_k) and +w when q is (dL = -n.P_J(q)).
+template <int K>
+__device__ __forceinline__ void gd_dl(const GalJ& j, float dx, float dy, float dz, float s, float dl[6])
+{
+    constexpr float ox = (float)sc_dx(K), oy = (float)sc_dy(K), oz = (float)sc_dz(K);
+    dl[0] = s * ox * j.isn;
+    dl[1] = s * oy * j.isn;
+    dl[2] = s * oz * j.isn;
+    dl[3] = s * (oy * dx - ox * dy) * j.i3;
+    dl[4] = s * (oz * dy - oy * dz) * j.i4;
+    dl[5] = s * (ox * dz - oz * dx) * j.i5;
+}
+
+template <int K, typename F>
+__device__ __forceinline__ void gd_for(F&& f)
+{
+    if constexpr (K < 18) {
+        f(std::integral_constant<int, K>{});
+        gd_for<K + 1>(f);
+    }
+}
+
+// Shared memory of k_galerkin0 for aggregates at most wm sites wide: the shell-sum table on J +- 1 (reused for the
+// moments once step 2 is done) and the f table on J +- 2.
+__host__ __device__ inline size_t gd_stab_bytes(int wm)
+{
+    const size_t e1 = (size_t)wm + 2, s = e1 * e1 * e1 * GD_SW * sizeof(float), m = sizeof(double) * 27 * 18 * 4;
+    return ((s > m ? s : m) + 15) & ~size_t(15);
+}
+__host__ __device__ inline size_t gd_smem(int wm)
+{
+    const size_t e2 = (size_t)wm + 4;
+    return gd_stab_bytes(wm) + e2 * e2 * e2 * 18 * sizeof(float);
+}
+
+__global__ void __launch_bounds__(GD_T, 3) k_galerkin0(BoxDev B, int a, int wm, int nx, int ny, int nz, int64_t N,
+                                                       const float* __restrict__ Kn, const float* __restrict__ Tv,
+                                                       float* __restrict__ A1)
+{
+    extern __shared__ __align__(16) unsigned char gsm[];
+    const int E1 = wm + 2, E2 = wm + 4;
+    float* stab = reinterpret_cast<float*>(gsm);                       // (E1^3, GD_SW) shell sums on J +- 1
+    double* mom = reinterpret_cast<double*>(gsm);                      // (27, 18, 4) moments, after step 2
+    float* ftab = reinterpret_cast<float*>(gsm + gd_stab_bytes(wm));  // (E2^3, 18) f_p on J +- 2, [a * 6 + m]
+
+    const int J = blockIdx.x, set = blockIdx.y;
+    const int cj[3] = {J % B.nch[0], (J / B.nch[0]) % B.nch[1], J / (B.nch[0] * B.nch[1])};
+    GalJ g;
+    int wj[3], r1lo[3], r1hi[3];
+    for (int ax = 0; ax < 3; ++ax) {
+        int s0;
+        chunk_range(cj[ax], a, B.nch[ax], B.L[ax], s0, wj[ax]);
+        g.lo[ax] = B.lo[ax] + s0;
+        g.hi[ax] = g.lo[ax] + wj[ax] - 1;
+        g.c[ax] = (float)g.lo[ax] + 0.5f * (float)(wj[ax] - 1);
+        r1lo[ax] = g.lo[ax] - 1;
+        r1hi[ax] = g.hi[ax] + 1;
+    }
+    agg_scales(wj[0], wj[1], wj[2], g.isn, g.i3, g.i4, g.i5);
+    const int lat_lo[3] = {0, 0, 0}, lat_hi[3] = {nx - 1, ny - 1, nz - 1};
+    const float* kn = Kn + (int64_t)set * 18 * N;
+    const float* tv = Tv + (int64_t)set * 18 * N;
+    const int e1[3] = {wj[0] + 2, wj[1] + 2, wj[2] + 2};
+    const int n1 = e1[0] * e1[1] * e1[2];
+    const int sy1 = E1, sz1 = E1 * E1;  // table strides (the table's extent is E1 per axis)
+    auto tab_at = [&](int l) -> const float4* { return reinterpret_cast<const float4*>(stab + l * GD_SW); };
+
+    // (1) shell sums on J +- 1.  Only bonds crossing J's surface have a stretch: a site of J through its slots leaving
+    // J, a site outside through its slots entering J.  Sites off the lattice hold zero.
+    for (int t = threadIdx.x; t < n1; t += GD_T) {
+        const int lx = t % e1[0], ly = (t / e1[0]) % e1[1], lz = t / (e1[0] * e1[1]);
+        const int p3[3] = {r1lo[0] + lx, r1lo[1] + ly, r1lo[2] + lz};
+        float s[24];
+#pragma unroll
+        for (int m = 0; m < 24; ++m) s[m] = 0.f;
+        if (p3[0] >= 0 && p3[0] < nx && p3[1] >= 0 && p3[1] < ny && p3[2] >= 0 && p3[2] < nz) {
+            const int64_t i = ((int64_t)p3[2] * ny + p3[1]) * nx + p3[0];
+            const bool pj = p3[0] >= g.lo[0] && p3[0] <= g.hi[0] && p3[1] >= g.lo[1] && p3[1] <= g.hi[1] &&
+                            p3[2] >= g.lo[2] && p3[2] <= g.hi[2];
+            const unsigned qj = gd_range(p3, g.lo, g.hi);
+            const unsigned cross = gd_range(p3, lat_lo, lat_hi) & (pj ? ~qj : qj);
+            const float dx = (float)p3[0] - g.c[0], dy = (float)p3[1] - g.c[1], dz = (float)p3[2] - g.c[2];
+            gd_for<0>([&](auto kc) {
+                constexpr int k = decltype(kc)::value;
+                if (!((cross >> k) & 1u)) return;
+                constexpr float w = k < 6 ? 1.f : (float)INV_SQRT2;
+                constexpr int c = k < 6 ? 0 : 12;
+                float dl[6];
+                if (pj)
+                    gd_dl<k>(g, dx, dy, dz, -w, dl);
+                else
+                    gd_dl<k>(g, dx + sc_dx(k), dy + sc_dy(k), dz + sc_dz(k), w, dl);
+                const float t_ = __ldg(tv + (int64_t)k * N + i);
+#pragma unroll
+                for (int m = 0; m < 6; ++m) {
+                    s[c + m] += dl[m];
+                    s[c + 6 + m] = fmaf(t_, dl[m], s[c + 6 + m]);
+                }
+            });
+        }
+        float4* o = reinterpret_cast<float4*>(stab + ((lz * E1 + ly) * E1 + lx) * GD_SW);
+#pragma unroll
+        for (int v = 0; v < 6; ++v) o[v] = make_float4(s[4 * v], s[4 * v + 1], s[4 * v + 2], s[4 * v + 3]);
+    }
+    __syncthreads();
+
+    // (2) f_p on the box's sites of J +- 2.  Items 0..n1-1: the sites of J +- 1 (every slot may contribute); items
+    // n1..n1+n2-1: the sites of J +- 2 outside J +- 1, which have no shell sums and no crossing bond, so only their
+    // slots reaching into J +- 1 contribute (F = TS_q/2 + Tv S_q/2), one to five of them.
+    const int e2[3] = {wj[0] + 4, wj[1] + 4, wj[2] + 4};
+    const int n2 = e2[0] * e2[1] * e2[2];
+    const int bhi[3] = {B.lo[0] + B.L[0] - 1, B.lo[1] + B.L[1] - 1, B.lo[2] + B.L[2] - 1};
+    for (int t = threadIdx.x; t < n1 + n2; t += GD_T) {
+        int l2[3];
+        if (t < n1) {
+            l2[0] = t % e1[0] + 1;
+            l2[1] = (t / e1[0]) % e1[1] + 1;
+            l2[2] = t / (e1[0] * e1[1]) + 1;
+        } else {
+            const int u = t - n1;
+            l2[0] = u % e2[0];
+            l2[1] = (u / e2[0]) % e2[1];
+            l2[2] = u / (e2[0] * e2[1]);
+            if (l2[0] >= 1 && l2[0] <= e1[0] && l2[1] >= 1 && l2[1] <= e1[1] && l2[2] >= 1 && l2[2] <= e1[2])
+                continue;  // a site of J +- 1: item t < n1
+        }
+        const int p3[3] = {g.lo[0] - 2 + l2[0], g.lo[1] - 2 + l2[1], g.lo[2] - 2 + l2[2]};
+        if (p3[0] < B.lo[0] || p3[0] > bhi[0] || p3[1] < B.lo[1] || p3[1] > bhi[1] || p3[2] < B.lo[2] ||
+            p3[2] > bhi[2])
+            continue;  // no row of K_ff
+        const int64_t i = ((int64_t)p3[2] * ny + p3[1]) * nx + p3[0];
+        const unsigned valid = gd_range(p3, lat_lo, lat_hi);
+        const unsigned qr1 = gd_range(p3, r1lo, r1hi) & valid;
+        const int lp = ((l2[2] - 1) * E1 + (l2[1] - 1)) * E1 + (l2[0] - 1);  // table index (p's own: J +- 1 only)
+        float f[18];
+#pragma unroll
+        for (int m = 0; m < 18; ++m) f[m] = 0.f;
+        auto add_f = [&](auto kc, const float F[6]) {  // f += F n_k, n_k = -w o_k
+            constexpr int k = decltype(kc)::value;
+            constexpr float w = k < 6 ? 1.f : (float)INV_SQRT2;
+            constexpr int o3[3] = {sc_dx(k), sc_dy(k), sc_dz(k)};
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax) {
+                if (o3[ax] == 0) continue;
+                const float nk = -w * (float)o3[ax];
+#pragma unroll
+                for (int m = 0; m < 6; ++m) f[ax * 6 + m] = fmaf(nk, F[m], f[ax * 6 + m]);
+            }
+        };
+        auto sums = [&](int l, int c, float sv[12]) {
+            const float4* p4 = tab_at(l) + c * 3;
+#pragma unroll
+            for (int v = 0; v < 3; ++v) {
+                const float4 q = p4[v];
+                sv[4 * v] = q.x;
+                sv[4 * v + 1] = q.y;
+                sv[4 * v + 2] = q.z;
+                sv[4 * v + 3] = q.w;
+            }
+        };
+        if (t < n1) {
+            const bool pj = p3[0] >= g.lo[0] && p3[0] <= g.hi[0] && p3[1] >= g.lo[1] && p3[1] <= g.hi[1] &&
+                            p3[2] >= g.lo[2] && p3[2] <= g.hi[2];
+            const unsigned qj = gd_range(p3, g.lo, g.hi);
+            const unsigned cross = valid & (pj ? ~qj : qj);
+            const float dx = (float)p3[0] - g.c[0], dy = (float)p3[1] - g.c[1], dz = (float)p3[2] - g.c[2];
+            float tvp[18];
+#pragma unroll
+            for (int k = 0; k < 18; ++k) tvp[k] = __ldg(tv + (int64_t)k * N + i);
+            float sp[24];
+            sums(lp, 0, sp);
+            sums(lp, 1, sp + 12);
+            gd_for<0>([&](auto kc) {
+                constexpr int k = decltype(kc)::value;
+                if (!((valid >> k) & 1u)) return;
+                constexpr int c = k < 6 ? 0 : 1;
+                float sq[12];
+                if ((qr1 >> k) & 1u) {
+                    sums(lp + sc_dx(k) + sc_dy(k) * sy1 + sc_dz(k) * sz1, c, sq);
+                } else {
+#pragma unroll
+                    for (int m = 0; m < 12; ++m) sq[m] = 0.f;
+                }
+                const float tvh = 0.5f * tvp[k];
+                float F[6];
+#pragma unroll
+                for (int m = 0; m < 6; ++m)
+                    F[m] = fmaf(tvh, sp[12 * c + m] + sq[m], 0.5f * (sp[12 * c + 6 + m] + sq[6 + m]));
+                if ((cross >> k) & 1u) {
+                    constexpr float w = k < 6 ? 1.f : (float)INV_SQRT2;
+                    float dl[6];
+                    if (pj)
+                        gd_dl<k>(g, dx, dy, dz, -w, dl);
+                    else
+                        gd_dl<k>(g, dx + sc_dx(k), dy + sc_dy(k), dz + sc_dz(k), w, dl);
+                    const float kn2 = 2.f * __ldg(kn + (int64_t)k * N + i);
+#pragma unroll
+                    for (int m = 0; m < 6; ++m) F[m] = fmaf(kn2, dl[m], F[m]);
+                }
+                add_f(kc, F);
+            });
+        } else if (qr1) {
+            gd_for<0>([&](auto kc) {
+                constexpr int k = decltype(kc)::value;
+                if (!((qr1 >> k) & 1u)) return;
+                constexpr int c = k < 6 ? 0 : 1;
+                float sq[12];
+                sums(lp + sc_dx(k) + sc_dy(k) * sy1 + sc_dz(k) * sz1, c, sq);
+                const float tvh = 0.5f * __ldg(tv + (int64_t)k * N + i);
+                float F[6];
+#pragma unroll
+                for (int m = 0; m < 6; ++m) F[m] = fmaf(tvh, sq[m], 0.5f * sq[6 + m]);
+                add_f(kc, F);
+            });
+        }
+        float* o = ftab + ((l2[2] * E2 + l2[1]) * E2 + l2[0]) * 18;
+#pragma unroll
+        for (int m = 0; m < 18; ++m) o[m] = f[m];
+    }
+    __syncthreads();  // the shell-sum table is dead from here: its memory takes the moments
+
+    // (3) moments sum f, sum dx f, sum dy f, sum dz f over the sites of each neighbour I within J +- 2
+    for (int it = threadIdx.x; it < 27 * 18; it += GD_T) {
+        const int e = it / 18, am = it % 18;
+        const int ci[3] = {cj[0] + e % 3 - 1, cj[1] + (e / 3) % 3 - 1, cj[2] + e / 9 - 1};
+        if (ci[0] < 0 || ci[0] >= B.nch[0] || ci[1] < 0 || ci[1] >= B.nch[1] || ci[2] < 0 || ci[2] >= B.nch[2])
+            continue;
+        int lo[3], hi[3];
+        float cc[3];
+        for (int ax = 0; ax < 3; ++ax) {
+            int s0, w;
+            chunk_range(ci[ax], a, B.nch[ax], B.L[ax], s0, w);
+            const int il = B.lo[ax] + s0;
+            cc[ax] = (float)il + 0.5f * (float)(w - 1);
+            lo[ax] = max(il, g.lo[ax] - 2);
+            hi[ax] = min(il + w - 1, g.hi[ax] + 2);
+        }
+        double m0 = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+        for (int z = lo[2]; z <= hi[2]; ++z)
+            for (int y = lo[1]; y <= hi[1]; ++y)
+                for (int x = lo[0]; x <= hi[0]; ++x) {
+                    const int l = ((z - g.lo[2] + 2) * E2 + (y - g.lo[1] + 2)) * E2 + (x - g.lo[0] + 2);
+                    const double v = (double)ftab[l * 18 + am];
+                    m0 += v;
+                    mx += (double)((float)x - cc[0]) * v;
+                    my += (double)((float)y - cc[1]) * v;
+                    mz += (double)((float)z - cc[2]) * v;
+                }
+        double* o = mom + (size_t)it * 4;
+        o[0] = m0;
+        o[1] = mx;
+        o[2] = my;
+        o[3] = mz;
+    }
+    __syncthreads();
+
+    // (4) A1[I][d][r][m] with J = I + off(d): off = -e
+    const int n1agg = B.n1;
+    for (int it = threadIdx.x; it < 27 * 36; it += GD_T) {
+        const int e = it / 36, r = (it % 36) / 6, m = it % 6;
+        const int ci[3] = {cj[0] + e % 3 - 1, cj[1] + (e / 3) % 3 - 1, cj[2] + e / 9 - 1};
+        if (ci[0] < 0 || ci[0] >= B.nch[0] || ci[1] < 0 || ci[1] >= B.nch[1] || ci[2] < 0 || ci[2] >= B.nch[2])
+            continue;
+        int wi[3];
+        for (int ax = 0; ax < 3; ++ax) {
+            int s0;
+            chunk_range(ci[ax], a, B.nch[ax], B.L[ax], s0, wi[ax]);
+        }
+        float isn, i3, i4, i5;
+        agg_scales(wi[0], wi[1], wi[2], isn, i3, i4, i5);
+        auto M = [&](int ax, int q) { return mom[((size_t)e * 18 + ax * 6 + m) * 4 + q]; };  // q: 0 sum, 1..3 d
+        double v;
+        switch (r) {
+        case 0: case 1: case 2: v = (double)isn * M(r, 0); break;
+        case 3: v = (double)i3 * (M(1, 1) - M(0, 2)); break;
+        case 4: v = (double)i4 * (M(2, 2) - M(1, 3)); break;
+        default: v = (double)i5 * (M(0, 3) - M(2, 1)); break;
+        }
+        const int I = (ci[2] * B.nch[1] + ci[1]) * B.nch[0] + ci[0];
+        const int d = ((1 - (e / 9 - 1)) * 3 + (1 - ((e / 3) % 3 - 1))) * 3 + (1 - (e % 3 - 1));
+        A1[((int64_t)set * ST + d * 36 + r * 6 + m) * n1agg + I] = (float)v;
+    }
+}
+
+
 
 // --------------------------------------------------------------------------------- finest power iteration
 // Systems q = set * nb0 + k (k-th box of the set) in the pair layout with rps = nb0.
@@ -1265,63 +1604,100 @@ __global__ void __launch_bounds__(GJ* GJ) k_gj_diag(int K, int ncp, const double
     Pinv[((int64_t)set * GJ + ty) * GJ + tx] = m[ty][tx];
 }
 
-__global__ void __launch_bounds__(LB) k_gj_row(int K, int ncp, double* __restrict__ D, const double* __restrict__ Pinv)
+// Row step: D_KJ = Pinv D_KJ for every block column J != K.  One block per (J, set): the 32 x 32 block and Pinv in
+// shared memory, 4 outputs per thread.
+__global__ void __launch_bounds__(256) k_gj_row(int K, int ncp, double* __restrict__ D, const double* __restrict__ Pinv)
 {
-    __shared__ double P[GJ][GJ];
-    const int set = blockIdx.y;
-    for (int e = threadIdx.x; e < GJ * GJ; e += LB) P[e / GJ][e % GJ] = Pinv[(int64_t)set * GJ * GJ + e];
-    __syncthreads();
-    const int j = blockIdx.x * LB + threadIdx.x;
-    if (j >= ncp || j / GJ == K) return;
+    __shared__ double P[GJ][GJ + 1], X[GJ][GJ + 1];
+    const int J = blockIdx.x, set = blockIdx.y;
+    if (J == K) return;
     double* Ds = D + (int64_t)set * ncp * ncp;
-    double col[GJ];
-    for (int k = 0; k < GJ; ++k) col[k] = Ds[(int64_t)(K * GJ + k) * ncp + j];
-    for (int r = 0; r < GJ; ++r) {
-        double s = 0.0;
-        for (int k = 0; k < GJ; ++k) s += P[r][k] * col[k];
-        Ds[(int64_t)(K * GJ + r) * ncp + j] = s;
-    }
-}
-
-__global__ void __launch_bounds__(GJ * 8) k_gj_trail(int K, int ncp, double* __restrict__ D)
-{
-    __shared__ double Aik[GJ][GJ + 1], Akj[GJ][GJ + 1];
-    const int bi = blockIdx.y, bj = blockIdx.x, set = blockIdx.z;
-    if (bi == K || bj == K) return;
-    double* Ds = D + (int64_t)set * ncp * ncp;
-    const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+    const int tx = threadIdx.x % GJ, ty = threadIdx.x / GJ;  // 32 x 8
     for (int r = ty; r < GJ; r += 8) {
-        Aik[r][tx] = Ds[(int64_t)(bi * GJ + r) * ncp + K * GJ + tx];
-        Akj[r][tx] = Ds[(int64_t)(K * GJ + r) * ncp + bj * GJ + tx];
+        P[r][tx] = Pinv[((int64_t)set * GJ + r) * GJ + tx];
+        X[r][tx] = Ds[(int64_t)(K * GJ + r) * ncp + J * GJ + tx];
     }
     __syncthreads();
     for (int r = ty; r < GJ; r += 8) {
         double s = 0.0;
-        for (int k = 0; k < GJ; ++k) s += Aik[r][k] * Akj[k][tx];
-        Ds[(int64_t)(bi * GJ + r) * ncp + bj * GJ + tx] -= s;
+#pragma unroll 8
+        for (int k = 0; k < GJ; ++k) s = fma(P[r][k], X[k][tx], s);
+        Ds[(int64_t)(K * GJ + r) * ncp + J * GJ + tx] = s;
     }
 }
 
-__global__ void __launch_bounds__(LB) k_gj_col(int K, int ncp, double* __restrict__ D, const double* __restrict__ Pinv)
+// Trailing step: D_IJ -= D_IK D_KJ for I, J != K, on 64 x 64 tiles (4 x 4 outputs per thread from shared-memory
+// panels of D_IK and D_KJ).  A tile may hold part of the pivot row or column block, which it leaves alone.
+constexpr int GT = 64;
+__global__ void __launch_bounds__(256) k_gj_trail(int K, int ncp, double* __restrict__ D)
 {
-    __shared__ double P[GJ][GJ];
-    const int set = blockIdx.y;
-    for (int e = threadIdx.x; e < GJ * GJ; e += LB) P[e / GJ][e % GJ] = Pinv[(int64_t)set * GJ * GJ + e];
-    __syncthreads();
-    const int i = blockIdx.x * LB + threadIdx.x;
-    if (i >= ncp) return;
+    __shared__ double Aik[GJ][GT + 1], Akj[GJ][GT];
+    const int i0 = blockIdx.y * GT, j0 = blockIdx.x * GT, set = blockIdx.z, k0 = K * GJ;
+    if (i0 >= ncp || j0 >= ncp) return;
+    if ((i0 / GJ == K && i0 + GJ >= ncp) || (j0 / GJ == K && j0 + GJ >= ncp)) return;  // only pivot rows / columns
     double* Ds = D + (int64_t)set * ncp * ncp;
-    double* row = Ds + (int64_t)i * ncp + K * GJ;
-    if (i / GJ == K) {
-        for (int c = 0; c < GJ; ++c) row[c] = P[i % GJ][c];
-        return;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < GT * GJ; e += 256) {
+        const int r = e / GJ, k = e % GJ;
+        Aik[k][r] = i0 + r < ncp ? Ds[(int64_t)(i0 + r) * ncp + k0 + k] : 0.0;
+        const int kk = e / GT, c = e % GT;
+        Akj[kk][c] = j0 + c < ncp ? Ds[(int64_t)(k0 + kk) * ncp + j0 + c] : 0.0;
     }
-    double rv[GJ];
-    for (int k = 0; k < GJ; ++k) rv[k] = row[k];
-    for (int c = 0; c < GJ; ++c) {
-        double s = 0.0;
-        for (int k = 0; k < GJ; ++k) s += rv[k] * P[k][c];
-        row[c] = -s;
+    __syncthreads();
+    const int tr = tid / 16, tc = tid % 16;  // rows tr + 16 q, columns tc + 16 s
+    double acc[4][4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int t = 0; t < 4; ++t) acc[q][t] = 0.0;
+#pragma unroll 4
+    for (int k = 0; k < GJ; ++k) {
+        double av[4], bv[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            av[q] = Aik[k][tr + 16 * q];
+            bv[q] = Akj[k][tc + 16 * q];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int t = 0; t < 4; ++t) acc[q][t] = fma(av[q], bv[t], acc[q][t]);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int i = i0 + tr + 16 * q;
+        if (i >= ncp || i / GJ == K) continue;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const int j = j0 + tc + 16 * t;
+            if (j < ncp && j / GJ != K) Ds[(int64_t)i * ncp + j] -= acc[q][t];
+        }
+    }
+}
+
+// Column step: D_IK = -D_IK Pinv for every block row I != K, and D_KK = Pinv.  One block per (I, set).
+__global__ void __launch_bounds__(256) k_gj_col(int K, int ncp, double* __restrict__ D, const double* __restrict__ Pinv)
+{
+    __shared__ double P[GJ][GJ + 1], X[GJ][GJ + 1];
+    const int I = blockIdx.x, set = blockIdx.y;
+    double* Ds = D + (int64_t)set * ncp * ncp;
+    const int tx = threadIdx.x % GJ, ty = threadIdx.x / GJ;
+    for (int r = ty; r < GJ; r += 8) {
+        P[r][tx] = Pinv[((int64_t)set * GJ + r) * GJ + tx];
+        X[r][tx] = Ds[(int64_t)(I * GJ + r) * ncp + K * GJ + tx];
+    }
+    __syncthreads();
+    for (int r = ty; r < GJ; r += 8) {
+        double s;
+        if (I == K) {
+            s = P[r][tx];
+        } else {
+            s = 0.0;
+#pragma unroll 8
+            for (int k = 0; k < GJ; ++k) s = fma(X[r][k], P[k][tx], s);
+            s = -s;
+        }
+        Ds[(int64_t)(I * GJ + r) * ncp + K * GJ + tx] = s;
     }
 }
 
@@ -1763,6 +2139,33 @@ cudaError_t fine_cycle(const lpm_amg& h, const FcgScalars& sc, bool dot, cudaStr
 }
 
 // ------------------------------------------------------------------------------------------- numeric setup
+// Widest aggregate of a box (the last chunk of an axis is the widest).  The direct level-1 product covers boxes whose
+// aggregates are at most GD_WMAX sites wide (a = 3: widths 3..5); wider aggregates are probed.
+int box_wmax(const lpm_amg::Box& b, int a)
+{
+    int wm = 1;
+    for (int ax = 0; ax < 3; ++ax) {
+        int s0, w;
+        chunk_range(b.nch[ax] - 1, a, b.nch[ax], b.L[ax], s0, w);
+        wm = std::max(wm, w);
+    }
+    return wm;
+}
+
+// Opt-in to k_galerkin0's dynamic shared memory (its largest size), once per device.
+cudaError_t galerkin0_attr()
+{
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if ((done.load() >> dev) & 1ull) return cudaSuccess;
+    e = cudaFuncSetAttribute(k_galerkin0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gd_smem(GD_WMAX));
+    if (e == cudaSuccess) done.fetch_or(1ull << dev);
+    return e;
+}
+
 int amg_setup(lpm_amg& h, const float* Kn, const float* Tv, const float* Minv, cudaStream_t st)
 {
     const int64_t N = h.L.N;
@@ -1813,27 +2216,37 @@ int amg_setup(lpm_amg& h, const float* Kn, const float* Tv, const float* Minv, c
             B.nch[ax] = b.nch[ax];
         }
         B.n1 = L1.n;
-        // ---- level 1 by probing: 27 colour classes x 6 modes in chunks of PCOL colours
         if ((e = cudaMemsetAsync(L1.A, 0, sizeof(float) * (size_t)h.nset * ST * L1.n, st)) != cudaSuccess) return (int)e;
-        float* pv = h.xp;
-        float* py = h.xp + (size_t)h.nset * PNP * N * 6;
-        PairArgs a = base;
-        a.nsys = h.nset * PQ;
-        a.rhs_per_set = PQ;
-        a.npp = PNP;
-        a.npair = h.nset * PNP;
-        a.zchunk = h.zchunk_probe;
-        a.variant = pair_variant(h.L.nx, h.L.ny, h.L.nz, a.npair);
-        a.u = pv;
-        a.out = py;
-        if ((e = cudaMemsetAsync(pv, 0, sizeof(float) * (size_t)h.nset * PNP * N * 6, st)) != cudaSuccess) return (int)e;
-        for (int chunk = 0; chunk < 27 / PCOL; ++chunk) {
-            k_probe_gen<<<grid2(N, VB, h.nset * PNP), VB, 0, st>>>(B, h.o.agg, h.L.nx, h.L.ny, N, chunk, pv);
-            if ((e = launch_sc_pair_mode(a, PM_NONE, st)) != cudaSuccess) return (int)e;
-            k_restrict0<true><<<dim3(b.t0.tiles, h.nset * PNP), 256, b.t0.smem, st>>>(
-                B, h.o.agg, b.t0.tw, b.t0.th, h.L.nx, h.L.ny, N, nullptr, nullptr, nullptr, py, chunk, L1.A);
+        const int wm = box_wmax(b, h.o.agg);
+        if (wm <= GD_WMAX) {
+            // ---- level 1 directly from the bonds
+            if ((e = galerkin0_attr()) != cudaSuccess) return (int)e;
+            k_galerkin0<<<dim3((unsigned)L1.n, h.nset), GD_T, gd_smem(wm), st>>>(B, h.o.agg, wm, h.L.nx, h.L.ny,
+                                                                                h.L.nz, N, h.Kn, h.Tv, L1.A);
+            if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+        } else {
+            // ---- level 1 by probing: 27 colour classes x 6 modes in chunks of PCOL colours
+            float* pv = h.xp;
+            float* py = h.xp + (size_t)h.nset * PNP * N * 6;
+            PairArgs a = base;
+            a.nsys = h.nset * PQ;
+            a.rhs_per_set = PQ;
+            a.npp = PNP;
+            a.npair = h.nset * PNP;
+            a.zchunk = h.zchunk_probe;
+            a.variant = pair_variant(h.L.nx, h.L.ny, h.L.nz, a.npair);
+            a.u = pv;
+            a.out = py;
+            if ((e = cudaMemsetAsync(pv, 0, sizeof(float) * (size_t)h.nset * PNP * N * 6, st)) != cudaSuccess)
+                return (int)e;
+            for (int chunk = 0; chunk < 27 / PCOL; ++chunk) {
+                k_probe_gen<<<grid2(N, VB, h.nset * PNP), VB, 0, st>>>(B, h.o.agg, h.L.nx, h.L.ny, N, chunk, pv);
+                if ((e = launch_sc_pair_mode(a, PM_NONE, st)) != cudaSuccess) return (int)e;
+                k_restrict0<true><<<dim3(b.t0.tiles, h.nset * PNP), 256, b.t0.smem, st>>>(
+                    B, h.o.agg, b.t0.tw, b.t0.th, h.L.nx, h.L.ny, N, nullptr, nullptr, nullptr, py, chunk, L1.A);
+            }
+            if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
         }
-        if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
         // ---- levels below: block inverses, rho, Galerkin products
         for (int l = 0; l < b.nlev - 1; ++l) {
             auto& Lv = b.lev[l];
@@ -1859,12 +2272,12 @@ int amg_setup(lpm_amg& h, const float* Kn, const float* Tv, const float* Minv, c
         k_dense_build<<<dim3((unsigned)((std::max(Lc.n, b.ncp) + 127) / 128), 27, h.nset), 128, 0, st>>>(
             Lc.g[0], Lc.g[1], Lc.g[2], b.ncp, Lc.A, b.Ainv);
         k_dense_sym<<<dim3((b.nc + 15) / 16, (b.nc + 15) / 16, h.nset), dim3(16, 16), 0, st>>>(b.nc, b.ncp, b.Ainv);
-        const int nbk = b.ncp / GJ;
+        const int nbk = b.ncp / GJ, ntl = (b.ncp + GT - 1) / GT;
         for (int K = 0; K < nbk; ++K) {
             k_gj_diag<<<h.nset, dim3(GJ, GJ), 0, st>>>(K, b.ncp, b.Ainv, h.Pinv);
-            k_gj_row<<<grid2(b.ncp, LB, h.nset), LB, 0, st>>>(K, b.ncp, b.Ainv, h.Pinv);
-            k_gj_trail<<<dim3(nbk, nbk, h.nset), dim3(GJ, 8), 0, st>>>(K, b.ncp, b.Ainv);
-            k_gj_col<<<grid2(b.ncp, LB, h.nset), LB, 0, st>>>(K, b.ncp, b.Ainv, h.Pinv);
+            k_gj_row<<<dim3(nbk, h.nset), 256, 0, st>>>(K, b.ncp, b.Ainv, h.Pinv);
+            k_gj_trail<<<dim3(ntl, ntl, h.nset), 256, 0, st>>>(K, b.ncp, b.Ainv);
+            k_gj_col<<<dim3(nbk, h.nset), 256, 0, st>>>(K, b.ncp, b.Ainv, h.Pinv);
         }
         const int64_t ne = (int64_t)h.nset * b.ncp * b.ncp;
         k_to_f32<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(b.Ainv, b.Ainv32, ne);

@@ -2,7 +2,8 @@
 pinned to the reference's timing/t3d/amg3d.py in test_oracle_amg.py): levels, rho, one cycle, PCG iterations, the
 mixed-precision solve, batching, and the reference-named mirror (AMGGeom / AMG3D).
 
-Tolerances: the CUDA hierarchy is FP32 (operators from FP32 K.u probes, FP32 smoothing), so levels and cycles agree with
+Tolerances: the CUDA hierarchy is FP32 (level 1 from the bonds in FP32 with FP64 moments, or from FP32 K.u probes for
+aggregates wider than 5 sites; FP32 smoothing), so levels and cycles agree with
 the FP64 oracle to FP32 round-off amplified by the operator's conditioning (<= 2e-4 relative); solved displacements
 agree to the solve tolerance.
 """
@@ -73,6 +74,25 @@ def test_amg_levels_match_oracle(case24):
             assert relmax(A, orc[k].A[lvl - 1]) < 2e-5, (k, lvl)
             if lvl < len(grids):
                 assert abs(rho - orc[k].rho[lvl - 1]) < 1e-4 * orc[k].rho[lvl - 1]
+
+
+@pytest.mark.parametrize("agg", [4, 5])
+def test_amg_level1_probing_path_matches_oracle(agg):
+    """Aggregates of 4 or 5 sites (chunks up to 7 or 9 wide) take the probing construction of the level-1 operator
+    instead of the direct bond product (which covers widths up to 5, all of agg = 3): both must give P^T K_ff P."""
+    n = 20
+    lat, Kn, Tv = specimen(n, 9, 2.5)
+    free, _ = bcs(lat, n, ("k_xx", "lr_tx"))
+    dl = core.DeviceLattice(lat, "cuda")
+    Kd = torch.as_tensor(Kn, device="cuda")[None]
+    Td = torch.as_tensor(Tv, device="cuda")[None]
+    ab = GA.AmgBatch(dl, 2, 2, free, agg=agg, coarse_max=100, nu=1, gamma=2, power_its=5)
+    ab.setup(core.pack(Kd, torch.float32), core.pack(Td, torch.float32), core.block_jacobi(dl, Kd, Td, torch.float32))
+    for k in range(2):
+        geo = OA.Geometry(lat, free[k], agg=agg, coarse_max=100)
+        A, _ = ab.level(k, 0, 1)
+        assert relmax(A, OA.galerkin0(geo, Kn, Tv)) < 2e-5, (agg, k)
+    ab.close()
 
 
 def test_amg_cycle_matches_oracle(case24):
