@@ -50,6 +50,10 @@ constexpr int PCOL = 3;           // colour classes per probing chunk
 constexpr int PQ = 6 * PCOL;      // probe systems per set and chunk
 constexpr int PNP = PQ / 2;       // probe pairs per set and chunk
 constexpr int ST = 972;           // 27 * 36 coefficients per stencil row
+// Level operators are symmetric (A_l = P^T K_ff P with K_ff symmetric), so a stencil is stored as its upper half:
+// directions d = 13..26 (the diagonal block and the offsets that come later in (z, y, x) order) at index d - 13; the
+// block of direction d < 13 at node I is the transpose of the block of direction 26 - d at node I + off(d).
+constexpr int STS = 14 * 36;      // stored coefficients per stencil row
 constexpr int RS = 8;             // systems per pass of the group kernels
 
 inline int nchunks(int L, int a) { return std::max(1, L / a); }
@@ -598,7 +602,7 @@ __global__ void __launch_bounds__(256) k_restrict0(BoxDev B, int a, int tw, int 
             }
             if (!ok) continue;
             const int d = ((off[2] + 1) * 3 + off[1] + 1) * 3 + off[0] + 1;
-            A1[((int64_t)set * ST + d * 36 + c * 6 + mode) * B.n1 + I] = v;
+            if (d >= 13) A1[((int64_t)set * STS + (d - 13) * 36 + c * 6 + mode) * B.n1 + I] = v;
         }
     }
 }
@@ -970,8 +974,9 @@ __global__ void __launch_bounds__(GD_T, 3) k_galerkin0(BoxDev B, int a, int wm, 
     }
     __syncthreads();  // the shell-sum table is dead from here: its memory takes the moments
 
-    // (3) moments sum f, sum dx f, sum dy f, sum dz f over the sites of each neighbour I within J +- 2
-    for (int it = threadIdx.x; it < 27 * 18; it += GD_T) {
+    // (3) moments sum f, sum dx f, sum dy f, sum dz f over the sites of each neighbour I within J +- 2.  Only the
+    // stored half is formed: I = J + e - (1, 1, 1) has J in direction d = 26 - e of I, kept when d >= 13 (e <= 13).
+    for (int it = threadIdx.x; it < 14 * 18; it += GD_T) {
         const int e = it / 18, am = it % 18;
         const int ci[3] = {cj[0] + e % 3 - 1, cj[1] + (e / 3) % 3 - 1, cj[2] + e / 9 - 1};
         if (ci[0] < 0 || ci[0] >= B.nch[0] || ci[1] < 0 || ci[1] >= B.nch[1] || ci[2] < 0 || ci[2] >= B.nch[2])
@@ -1007,7 +1012,7 @@ __global__ void __launch_bounds__(GD_T, 3) k_galerkin0(BoxDev B, int a, int wm, 
 
     // (4) A1[I][d][r][m] with J = I + off(d): off = -e
     const int n1agg = B.n1;
-    for (int it = threadIdx.x; it < 27 * 36; it += GD_T) {
+    for (int it = threadIdx.x; it < 14 * 36; it += GD_T) {
         const int e = it / 36, r = (it % 36) / 6, m = it % 6;
         const int ci[3] = {cj[0] + e % 3 - 1, cj[1] + (e / 3) % 3 - 1, cj[2] + e / 9 - 1};
         if (ci[0] < 0 || ci[0] >= B.nch[0] || ci[1] < 0 || ci[1] >= B.nch[1] || ci[2] < 0 || ci[2] >= B.nch[2])
@@ -1029,7 +1034,7 @@ __global__ void __launch_bounds__(GD_T, 3) k_galerkin0(BoxDev B, int a, int wm, 
         }
         const int I = (ci[2] * B.nch[1] + ci[1]) * B.nch[0] + ci[0];
         const int d = ((1 - (e / 9 - 1)) * 3 + (1 - ((e / 3) % 3 - 1))) * 3 + (1 - (e % 3 - 1));
-        A1[((int64_t)set * ST + d * 36 + r * 6 + m) * n1agg + I] = (float)v;
+        A1[((int64_t)set * STS + (d - 13) * 36 + r * 6 + m) * n1agg + I] = (float)v;
     }
 }
 
@@ -1139,9 +1144,26 @@ __global__ void k_level_weights(int nset, const double* __restrict__ rho, double
 }
 
 // ------------------------------------------------------------------------------------------ coarse levels
+// The 6 x 6 block of direction d at node I (J = I + off(d)) of an upper-half stencil, row-major into av.
+__device__ __forceinline__ void lv_block(const float* __restrict__ As, int64_t n, int set, int I, int J, int d,
+                                         float av[36])
+{
+    if (d >= 13) {
+        const float* p = As + ((int64_t)set * STS + (d - 13) * 36) * n + I;
+#pragma unroll
+        for (int e = 0; e < 36; ++e) av[e] = __ldg(p + (int64_t)e * n);
+    } else {
+        const float* p = As + ((int64_t)set * STS + (13 - d) * 36) * n + J;
+#pragma unroll
+        for (int r = 0; r < 6; ++r)
+#pragma unroll
+            for (int c = 0; c < 6; ++c) av[r * 6 + c] = __ldg(p + (int64_t)(c * 6 + r) * n);
+    }
+}
+
 struct LvView {
     int gx, gy, gz, n;
-    const float* A;     // (nset, ST, n)
+    const float* A;     // (nset, STS, n): upper-half stencil
     const float* Minv;  // (nset, 36, n)
     const float* w;     // (nset)
 };
@@ -1161,7 +1183,8 @@ __device__ __forceinline__ bool row_set(const int* sys, int rps, const int* act,
 
 // MODE 0: y = A x;  1: y = b - A x;  2: y = x + w M (b - A x).  out = y, or out += y when acc.  One thread per node
 // and system group g = (set, first row j0, rows cnt) -- the systems of one coefficient set in this box, RS per pass --
-// so each stencil row of A (and M) is read once for all of them.  Rows of inactive systems are skipped.
+// so each stencil row of A (and M) is read once for all of them (splitting a group's systems over threads re-reads
+// the rows and measured slower).  Rows of inactive systems are skipped.
 template <int MODE>
 __global__ void __launch_bounds__(LB) k_lv_op(LvView V, const int* __restrict__ grp, const int* __restrict__ sys,
                                               const int* __restrict__ act, const float* __restrict__ x,
@@ -1171,7 +1194,6 @@ __global__ void __launch_bounds__(LB) k_lv_op(LvView V, const int* __restrict__ 
     if (I >= V.n) return;
     const int set = grp[3 * blockIdx.y], j0 = grp[3 * blockIdx.y + 1], cnt = grp[3 * blockIdx.y + 2];
     const int i0 = I % V.gx, i1 = (I / V.gx) % V.gy, i2 = I / (V.gx * V.gy);
-    const float* Ab = V.A + (int64_t)set * ST * V.n + I;
     for (int c0 = 0; c0 < cnt; c0 += RS) {
         const int nc = min(RS, cnt - c0);
         bool on[RS];
@@ -1191,11 +1213,10 @@ __global__ void __launch_bounds__(LB) k_lv_op(LvView V, const int* __restrict__ 
         for (int d = 0; d < 27; ++d) {
             const int q0 = i0 + d % 3 - 1, q1 = i1 + (d / 3) % 3 - 1, q2 = i2 + d / 9 - 1;
             if (q0 < 0 || q0 >= V.gx || q1 < 0 || q1 >= V.gy || q2 < 0 || q2 >= V.gz) continue;
-            const int64_t Jo = (int64_t)((q2 * V.gy + q1) * V.gx + q0) * 6;
-            const float* Ad = Ab + (int64_t)d * 36 * V.n;
+            const int Jn = (q2 * V.gy + q1) * V.gx + q0;
+            const int64_t Jo = (int64_t)Jn * 6;
             float av[36];
-#pragma unroll
-            for (int e = 0; e < 36; ++e) av[e] = __ldg(Ad + (int64_t)e * V.n);
+            lv_block(V.A, V.n, set, I, Jn, d, av);
 #pragma unroll
             for (int r = 0; r < RS; ++r) {
                 if (!on[r]) continue;
@@ -1421,7 +1442,7 @@ __global__ void k_lv_diag_inv(int n, int nset, const float* __restrict__ A, floa
     const int set = blockIdx.y;
     if (I >= n || set >= nset) return;
     double m[6][12];
-    const float* Ab = A + ((int64_t)set * ST + 13 * 36) * n + I;
+    const float* Ab = A + (int64_t)set * STS * n + I;  // direction 13, stored first
     for (int r = 0; r < 6; ++r)
         for (int c = 0; c < 6; ++c) {
             m[r][c] = (double)Ab[(int64_t)(r * 6 + c) * n];
@@ -1498,10 +1519,10 @@ __global__ void __launch_bounds__(256) k_galerkin(int gx, int gy, int gz, int cx
                                                   const float* __restrict__ A, const float* __restrict__ Q,
                                                   float* __restrict__ Ac)
 {
-    __shared__ double acc[ST];
+    __shared__ double acc[STS];  // the stored half: coarse directions dd = 13..26
     const int J = blockIdx.x, set = blockIdx.y;
     const int n = gx * gy * gz, nc = cx * cy * cz;
-    for (int e = threadIdx.x; e < ST; e += blockDim.x) acc[e] = 0.0;
+    for (int e = threadIdx.x; e < STS; e += blockDim.x) acc[e] = 0.0;
     __syncthreads();
     const int c[3] = {J % cx, (J / cx) % cy, J / (cx * cy)};
     const int g[3] = {gx, gy, gz}, nch[3] = {cx, cy, cz};
@@ -1516,10 +1537,9 @@ __global__ void __launch_bounds__(256) k_galerkin(int gx, int gy, int gz, int cx
         const int m = (mz * gy + my) * gx + mx, q = (nzq * gy + nyq) * gx + nxq;
         const int Jx = chunk_of(nxq, a, cx), Jy = chunk_of(nyq, a, cy), Jz = chunk_of(nzq, a, cz);
         const int dd = ((Jz - c[2] + 1) * 3 + Jy - c[1] + 1) * 3 + Jx - c[0] + 1;
-        const float* Ad = A + ((int64_t)set * ST + d * 36) * n + m;
+        if (dd < 13) continue;
         float Ab[36], Cq[36];
-#pragma unroll
-        for (int e = 0; e < 36; ++e) Ab[e] = __ldg(Ad + (int64_t)e * n);
+        lv_block(A, n, set, m, q, d, Ab);
         const float* Qm = Q + (int64_t)m * 36;
         const float* Qq = Q + (int64_t)q * 36;
 #pragma unroll
@@ -1539,12 +1559,12 @@ __global__ void __launch_bounds__(256) k_galerkin(int gx, int gy, int gz, int cx
                 float s = 0.f;
 #pragma unroll
                 for (int b = 0; b < 6; ++b) s += __ldg(Qm + b * 6 + r) * Cq[b * 6 + cc];
-                atomicAdd(&acc[dd * 36 + r * 6 + cc], (double)s);
+                atomicAdd(&acc[(dd - 13) * 36 + r * 6 + cc], (double)s);
             }
     }
     __syncthreads();
-    float* o = Ac + (int64_t)set * ST * nc + J;
-    for (int e = threadIdx.x; e < ST; e += blockDim.x) o[(int64_t)e * nc] = (float)acc[e];
+    float* o = Ac + (int64_t)set * STS * nc + J;
+    for (int e = threadIdx.x; e < STS; e += blockDim.x) o[(int64_t)e * nc] = (float)acc[e];
 }
 
 // Dense (ncp x ncp) matrix of the coarsest stencil (padding rows / columns: identity).
@@ -1563,9 +1583,10 @@ __global__ void k_dense_build(int gx, int gy, int gz, int ncp, const float* __re
     const int j0 = i0 + d % 3 - 1, j1 = i1 + (d / 3) % 3 - 1, j2 = i2 + d / 9 - 1;
     if (j0 < 0 || j0 >= gx || j1 < 0 || j1 >= gy || j2 < 0 || j2 >= gz) return;
     const int J = (j2 * gy + j1) * gx + j0;
-    const float* Ad = A + ((int64_t)set * ST + d * 36) * n + I;
+    float av[36];
+    lv_block(A, n, set, I, J, d, av);
     for (int r = 0; r < 6; ++r)
-        for (int c = 0; c < 6; ++c) Ds[(int64_t)(6 * I + r) * ncp + 6 * J + c] = (double)Ad[(int64_t)(r * 6 + c) * n];
+        for (int c = 0; c < 6; ++c) Ds[(int64_t)(6 * I + r) * ncp + 6 * J + c] = (double)av[r * 6 + c];
 }
 
 // D = (D + D^T) / 2 over the leading nc x nc block (as amg3d.py:568-569)
@@ -1893,7 +1914,7 @@ void carve_amg(lpm_amg& h, Carver2& c)
         for (int l = 0; l < b.nlev; ++l) {
             auto& Lv = b.lev[l];
             const size_t vn = (size_t)std::max(1, b.nsb) * Lv.n * 6;
-            Lv.A = c.take<float>((size_t)h.nset * ST * Lv.n);
+            Lv.A = c.take<float>((size_t)h.nset * STS * Lv.n);
             Lv.B = c.take<float>(vn);
             Lv.E = c.take<float>(vn);
             Lv.RB = c.take<float>(vn);
@@ -2216,7 +2237,8 @@ int amg_setup(lpm_amg& h, const float* Kn, const float* Tv, const float* Minv, c
             B.nch[ax] = b.nch[ax];
         }
         B.n1 = L1.n;
-        if ((e = cudaMemsetAsync(L1.A, 0, sizeof(float) * (size_t)h.nset * ST * L1.n, st)) != cudaSuccess) return (int)e;
+        if ((e = cudaMemsetAsync(L1.A, 0, sizeof(float) * (size_t)h.nset * STS * L1.n, st)) != cudaSuccess)
+            return (int)e;
         const int wm = box_wmax(b, h.o.agg);
         if (wm <= GD_WMAX) {
             // ---- level 1 directly from the bonds
@@ -2672,10 +2694,23 @@ int lpm_amg_get_level(const lpm_amg* h, int32_t box, int32_t set, int32_t level,
     const auto& Lv = b.lev[level - 1];
     cudaError_t e = cudaDeviceSynchronize();
     if (e == cudaSuccess && A_host) {
-        std::vector<float> t((size_t)ST * Lv.n);
-        e = cudaMemcpy(t.data(), Lv.A + (size_t)set * ST * Lv.n, sizeof(float) * t.size(), cudaMemcpyDeviceToHost);
-        for (int I = 0; I < Lv.n; ++I)
-            for (int q = 0; q < ST; ++q) A_host[(size_t)I * ST + q] = t[(size_t)q * Lv.n + I];
+        std::vector<float> t((size_t)STS * Lv.n);
+        e = cudaMemcpy(t.data(), Lv.A + (size_t)set * STS * Lv.n, sizeof(float) * t.size(), cudaMemcpyDeviceToHost);
+        // the full stencil (A_host: n x 27 x 6 x 6); directions whose neighbour lies off the grid stay zero
+        std::fill(A_host, A_host + (size_t)Lv.n * ST, 0.f);
+        for (int I = 0; I < Lv.n; ++I) {
+            const int i0 = I % Lv.g[0], i1 = (I / Lv.g[0]) % Lv.g[1], i2 = I / (Lv.g[0] * Lv.g[1]);
+            for (int d = 0; d < 27; ++d) {
+                const int j0 = i0 + d % 3 - 1, j1 = i1 + (d / 3) % 3 - 1, j2 = i2 + d / 9 - 1;
+                if (j0 < 0 || j0 >= Lv.g[0] || j1 < 0 || j1 >= Lv.g[1] || j2 < 0 || j2 >= Lv.g[2]) continue;
+                const int J = (j2 * Lv.g[1] + j1) * Lv.g[0] + j0;
+                for (int r = 0; r < 6; ++r)
+                    for (int c = 0; c < 6; ++c)
+                        A_host[(size_t)I * ST + d * 36 + r * 6 + c] =
+                            d >= 13 ? t[(size_t)((d - 13) * 36 + r * 6 + c) * Lv.n + I]
+                                    : t[(size_t)((13 - d) * 36 + c * 6 + r) * Lv.n + J];
+            }
+        }
     }
     if (e == cudaSuccess && rho_host) {
         if (level < b.nlev)
