@@ -729,7 +729,7 @@ def run_kernels(a):
     u64 = torch.randn(S * R, N, 3, device=dev, dtype=torch.float64)
     u1 = u64[:R].contiguous()
     lam = torch.randn(R, N, 3, device=dev, dtype=torch.float64)
-    row("a3", "SC K.u FP64 packed, 48^3 x 16 sets x 6", "k_sc_tma<double>",
+    row("a3", "SC K.u FP64 packed, 48^3 x 16 sets x 6", "k_sc_pair<double> (FP64 lean)",
         lambda: core.kmv(dl, u64, K64, T64, layout=L.LAYOUT_SOA, rhs_per_set=R), S * N * 288 + S * R * N * 48)
     row("a4", "SC K.u FP64 reference layout, 48^3 x 6", "k_shell_sums + k_apply",
         lambda: core.kmv(dl, u1, Kd[:1], Td[:1]), N * 288 + R * N * 48)
@@ -982,7 +982,7 @@ def main():
         del K64, T64, x64
         fp64_cg = {"solves_per_s": nsys / (ev0.elapsed_time(ev1) / 1e3), "iters_mean": float(i64.iters.mean()),
                    "all_converged": bool((i64.status == 0).all()),
-                   "path": "FP64 plain CG, packed coefficients, TMA-fed fused operator (k_sc_tma<double>)"}
+                   "path": "FP64 plain CG, packed coefficients, FP64 instantiation of the pair operator (k_sc_pair<double>, lean)"}
     M64 = core.block_jacobi(dl, Kn[0:1, 0], Tv[0:1, 0], torch.float64)
     xr, ir_ = core.cg(dl, Kn[0:1], Tv[0:1], b[0:1], Minv=M64, free=free, tol=1e-12, maxit=20000, check=1, poll=20)
     uref = ups[0:1] + xr

@@ -71,6 +71,13 @@ int kmv_impl(int dim, const lpm_lattice* lat, const T* u, const T* Kn, const T* 
             return ret(e);
         }
     }
+    if constexpr (sizeof(T) == 8) {
+        if (dim == 3 && !L.nbr && layout == LPM_LAYOUT_SOA && pair64_supported(L.nx) && tma_aligned(u, Kn, Tv)) {
+            // full SC box, packed FP64 coefficients: the FP64 instantiation of the pair operator (no scratch)
+            const PairArgs a = pair64_args(L.nx, L.ny, L.nz, L.N, bt.nsys, bt.rhs_per_set, u, Kn, Tv, out);
+            return ret(launch_sc_pair64(a, false, S(stream)));
+        }
+    }
     if (dim == 3 && !L.nbr && layout == LPM_LAYOUT_SOA && tma_supported(L.nx, (int)sizeof(T)) &&
         tma_aligned(u, Kn, Tv)) {
         // full SC box with packed coefficients: TMA-fed single-pass operator (needs no scratch)

@@ -567,7 +567,11 @@ int ir_solve(const Lattice& L, const double* Kn64, const double* Tv64, const Coe
     for (int k = 0;; ++k) {
         // true residual in FP64
         if (!x_zero) {
-            if (fused_ok(L, cl64, 8) && tma_aligned(x, Kn64, Tv64)) {  // packed FP64 coefficients: TMA operator
+            if (fused_ok(L, cl64, 8) && pair64_supported(L.nx) && tma_aligned(x, Kn64, Tv64)) {
+                // packed FP64 coefficients: the FP64 instantiation of the pair operator
+                const PairArgs a = pair64_args(L.nx, L.ny, L.nz, N, bt.nsys, bt.rhs_per_set, x, Kn64, Tv64, w.Kx);
+                e = launch_sc_pair64(a, false, st);
+            } else if (fused_ok(L, cl64, 8) && tma_aligned(x, Kn64, Tv64)) {  // packed FP64 coefficients: TMA operator
                 TmaArgs<double> a{};
                 a.nx = L.nx;
                 a.ny = L.ny;

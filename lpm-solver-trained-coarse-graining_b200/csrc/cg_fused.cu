@@ -584,6 +584,14 @@ bool use_pairs(const Lattice& L)
     return sizeof(T) == 4 && pair_supported(L.nx);
 }
 
+// FP64 systems on the FP64 instantiation of the pair operator (natural layout; p stays zero on fixed DOFs, so its
+// unmasked p.Ap is the masked one).
+template <typename T>
+bool use_pair64(const Lattice& L)
+{
+    return sizeof(T) == 8 && pair64_supported(L.nx);
+}
+
 template <typename T>
 void carve(Carve& c, const Lattice& L, int nsys, int rps, bool precond, FWork<T>& w)
 {
@@ -592,8 +600,8 @@ void carve(Carve& c, const Lattice& L, int nsys, int rps, bool precond, FWork<T>
     const bool paired = use_pairs<T>(L);
     const size_t nv = paired ? (size_t)nset * npp * L.N * 6 : (size_t)nsys * L.N * 3;
     const int nb = (int)((L.N + VB - 1) / VB);
-    const int dots = paired ? pair_dot_blocks_max(L.nx, L.ny, L.nz)
-                            : tma_dot_blocks_max(L.nx, L.ny, L.nz, (int)sizeof(T));
+    const int dots = (paired || use_pair64<T>(L)) ? pair_dot_blocks_max(L.nx, L.ny, L.nz)
+                                                  : tma_dot_blocks_max(L.nx, L.ny, L.nz, (int)sizeof(T));
     w.r = c.take<T>(nv);
     w.p = c.take<T>(nv);
     w.Ap = c.take<T>(nv);
@@ -619,7 +627,8 @@ void carve(Carve& c, const Lattice& L, int nsys, int rps, bool precond, FWork<T>
 // One operator launch: out = K u, with the alpha-step epilogue when epi.
 template <typename T>
 struct Operator {
-    bool paired;
+    bool paired;  // FP32 pair layout
+    bool p64;     // FP64 pair operator on natural-layout vectors
     TmaArgs<T> ta;
     PairArgs pa;
     cudaError_t run(const T* u, T* out, bool epi, int it, cudaStream_t st)
@@ -636,6 +645,19 @@ struct Operator {
                     a.has_sc = 0;
                 }
                 return launch_sc_pair(a, epi, st);
+            }
+        } else {
+            if (p64) {
+                PairArgs a = pa;
+                a.u = reinterpret_cast<const float*>(u);
+                a.out = reinterpret_cast<float*>(out);
+                a.it = it;
+                if (!epi) {
+                    a.act = nullptr;
+                    a.part = nullptr;
+                    a.has_sc = 0;
+                }
+                return launch_sc_pair64(a, epi, st);
             }
         }
         TmaArgs<T> a = ta;
@@ -735,7 +757,19 @@ int cg_solve_fused(const Lattice& L, const T* Kn, const T* Tv, const Batch& bt, 
 
     Operator<T> op{};
     op.paired = paired;
-    if (paired) {
+    op.p64 = use_pair64<T>(L);
+    if (op.p64) {
+        PairArgs& a = op.pa;
+        a = pair64_args(L.nx, L.ny, L.nz, N, bt.nsys, bt.rhs_per_set, reinterpret_cast<const double*>(x),
+                        reinterpret_cast<const double*>(Kn), reinterpret_cast<const double*>(Tv),
+                        reinterpret_cast<double*>(w.Ap));
+        a.act = w.sc.act;
+        a.part = w.mpart;
+        a.cnt = w.mcnt;
+        a.scv = w.sc;
+        a.has_sc = 1;
+        a.err = w.err;
+    } else if (paired) {
         PairArgs& a = op.pa;
         a.nx = L.nx;
         a.ny = L.ny;

@@ -53,6 +53,7 @@ using namespace ptx;
 
 constexpr int PX = 16, PY = 16, PNT = PX * PY;
 constexpr int PUW = 6 * (PX + 4);  // floats per u row: sites x0-2 .. x0+17, 3 components x 2 lanes
+constexpr int PUWE = 3 * (PX + 4); // u elements (8-byte lane groups: an FP32 pair or one FP64 value) per row
 constexpr int PUH = PY + 4;        // u rows y0-2 .. y0+17
 constexpr int PSW = PX + 2, PSH = PY + 2, PSPL = PSW * PSH;  // tile + 1-site ring
 constexpr int PTVW = 24;           // Tv sites per row (x0-4 .. x0+19)
@@ -67,7 +68,7 @@ static_assert(PNRING <= PRING_THREADS, "ring warps cover the ring");
 constexpr unsigned FULL18 = 0x3FFFFu;
 
 constexpr size_t PU_SLOT = (size_t)PUH * PUW * 4;
-constexpr size_t PTV_SLOT = (size_t)18 * PSH * PTVW * 4;
+constexpr size_t PTV_SLOT = (size_t)18 * PSH * PTVW * 4;  // FP32 coefficients; FP64 doubles it (tv_slot_bytes)
 constexpr size_t PKN_SLOT = (size_t)18 * PY * PKNW * 4;
 constexpr size_t PBA_SLOT = (size_t)2 * PSPL * 16;
 // Two variants share the kernel.  Staged (LEAN = false): Tv double-buffered and Kn staged by TMA, five u planes and
@@ -76,17 +77,69 @@ constexpr size_t PBA_SLOT = (size_t)2 * PSPL * 16;
 // read it, Kn of the own sites read from global memory in phase 1 and Tv of the own sites from global memory (L2) in
 // phase 2, four u and three (B, A) planes with two block barriers per step, 101 KB and at most 128 registers: two
 // CTAs (16 warps) per SM.
+//
+// FP64 (CT = double): the same kernel for one FP64 system per lane group ("pair" = one system), on natural-layout
+// vectors (nsys, N, 3), which are this layout with one lane.  Only the lean variant: the staged rings of doubled
+// coefficient planes would not fit (131 KB lean, one CTA per SM).
 __host__ __device__ constexpr int u_slots(bool lean) { return lean ? 4 : 5; }
 __host__ __device__ constexpr int ba_slots(bool lean) { return lean ? 3 : 4; }
 __host__ __device__ constexpr int tv_slots(bool lean) { return lean ? 1 : 2; }
+__host__ __device__ constexpr size_t tv_slot_bytes(int es) { return PTV_SLOT / 4 * es; }
+__host__ __device__ constexpr size_t kn_slot_bytes(int es) { return PKN_SLOT / 4 * es; }
 __host__ __device__ constexpr size_t off_tv(bool lean) { return u_slots(lean) * PU_SLOT; }
-__host__ __device__ constexpr size_t off_kn(bool lean) { return off_tv(lean) + tv_slots(lean) * PTV_SLOT; }
-__host__ __device__ constexpr size_t off_ba(bool lean) { return off_kn(lean) + (lean ? 0 : 2 * PKN_SLOT); }
-__host__ __device__ constexpr size_t pair_bytes(bool lean) { return off_ba(lean) + ba_slots(lean) * PBA_SLOT; }
+__host__ __device__ constexpr size_t off_kn(bool lean, int es = 4)
+{
+    return off_tv(lean) + tv_slots(lean) * tv_slot_bytes(es);
+}
+__host__ __device__ constexpr size_t off_ba(bool lean, int es = 4)
+{
+    return off_kn(lean, es) + (lean ? 0 : 2 * kn_slot_bytes(es));
+}
+__host__ __device__ constexpr size_t pair_bytes(bool lean, int es = 4)
+{
+    return off_ba(lean, es) + ba_slots(lean) * PBA_SLOT;
+}
 static_assert(PU_SLOT % 128 == 0 && PTV_SLOT % 128 == 0 && PKN_SLOT % 128 == 0 && PBA_SLOT % 128 == 0,
               "TMA destinations must stay 128-byte aligned");
 static_assert(pair_bytes(false) <= 227 * 1024, "shared memory budget");
 static_assert(2 * (pair_bytes(true) + 2048) <= 228 * 1024, "two lean CTAs per SM");
+static_assert(pair_bytes(true, 8) <= 227 * 1024, "FP64 lean shared memory budget");
+
+// Lane type of a coefficient type: FP32 -> a packed pair of two systems, FP64 -> one system.
+template <typename CT>
+struct PairLane;
+template <>
+struct PairLane<float> {
+    using V = pair_t;
+    using BA = float4;  // {B lane 0, B lane 1, A lane 0, A lane 1}
+    static constexpr int NL = 2;
+    static __device__ __forceinline__ BA make_ba(V b, V a)
+    {
+        float bl, bh, al, ah;
+        unpk(b, bl, bh);
+        unpk(a, al, ah);
+        return make_float4(bl, bh, al, ah);
+    }
+    static __device__ __forceinline__ V b_of(const BA& v) { return pk(v.x, v.y); }
+    static __device__ __forceinline__ V a_of(const BA& v) { return pk(v.z, v.w); }
+    static __device__ __forceinline__ BA zero_ba() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+    static __device__ __forceinline__ void lanes(V v, float& l0, float& l1) { unpk(v, l0, l1); }
+};
+template <>
+struct PairLane<double> {
+    using V = double;
+    using BA = double2;  // {B, A}
+    static constexpr int NL = 1;
+    static __device__ __forceinline__ BA make_ba(V b, V a) { return make_double2(b, a); }
+    static __device__ __forceinline__ V b_of(const BA& v) { return v.x; }
+    static __device__ __forceinline__ V a_of(const BA& v) { return v.y; }
+    static __device__ __forceinline__ BA zero_ba() { return make_double2(0.0, 0.0); }
+    static __device__ __forceinline__ void lanes(V v, double& l0, double& l1)
+    {
+        l0 = v;
+        l1 = 0.0;
+    }
+};
 
 __host__ __device__ constexpr unsigned dir_bits(int axis, int sgn)
 {
@@ -121,13 +174,19 @@ __host__ __device__ constexpr SlotGeo slot_geo(int k)
     return g;
 }
 
-__device__ __forceinline__ pair_t ld2(const float* p) { return *reinterpret_cast<const pair_t*>(p); }
 
-template <int MODE, bool LEAN>
-__global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
+template <int MODE, bool LEAN, typename CT = float>
+__global__ void __launch_bounds__(pair_threads(LEAN), (LEAN && sizeof(CT) == 4) ? 2 : 1)
     k_sc_pair(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ CUtensorMap tm_tv,
               const __grid_constant__ CUtensorMap tm_kn, PairArgs P)
 {
+    static_assert(sizeof(CT) == 4 || (LEAN && MODE <= PM_DOT), "FP64: lean variant, plain and dot epilogues only");
+    using LN = PairLane<CT>;
+    using V = typename LN::V;
+    using BA = typename LN::BA;
+    constexpr int NL = LN::NL;
+    constexpr int ES = (int)sizeof(CT);
+    constexpr V VZ = V(0);
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int NUS = u_slots(LEAN), NBAS = ba_slots(LEAN);
     constexpr int BTV = NUS, BKN = NUS + 2, NBAR = NUS + 4;  // mbarriers: u 0..NUS-1, Tv BTV.., Kn BKN..
@@ -136,10 +195,12 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
     __shared__ int abort_flag;  // set before the first block barrier only (shared-memory alignment check)
     __shared__ bool last_flag;
 
-    float* su = reinterpret_cast<float*>(smem);
-    float* stv = reinterpret_cast<float*>(smem + off_tv(LEAN));
-    float* skn = reinterpret_cast<float*>(smem + off_kn(LEAN));
-    float4* sba = reinterpret_cast<float4*>(smem + off_ba(LEAN));
+    V* su = reinterpret_cast<V*>(smem);  // u elements: (slot, PUH rows, PUWE)
+    CT* stv = reinterpret_cast<CT*>(smem + off_tv(LEAN));
+    CT* skn = reinterpret_cast<CT*>(smem + off_kn(LEAN, ES));
+    BA* sba = reinterpret_cast<BA*>(smem + off_ba(LEAN, ES));
+    constexpr size_t TVS = tv_slot_bytes(ES) / ES, KNS = kn_slot_bytes(ES) / ES;  // elements per Tv / Kn slot
+    constexpr size_t US = PU_SLOT / 8, BAS = PBA_SLOT / 16;                     // elements per u / (B, A) slot
 
     constexpr int NTH = pair_threads(LEAN);
     const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31;
@@ -149,13 +210,17 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
     const bool producer = tid == (LEAN ? 0 : NTH - 1);
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const int ntx = (nx + PX - 1) / PX, nty = (ny + PY - 1) / PY;
-    const int tile = blockIdx.x % (ntx * nty), zc = blockIdx.x / (ntx * nty);
+    // Grid: x = (pair of the set, column tile, z chunk) with the pair fastest, y = coefficient set.  The pairs of a set
+    // are adjacent in launch order, so they run together and the second and later pairs find the set's coefficient
+    // tiles in L2 (with the pairs far apart, a batch too large for L2 streams the coefficients once per pair).
+    const int jp = blockIdx.x % P.npp, tz = blockIdx.x / P.npp;  // tz: this CTA's block index within its system
+    const int tile = tz % (ntx * nty), zc = tz / (ntx * nty);
     const int x0 = (tile % ntx) * PX, y0 = (tile / ntx) * PY;
-    const int pr = blockIdx.y + P.pair0;
-    const int set = pr / P.npp, jp = pr % P.npp;
-    const int sbase = set * P.rhs_per_set + 2 * jp;
-    int nr = P.rhs_per_set - 2 * jp;
-    nr = nr < 2 ? nr : 2;
+    const int set = blockIdx.y + P.set0;
+    const int pr = set * P.npp + jp;
+    const int sbase = set * P.rhs_per_set + NL * jp;
+    int nr = P.rhs_per_set - NL * jp;
+    nr = nr < NL ? nr : NL;
     if (sbase + nr > P.nsys) nr = P.nsys - sbase;
     const int zbeg = zc * P.zchunk;
     const int zend = min(nz, zbeg + P.zchunk);
@@ -196,11 +261,10 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
         }
     }
     {
-        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int e = tid; e < NBAS * 2 * PSPL; e += NTH) sba[e] = z4;
+        for (int e = tid; e < NBAS * 2 * PSPL; e += NTH) sba[e] = LN::zero_ba();
         // u slots standing for planes below 0 are never loaded; keep them finite
         const int nneg = zbeg - 2 < 0 ? 2 - zbeg : 0;
-        for (int e = tid; e < nneg * (int)(PU_SLOT / 4); e += NTH) su[e] = 0.f;
+        for (int e = tid; e < nneg * (int)US; e += NTH) su[e] = VZ;
     }
     __syncthreads();
     if (abort_flag) any_on = false;
@@ -222,7 +286,7 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
             return;
         }
         mbar_expect_arrive(bar, (uint32_t)PU_SLOT);
-        tma_load4(su + (size_t)(n % NUS) * (PU_SLOT / 4), &tm_u, bar, 6 * (x0 - 2), y0 - 2, p, pr);
+        tma_load4(su + (size_t)(n % NUS) * US, &tm_u, bar, 3 * NL * (x0 - 2), y0 - 2, p, pr);
         note(n % NUS, (n / NUS) & 1);
     };
     // Tv fill n: slot n % tv_slots, barrier BTV + slot, parity (n / tv_slots) & 1
@@ -234,8 +298,8 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
             mbar_arrive(bar);
             return;
         }
-        mbar_expect_arrive(bar, (uint32_t)PTV_SLOT);
-        tma_load4(stv + (size_t)(n % NTV) * (PTV_SLOT / 4), &tm_tv, bar, x0 - 4, y0 - 1, p, 18 * set);
+        mbar_expect_arrive(bar, (uint32_t)tv_slot_bytes(ES));
+        tma_load4(stv + (size_t)(n % NTV) * TVS, &tm_tv, bar, x0 - 4, y0 - 1, p, 18 * set);
         note(BTV + n % NTV, (n / NTV) & 1);
     };
     auto issue_kn = [&](int p) {
@@ -245,8 +309,8 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
             mbar_arrive(bar);
             return;
         }
-        mbar_expect_arrive(bar, (uint32_t)PKN_SLOT);
-        tma_load4(skn + (size_t)(n & 1) * (PKN_SLOT / 4), &tm_kn, bar, x0, y0, p, 18 * set);
+        mbar_expect_arrive(bar, (uint32_t)kn_slot_bytes(ES));
+        tma_load4(skn + (size_t)(n & 1) * KNS, &tm_kn, bar, x0, y0, p, 18 * set);
         note(BKN + (n & 1), (n >> 1) & 1);
     };
     // Every thread waits (bounded) for the in-range fills it is about to read; an expired wait sets the thread's own
@@ -269,42 +333,42 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
             wait_fill(BKN + ((pkn - kn0) & 1), ((pkn - kn0) >> 1) & 1);
     };
 
-    auto u_slot = [&](int p) { return su + (size_t)((p - u0) % NUS) * (PU_SLOT / 4); };
-    auto tv_slot = [&](int p) { return stv + (size_t)((p - tv0) % NTV) * (PTV_SLOT / 4); };
-    auto kn_slot = [&](int p) { return skn + (size_t)((p - kn0) & 1) * (PKN_SLOT / 4); };
-    auto ba_slot = [&](int p) { return sba + (size_t)(((p % NBAS) + NBAS) % NBAS) * (PBA_SLOT / 16); };
+    auto u_slot = [&](int p) { return su + (size_t)((p - u0) % NUS) * US; };
+    auto tv_slot = [&](int p) { return stv + (size_t)((p - tv0) % NTV) * TVS; };
+    auto kn_slot = [&](int p) { return skn + (size_t)((p - kn0) & 1) * KNS; };
+    auto ba_slot = [&](int p) { return sba + (size_t)(((p % NBAS) + NBAS) % NBAS) * BAS; };
 
     // ---------------------------------------------------------------------------------------------- phase 1
     // Shell sums of the site (qx, qy) (ring coordinates, 0 = x0-1 / y0-1) of plane zp for both lanes, stored as
     // (B, A); with OWN also the own terms.  Slot loop fully unrolled; signs are compile-time, so every accumulation is
     // an add or FMA into a "plus" or "minus" accumulator.  Diagonal slots use d' = o.(u_q - u_i) unscaled.
-    pair_t own_next[3] = {0ull, 0ull, 0ull};
-    float tv_next[18];
+    V own_next[3] = {VZ, VZ, VZ};
+    CT tv_next[18];
 #pragma unroll
-    for (int k = 0; k < 18; ++k) tv_next[k] = 0.f;
+    for (int k = 0; k < 18; ++k) tv_next[k] = CT(0);
 
     // pm, p0, pp: the u slots of planes zp-1, zp, zp+1; bsl: the (B, A) slot of plane zp.
-    auto site = [&](auto own_tag, auto mask_tag, int qx, int qy, const float* pm, const float* p0, const float* pp,
-                    float4* bsl, unsigned vm, const float* tvs, const float* kns, int64_t kst) {
+    auto site = [&](auto own_tag, auto mask_tag, int qx, int qy, const V* pm, const V* p0, const V* pp, BA* bsl,
+                    unsigned vm, const CT* tvs, const CT* kns, int64_t kst) {
         constexpr bool OWN = decltype(own_tag)::value;
         constexpr bool MASKED = decltype(mask_tag)::value;
-        const int ci = (qy + 1) * PUW + 6 * (qx + 1);
-        const pair_t ui[3] = {ld2(p0 + ci), ld2(p0 + ci + 2), ld2(p0 + ci + 4)};
-        const pair_t cpl[3] = {add2(ui[0], ui[1]), add2(ui[0], ui[2]), add2(ui[1], ui[2])};
-        const pair_t cmi[3] = {sub2(ui[0], ui[1]), sub2(ui[0], ui[2]), sub2(ui[1], ui[2])};
-        pair_t Sp0 = 0ull, Sm0 = 0ull, Sp1 = 0ull, Sm1 = 0ull, Tp0 = 0ull, Tm0 = 0ull, Tp1 = 0ull, Tm1 = 0ull;
-        pair_t fp[3] = {0ull, 0ull, 0ull}, fm[3] = {0ull, 0ull, 0ull};
-        float s0[3] = {0.f, 0.f, 0.f}, s1[3] = {0.f, 0.f, 0.f}, T0[3] = {0.f, 0.f, 0.f}, T1[3] = {0.f, 0.f, 0.f};
+        const int ci = (qy + 1) * PUWE + 3 * (qx + 1);
+        const V ui[3] = {p0[ci], p0[ci + 1], p0[ci + 2]};
+        const V cpl[3] = {add2(ui[0], ui[1]), add2(ui[0], ui[2]), add2(ui[1], ui[2])};
+        const V cmi[3] = {sub2(ui[0], ui[1]), sub2(ui[0], ui[2]), sub2(ui[1], ui[2])};
+        V Sp0 = VZ, Sm0 = VZ, Sp1 = VZ, Sm1 = VZ, Tp0 = VZ, Tm0 = VZ, Tp1 = VZ, Tm1 = VZ;
+        V fp[3] = {VZ, VZ, VZ}, fm[3] = {VZ, VZ, VZ};
+        CT s0[3] = {0, 0, 0}, s1[3] = {0, 0, 0}, T0[3] = {0, 0, 0}, T1[3] = {0, 0, 0};
 #pragma unroll
         for (int k = 0; k < 18; ++k) {
             const SlotGeo g = slot_geo(k);
-            const float* pl = sc_dz(k) < 0 ? pm : (sc_dz(k) > 0 ? pp : p0);
-            const int qo = ci + sc_dy(k) * PUW + 6 * sc_dx(k);
-            const float tv = tvs[k * PSH * PTVW];
+            const V* pl = sc_dz(k) < 0 ? pm : (sc_dz(k) > 0 ? pp : p0);
+            const int qo = ci + sc_dy(k) * PUWE + 3 * sc_dx(k);
+            const CT tv = tvs[k * PSH * PTVW];
             const bool vb = !MASKED || ((vm >> k) & 1u);
             if (sc_shell(k) == 0) {
-                pair_t t = sub2(ld2(pl + qo + 2 * g.a), ui[g.a]);  // u_q,a - u_i,a ; dL = sa t
-                if (MASKED && !vb) t = 0ull;
+                V t = sub2(pl[qo + g.a], ui[g.a]);  // u_q,a - u_i,a ; dL = sa t
+                if (MASKED && !vb) t = VZ;
                 if (g.sa > 0) {
                     Sp0 = add2(Sp0, t);
                     Tp0 = fma2(dup(tv), t, Tp0);
@@ -313,18 +377,18 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
                     Tm0 = fma2(dup(tv), t, Tm0);
                 }
                 if constexpr (OWN) {
-                    const float kn = LEAN ? __ldg(kns + k * kst) : kns[k * kst];
-                    fm[g.a] = fma2(dup(2.f * kn), t, fm[g.a]);  // f_a -= 2 Kn t
+                    const CT kn = LEAN ? __ldg(kns + k * kst) : kns[k * kst];
+                    fm[g.a] = fma2(dup(CT(2) * kn), t, fm[g.a]);  // f_a -= 2 Kn t
                     if (vb) {
-                        s0[g.a] -= (float)g.sa;
-                        T0[g.a] -= (float)g.sa * tv;
+                        s0[g.a] -= (CT)g.sa;
+                        T0[g.a] -= (CT)g.sa * tv;
                     }
                 }
             } else {
-                const pair_t qa = ld2(pl + qo + 2 * g.a), qb = ld2(pl + qo + 2 * g.b);
+                const V qa = pl[qo + g.a], qb = pl[qo + g.b];
                 // d' = sa t with t = (u_q,a +- u_q,b) - (u_i,a +- u_i,b)
-                pair_t t = g.sa == g.sb ? sub2(add2(qa, qb), cpl[g.plane]) : sub2(sub2(qa, qb), cmi[g.plane]);
-                if (MASKED && !vb) t = 0ull;
+                V t = g.sa == g.sb ? sub2(add2(qa, qb), cpl[g.plane]) : sub2(sub2(qa, qb), cmi[g.plane]);
+                if (MASKED && !vb) t = VZ;
                 if (g.sa > 0) {
                     Sp1 = add2(Sp1, t);
                     Tp1 = fma2(dup(tv), t, Tp1);
@@ -333,39 +397,34 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
                     Tm1 = fma2(dup(tv), t, Tm1);
                 }
                 if constexpr (OWN) {
-                    const float kn = LEAN ? __ldg(kns + k * kst) : kns[k * kst];
-                    const pair_t kn2 = dup(kn);
+                    const CT kn = LEAN ? __ldg(kns + k * kst) : kns[k * kst];
+                    const V kn2 = dup(kn);
                     fm[g.a] = fma2(kn2, t, fm[g.a]);  // f_a -= sa Kn d' = Kn t
                     if (g.sa == g.sb)
                         fm[g.b] = fma2(kn2, t, fm[g.b]);
                     else
                         fp[g.b] = fma2(kn2, t, fp[g.b]);
                     if (vb) {
-                        s1[g.a] -= (float)g.sa;
-                        s1[g.b] -= (float)g.sb;
-                        T1[g.a] -= (float)g.sa * tv;
-                        T1[g.b] -= (float)g.sb * tv;
+                        s1[g.a] -= (CT)g.sa;
+                        s1[g.b] -= (CT)g.sb;
+                        T1[g.a] -= (CT)g.sa * tv;
+                        T1[g.b] -= (CT)g.sb * tv;
                     }
                 }
             }
             if constexpr (OWN && !LEAN) tv_next[k] = tv;
         }
         // B0 = S0/2, A0 = TS0/2; shell 1 pre-scaled by 1/sqrt2: B1w = S1'/4, A1w = TS1'/4
-        const pair_t h = dup(0.5f), q = dup(0.25f);
-        const pair_t B0 = mul2(h, sub2(Sp0, Sm0)), A0 = mul2(h, sub2(Tp0, Tm0));
-        const pair_t B1 = mul2(q, sub2(Sp1, Sm1)), A1 = mul2(q, sub2(Tp1, Tm1));
-        float4* dst = bsl + qy * PSW + qx;
-        float b0l, b0h, a0l, a0h, b1l, b1h, a1l, a1h;
-        unpk(B0, b0l, b0h);
-        unpk(A0, a0l, a0h);
-        unpk(B1, b1l, b1h);
-        unpk(A1, a1l, a1h);
-        dst[0] = make_float4(b0l, b0h, a0l, a0h);
-        dst[PSPL] = make_float4(b1l, b1h, a1l, a1h);
+        const V h = dup(CT(0.5)), q = dup(CT(0.25));
+        const V B0 = mul2(h, sub2(Sp0, Sm0)), A0 = mul2(h, sub2(Tp0, Tm0));
+        const V B1 = mul2(q, sub2(Sp1, Sm1)), A1 = mul2(q, sub2(Tp1, Tm1));
+        BA* dst = bsl + qy * PSW + qx;
+        dst[0] = LN::make_ba(B0, A0);
+        dst[PSPL] = LN::make_ba(B1, A1);
         if constexpr (OWN) {
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-                pair_t o = sub2(fp[a], fm[a]);
+                V o = sub2(fp[a], fm[a]);
                 o = fma2(B0, dup(T0[a]), o);
                 o = fma2(B1, dup(T1[a]), o);
                 if constexpr (MASKED) {  // s_c vanishes for a site with all bonds
@@ -421,23 +480,23 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
     using F_ = std::false_type;
     // Phase 1 of plane zp: pm, p0, pp are its u slots (planes zp-1, zp, zp+1), tvsl / knsl its Tv / Kn slots and bsl
     // its (B, A) slot.
-    auto phase1 = [&](int zp, bool own, const float* pm, const float* p0, const float* pp, const float* tvsl,
-                      const float* knsl, float4* bsl) {
+    auto phase1 = [&](int zp, bool own, const V* pm, const V* p0, const V* pp, const CT* tvsl, const CT* knsl,
+                      BA* bsl) {
         if (zp < 0 || zp >= nz) {
-            const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-            for (int e = tid; e < 2 * PSPL; e += NTH) bsl[e] = z4;
+            for (int e = tid; e < 2 * PSPL; e += NTH) bsl[e] = LN::zero_ba();
             return;
         }
         const unsigned zm = z_mask(zp);
         const unsigned vm = own_mxy & zm;
         const bool uni = __all_sync(0xffffffffu, !own_xy || vm == FULL18);
         if (own_xy) {
-            const float* tvs = tvsl + (ty + 1) * PTVW + tx + 4;
+            const CT* tvs = tvsl + (ty + 1) * PTVW + tx + 4;
             if (own) {
-                const float* kns;
+                const CT* kns;
                 int64_t kst;
                 if constexpr (LEAN) {
-                    kns = P.Kn + (int64_t)18 * set * P.N + ((int64_t)zp * ny + gy) * nx + gx;
+                    kns = reinterpret_cast<const CT*>(P.Kn) + (int64_t)18 * set * P.N + ((int64_t)zp * ny + gy) * nx +
+                          gx;
                     kst = P.N;
                 } else {
                     kns = knsl + ty * PKNW + tx;
@@ -457,7 +516,7 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
         const unsigned rvm = ring_mxy & zm;
         const bool runi = __all_sync(0xffffffffu, !ring_in || rvm == FULL18);
         if (ring_in) {
-            const float* tvs = tvsl + rqy * PTVW + rqx + 3;
+            const CT* tvs = tvsl + rqy * PTVW + rqx + 3;
             if (runi)
                 site(F_{}, F_{}, rqx, rqy, pm, p0, pp, bsl, rvm, tvs, nullptr, 0);
             else
@@ -466,38 +525,38 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
     };
 
     // ---------------------------------------------------------------------------------------------- phase 2
-    pair_t own_cur[3] = {0ull, 0ull, 0ull};
-    float tv_cur[18];
-    pair_t dotp = 0ull;
+    V own_cur[3] = {VZ, VZ, VZ};
+    CT tv_cur[18];
+    V dotp = VZ;
     // Phase 2 of plane z: bm, b0, bp are the (B, A) slots of planes z-1, z, z+1 and uz the u slot of plane z.
-    auto phase2 = [&](int z, const float4* bm, const float4* b0, const float4* bp, const float* uz) {
+    auto phase2 = [&](int z, const BA* bm, const BA* b0, const BA* bp, const V* uz) {
         if (!own_xy) return;
         const int64_t i = ((int64_t)z * ny + gy) * nx + gx;
         const int c0 = (ty + 1) * PSW + (tx + 1);
-        pair_t f[3] = {own_cur[0], own_cur[1], own_cur[2]};
-        const float* tvg = P.Tv + (int64_t)18 * set * P.N + i;
+        V f[3] = {own_cur[0], own_cur[1], own_cur[2]};
+        const CT* tvg = reinterpret_cast<const CT*>(P.Tv) + (int64_t)18 * set * P.N + i;
 #pragma unroll
         for (int k = 0; k < 18; ++k) {
             const SlotGeo g = slot_geo(k);
-            const float4* pl = sc_dz(k) < 0 ? bm : (sc_dz(k) > 0 ? bp : b0);
-            const float4 v = pl[sc_shell(k) * PSPL + c0 + sc_dy(k) * PSW + sc_dx(k)];
-            const float tvk = LEAN ? __ldg(tvg + (int64_t)k * P.N) : tv_cur[k];
-            const pair_t gw = fma2(dup(tvk), pk(v.x, v.y), pk(v.z, v.w));  // zero for bonds leaving the box
+            const BA* pl = sc_dz(k) < 0 ? bm : (sc_dz(k) > 0 ? bp : b0);
+            const BA v = pl[sc_shell(k) * PSPL + c0 + sc_dy(k) * PSW + sc_dx(k)];
+            const CT tvk = LEAN ? __ldg(tvg + (int64_t)k * P.N) : tv_cur[k];
+            const V gw = fma2(dup(tvk), LN::b_of(v), LN::a_of(v));  // zero for bonds leaving the box
             f[g.a] = g.sa > 0 ? sub2(f[g.a], gw) : add2(f[g.a], gw);
             if (sc_shell(k) == 1) f[g.b] = g.sb > 0 ? sub2(f[g.b], gw) : add2(f[g.b], gw);
         }
-        pair_t* o = reinterpret_cast<pair_t*>(P.out + (((int64_t)pr * P.N + i) * 3) * 2);
+        V* o = reinterpret_cast<V*>(P.out) + ((int64_t)pr * P.N + i) * 3;
         if constexpr (MODE <= PM_DOT) {
             o[0] = f[0];
             o[1] = f[1];
             o[2] = f[2];
             if constexpr (EPI) {
-                const float* pu = uz + (ty + 2) * PUW + 6 * (tx + 2);
-                dotp = fma2(ld2(pu), f[0], dotp);
-                dotp = fma2(ld2(pu + 2), f[1], dotp);
-                dotp = fma2(ld2(pu + 4), f[2], dotp);
+                const V* pu = uz + (ty + 2) * PUWE + 3 * (tx + 2);
+                dotp = fma2(pu[0], f[0], dotp);
+                dotp = fma2(pu[1], f[1], dotp);
+                dotp = fma2(pu[2], f[2], dotp);
             }
-        } else {
+        } else if constexpr (NL == 2) {
             const bool in0 = gx >= bl0[0] && gx <= bh0[0] && gy >= bl0[1] && gy <= bh0[1] && z >= bl0[2] &&
                              z <= bh0[2];
             const bool in1 = gx >= bl1[0] && gx <= bh1[0] && gy >= bl1[1] && gy <= bh1[1] && z >= bl1[2] &&
@@ -514,13 +573,13 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
                 float m9[9];
 #pragma unroll
                 for (int e = 0; e < 9; ++e) m9[e] = __ldg(ms + (int64_t)e * P.N);
-                const float* pu = uz + (ty + 2) * PUW + 6 * (tx + 2);
+                const V* pu = uz + (ty + 2) * PUWE + 3 * (tx + 2);
                 const float c0 = in0 ? w0 : 0.f, c1 = in1 ? w1 : 0.f;
 #pragma unroll
                 for (int a = 0; a < 3; ++a) {
                     const float z0 = m9[3 * a] * t0[0] + m9[3 * a + 1] * t0[1] + m9[3 * a + 2] * t0[2];
                     const float z1 = m9[3 * a] * t1[0] + m9[3 * a + 1] * t1[1] + m9[3 * a + 2] * t1[2];
-                    const pair_t v = fma2(pk(c0, c1), pk(z0, z1), ld2(pu + 2 * a));
+                    const pair_t v = fma2(pk(c0, c1), pk(z0, z1), pu[a]);
                     o[a] = v;
                     if constexpr (EPI) dotp = fma2(rh[a], v, dotp);
                 }
@@ -582,7 +641,7 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
                 const int ib0 = wrapb(ib + 1), ib1 = wrapb(ib0 + 1);
                 const int itv = NTV == 2 ? (s & 1) : 0, ptv = NTV == 2 ? (((s + 2) >> 1) & 1) : (s & 1);
                 const int ikn = (s + 1) & 1, pkn = ((s + 1) >> 1) & 1;
-                const float* uz = su + (size_t)iu0 * (PU_SLOT / 4);
+                const V* uz = su + (size_t)iu0 * US;
 #pragma unroll
                 for (int a = 0; a < 3; ++a) own_cur[a] = own_next[a];
                 if constexpr (!LEAN) {
@@ -600,9 +659,8 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
                 if (z + 2 < nz) wait_fill(iu2, pu2);
                 if (z + 1 < nz) wait_fill(BTV + itv, ptv);
                 if (!LEAN && z + 1 < zend) wait_fill(BKN + ikn, pkn);
-                phase1(z + 1, z + 1 < zend, uz, su + (size_t)iu1 * (PU_SLOT / 4), su + (size_t)iu2 * (PU_SLOT / 4),
-                       stv + (size_t)itv * (PTV_SLOT / 4), skn + (size_t)ikn * (PKN_SLOT / 4),
-                       sba + (size_t)ib1 * (PBA_SLOT / 16));
+                phase1(z + 1, z + 1 < zend, uz, su + (size_t)iu1 * US, su + (size_t)iu2 * US, stv + (size_t)itv * TVS,
+                       skn + (size_t)ikn * KNS, sba + (size_t)ib1 * BAS);
                 if (__syncthreads_or(lost)) {  // uniform: every thread leaves the loop at this barrier
                     ok = false;
                     break;
@@ -611,8 +669,7 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
                     fence_proxy_async();
                     if (z + 2 <= zend) issue_tv(z + 2);
                 }
-                phase2(z, sba + (size_t)ib * (PBA_SLOT / 16), sba + (size_t)ib0 * (PBA_SLOT / 16),
-                       sba + (size_t)ib1 * (PBA_SLOT / 16), uz);
+                phase2(z, sba + (size_t)ib * BAS, sba + (size_t)ib0 * BAS, sba + (size_t)ib1 * BAS, uz);
                 // Lean: the next step's Tv fill and phase 1 reuse buffers phase 2 may still read.  Staged: the next
                 // step's fills go to the u slot of plane z - 1 and phase 1 writes the (B, A) slot of plane z + 2,
                 // neither of which this phase 2 reads, and every warp has left phase 2 of plane z - 1 before any
@@ -631,14 +688,14 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
 
     if constexpr (EPI) {
         if (!P.part) return;
-        float d0, d1;
-        unpk(dotp, d0, d1);
-        const int nblk = gridDim.x;
+        CT d0, d1;
+        LN::lanes(dotp, d0, d1);
+        const int nblk = gridDim.x / P.npp;  // CTAs per system
         for (int j = 0; j < nr; ++j) {
             const int s = sbase + j;
             const double v = block_sum(ok ? (double)(j == 0 ? d0 : d1) : 0.0, red);
             if (tid == 0) {
-                P.part[(int64_t)s * nblk + blockIdx.x] = v;
+                P.part[(int64_t)s * nblk + tz] = v;
                 __threadfence();
                 last_flag = atomicAdd(P.cnt + s, 1u) == (unsigned)(nblk - 1);
             }
@@ -663,7 +720,7 @@ __global__ void __launch_bounds__(pair_threads(LEAN), LEAN ? 2 : 1)
 }
 
 // Opt-in to the kernel's dynamic shared memory, once per device (outside any stream capture: pair_prepare).
-template <int MODE, bool LEAN>
+template <int MODE, bool LEAN, typename CT = float>
 cudaError_t pair_attr()
 {
     static unsigned long long attr_set = 0;
@@ -671,47 +728,54 @@ cudaError_t pair_attr()
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if (!((attr_set >> dev) & 1ull)) {
-        cudaError_t e = cudaFuncSetAttribute(k_sc_pair<MODE, LEAN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)pair_bytes(LEAN));
+        cudaError_t e = cudaFuncSetAttribute(k_sc_pair<MODE, LEAN, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)pair_bytes(LEAN, (int)sizeof(CT)));
         if (e != cudaSuccess) return e;
         attr_set |= 1ull << dev;
     }
     return cudaSuccess;
 }
 
-template <int MODE, bool LEAN>
+// CT = float: u and out in the pair layout (npair, N, 3, 2); CT = double: natural layout (nsys, N, 3), the FP64
+// arrays passed through the float pointers of PairArgs (u, out, Kn, Tv).
+template <int MODE, bool LEAN, typename CT = float>
 cudaError_t launch_pair(const PairArgs& a, cudaStream_t st)
 {
+    constexpr int ES = (int)sizeof(CT), NL = PairLane<CT>::NL;
     const int nset = (a.nsys + a.rhs_per_set - 1) / a.rhs_per_set;
     CUtensorMap mu, mtv, mkn;
     {
-        const uint64_t dims[4] = {(uint64_t)6 * a.nx, (uint64_t)a.ny, (uint64_t)a.nz, (uint64_t)a.npair};
-        const uint64_t str[3] = {(uint64_t)6 * a.nx * 4, (uint64_t)6 * a.nx * a.ny * 4,
-                                 (uint64_t)6 * a.nx * a.ny * a.nz * 4};
-        const uint32_t box[4] = {(uint32_t)PUW, (uint32_t)PUH, 1, 1};
-        if (!make_tensor_map4(&mu, 4, a.u, dims, str, box)) return cudaErrorInvalidValue;
+        // u rows of 3 * NL elements per site; FP64: the systems themselves (a trailing partial set reads zeros)
+        const uint64_t nu = NL == 2 ? (uint64_t)a.npair : (uint64_t)a.nsys;
+        const uint64_t dims[4] = {(uint64_t)3 * NL * a.nx, (uint64_t)a.ny, (uint64_t)a.nz, nu};
+        const uint64_t str[3] = {(uint64_t)3 * NL * a.nx * ES, (uint64_t)3 * NL * a.nx * a.ny * ES,
+                                 (uint64_t)3 * NL * a.nx * a.ny * a.nz * ES};
+        const uint32_t box[4] = {(uint32_t)(3 * NL * (PX + 4)), (uint32_t)PUH, 1, 1};
+        if (!make_tensor_map4(&mu, ES, a.u, dims, str, box)) return cudaErrorInvalidValue;
     }
     {
         const uint64_t dims[4] = {(uint64_t)a.nx, (uint64_t)a.ny, (uint64_t)a.nz, (uint64_t)18 * nset};
-        const uint64_t str[3] = {(uint64_t)a.nx * 4, (uint64_t)a.nx * a.ny * 4, (uint64_t)a.nx * a.ny * a.nz * 4};
+        const uint64_t str[3] = {(uint64_t)a.nx * ES, (uint64_t)a.nx * a.ny * ES, (uint64_t)a.nx * a.ny * a.nz * ES};
         const uint32_t btv[4] = {(uint32_t)PTVW, (uint32_t)PSH, 1, 18};
         const uint32_t bkn[4] = {(uint32_t)PKNW, (uint32_t)PY, 1, 18};
-        if (!make_tensor_map4(&mtv, 4, a.Tv, dims, str, btv)) return cudaErrorInvalidValue;
+        if (!make_tensor_map4(&mtv, ES, a.Tv, dims, str, btv)) return cudaErrorInvalidValue;
         if (LEAN)
             mkn = mtv;  // not read by the lean variant
-        else if (!make_tensor_map4(&mkn, 4, a.Kn, dims, str, bkn))
+        else if (!make_tensor_map4(&mkn, ES, a.Kn, dims, str, bkn))
             return cudaErrorInvalidValue;
     }
-    cudaError_t e = pair_attr<MODE, LEAN>();
+    cudaError_t e = pair_attr<MODE, LEAN, CT>();
     if (e != cudaSuccess) return e;
     const int ntile = ((a.nx + PX - 1) / PX) * ((a.ny + PY - 1) / PY);
     const int nzc = (a.nz + a.zchunk - 1) / a.zchunk;
-    for (int g0 = 0; g0 < a.npair; g0 += 65535) {
+    if (a.npair != nset * a.npp || (int64_t)a.npp * ntile * nzc > 0x7FFFFFFF) return cudaErrorInvalidValue;
+    for (int s0 = 0; s0 < nset; s0 += 65535) {
         PairArgs b = a;
-        b.pair0 = g0;
+        b.set0 = s0;
         b.wait_polls = tma_wait_polls();
-        const int ng = a.npair - g0 < 65535 ? a.npair - g0 : 65535;
-        k_sc_pair<MODE, LEAN><<<dim3(ntile * nzc, ng), pair_threads(LEAN), pair_bytes(LEAN), st>>>(mu, mtv, mkn, b);
+        const int ns = nset - s0 < 65535 ? nset - s0 : 65535;
+        k_sc_pair<MODE, LEAN, CT><<<dim3(a.npp * ntile * nzc, ns), pair_threads(LEAN), pair_bytes(LEAN, ES), st>>>(
+            mu, mtv, mkn, b);
     }
     return cudaGetLastError();
 }
@@ -845,12 +909,43 @@ cudaError_t pair_prepare()
     if (e == cudaSuccess) e = pair_attr<PM_SMOOTH, true>();
     if (e == cudaSuccess) e = pair_attr<PM_SMOOTH_DOT, false>();
     if (e == cudaSuccess) e = pair_attr<PM_SMOOTH_DOT, true>();
+    if (e == cudaSuccess) e = pair_attr<PM_NONE, true, double>();
+    if (e == cudaSuccess) e = pair_attr<PM_DOT, true, double>();
     return e;
 }
 
 cudaError_t launch_sc_pair(const PairArgs& a, bool epi, cudaStream_t st)
 {
     return launch_sc_pair_mode(a, epi ? PM_DOT : PM_NONE, st);
+}
+
+bool pair64_supported(int nx) { return nx % 2 == 0 && tma_supported(nx, 8); }
+
+PairArgs pair64_args(int nx, int ny, int nz, int64_t N, int nsys, int rps, const double* u, const double* Kn,
+                     const double* Tv, double* out)
+{
+    PairArgs a{};
+    a.nx = nx;
+    a.ny = ny;
+    a.nz = nz;
+    a.N = N;
+    a.nsys = nsys;
+    a.rhs_per_set = rps;
+    a.npp = rps;
+    a.npair = (nsys + rps - 1) / rps * rps;
+    a.zchunk = pair_zchunk_heuristic(nx, ny, nz, a.npair);
+    a.variant = 1;
+    a.u = reinterpret_cast<const float*>(u);
+    a.Kn = reinterpret_cast<const float*>(Kn);
+    a.Tv = reinterpret_cast<const float*>(Tv);
+    a.out = reinterpret_cast<float*>(out);
+    return a;
+}
+
+cudaError_t launch_sc_pair64(const PairArgs& a, bool epi, cudaStream_t st)
+{
+    if (a.npair < 1 || a.npp != a.rhs_per_set || a.zchunk < 1) return cudaErrorInvalidValue;
+    return epi ? launch_pair<PM_DOT, true, double>(a, st) : launch_pair<PM_NONE, true, double>(a, st);
 }
 
 }  // namespace lpm

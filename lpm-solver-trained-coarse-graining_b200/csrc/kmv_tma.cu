@@ -114,10 +114,12 @@ __global__ void __launch_bounds__(TX*(TY + RY), 1)
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const int ntx = (nx + TX - 1) / TX, nty = (ny + TY - 1) / TY;
-    const int tile = blockIdx.x % (ntx * nty), zc = blockIdx.x / (ntx * nty);
+    // Grid: x = (system group of the set, column tile, z chunk) with the group fastest, y = coefficient set: the groups
+    // of a set run together and share the set's coefficient tiles through L2.
+    const int g = blockIdx.x % P.ngrp, tz = blockIdx.x / P.ngrp;  // tz: this CTA's block index within its systems
+    const int tile = tz % (ntx * nty), zc = tz / (ntx * nty);
     const int x0 = (tile % ntx) * TX, y0 = (tile / ntx) * TY;
-    const int grp = blockIdx.y + P.grp0;
-    const int set = grp / P.ngrp, g = grp % P.ngrp;
+    const int set = blockIdx.y + P.set0;
     const int sbase = set * P.rhs_per_set + g * NR;
     int nr = P.rhs_per_set - g * NR;
     nr = nr < NR ? nr : NR;
@@ -521,14 +523,14 @@ __global__ void __launch_bounds__(TX*(TY + RY), 1)
 
     if constexpr (EPI) {
         if (!P.part) return;
-        const int nblk = gridDim.x;
+        const int nblk = gridDim.x / P.ngrp;  // CTAs per system
 #pragma unroll
         for (int j = 0; j < NR; ++j) {
             if (j >= nr) break;
             const int s = sbase + j;
             const double v = block_sum(ok ? dot[j] : 0.0, red);
             if (tid == 0) {
-                P.part[(int64_t)s * nblk + blockIdx.x] = v;
+                P.part[(int64_t)s * nblk + tz] = v;
                 __threadfence();
                 last_flag = atomicAdd(P.cnt + s, 1u) == (unsigned)(nblk - 1);
             }
@@ -588,12 +590,14 @@ cudaError_t launch_one(const TmaArgs<T>& a, int ngt, int nzc, cudaStream_t st)
         attr_set |= 1ull << dev;
     }
     const int ntile = ((a.nx + TX - 1) / TX) * ((a.ny + TY - 1) / TY);
-    for (int g0 = 0; g0 < ngt; g0 += 65535) {
+    if (ngt != nset * a.ngrp || (int64_t)a.ngrp * ntile * nzc > 0x7FFFFFFF) return cudaErrorInvalidValue;
+    for (int s0 = 0; s0 < nset; s0 += 65535) {
         TmaArgs<T> b = a;
         b.wait_polls = tma_wait_polls();
-        b.grp0 = g0;
-        const int ng = ngt - g0 < 65535 ? ngt - g0 : 65535;
-        k_sc_tma<T, NR, TY, EPI><<<dim3(ntile * nzc, ng), dim3(TX, TY + RY), Lay::BYTES, st>>>(mu, mtv, mkn, b);
+        b.set0 = s0;
+        const int ns = nset - s0 < 65535 ? nset - s0 : 65535;
+        k_sc_tma<T, NR, TY, EPI><<<dim3(a.ngrp * ntile * nzc, ns), dim3(TX, TY + RY), Lay::BYTES, st>>>(mu, mtv, mkn,
+                                                                                                        b);
     }
     return cudaGetLastError();
 }

@@ -100,5 +100,13 @@ __device__ __forceinline__ pair_t fma2(pair_t a, pair_t b, pair_t c)
     return d;
 }
 
+// One FP64 system in place of a pair (the FP64 instantiation of the pair operator): the same names, scalar
+// round-to-nearest arithmetic without contraction, as the packed instructions.
+__device__ __forceinline__ double dup(double a) { return a; }
+__device__ __forceinline__ double add2(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub2(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double mul2(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double fma2(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 }  // namespace ptx
 }  // namespace lpm

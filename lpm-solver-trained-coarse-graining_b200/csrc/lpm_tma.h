@@ -13,7 +13,7 @@ struct TmaArgs {
     int nsys, rhs_per_set, nmask;
     int nr;      // systems per CTA
     int ngrp;    // CTA groups per coefficient set = ceil(rhs_per_set / nr)
-    int grp0;    // first group of this launch (grid.y chunking)
+    int set0;    // first coefficient set of this launch (grid.y chunking)
     int zchunk;  // z planes per CTA
     const T* u;  // (nsys, N, 3)
     const T* Kn; // (nset, 18, N)
@@ -51,14 +51,15 @@ template <typename T>
 cudaError_t launch_sc_tma(const TmaArgs<T>& a, bool epi, cudaStream_t st);
 
 // Pair-packed FP32 operator (kmv_pair.cu): vectors in the pair layout (npair, N, 3, 2), pair = set * npp + j / 2,
-// lane = j % 2 for system j of a set; unmasked output; epilogue as above.
+// lane = j % 2 for system j of a set; unmasked output; epilogue as above.  Its FP64 instantiation (one system per
+// lane group) takes natural-layout vectors: launch_sc_pair64 below.
 struct PairArgs {
     int nx, ny, nz;
     int64_t N;
     int nsys, rhs_per_set;
     int npp;     // pairs per coefficient set = ceil(rhs_per_set / 2)
     int npair;   // pairs in the batch = nset * npp
-    int pair0;   // first pair of this launch (grid.y chunking)
+    int set0;    // first coefficient set of this launch (grid.y chunking)
     int zchunk;  // z planes per CTA
     int variant; // 0: staged (Tv, Kn through shared memory, one CTA per SM); 1: lean (two CTAs per SM)
     const float* u;   // pair layout
@@ -99,6 +100,14 @@ int pair_zchunk_max_chunks(int nz);                               // z chunks al
 int pair_dot_blocks_max(int nx, int ny, int nz);
 cudaError_t launch_sc_pair(const PairArgs& a, bool epi, cudaStream_t st);
 cudaError_t launch_sc_pair_mode(const PairArgs& a, int mode, cudaStream_t st);
+// FP64 instantiation (lean variant, one system per lane group): u and out natural-layout (nsys, N, 3) FP64 arrays and
+// Kn / Tv packed FP64 coefficients, all passed through PairArgs' float pointers; npp = rhs_per_set, npair = nset *
+// npp.  epi: PM_DOT (u.out per system into part / cnt, and the CG alpha step when has_sc).
+bool pair64_supported(int nx);
+cudaError_t launch_sc_pair64(const PairArgs& a, bool epi, cudaStream_t st);
+// Arguments of the FP64 operator for a batch (no epilogue fields set).
+PairArgs pair64_args(int nx, int ny, int nz, int64_t N, int nsys, int rps, const double* u, const double* Kn,
+                     const double* Tv, double* out);
 // Shared-memory opt-in of every pair-operator kernel on the current device (call before capturing launches).
 cudaError_t pair_prepare();
 // (nsys, N, 3) FP32 -> pair layout (dummy lanes written as zero) and back (real systems only); npair <= 65535.
