@@ -187,6 +187,11 @@ __global__ void __launch_bounds__(pair_threads(LEAN), (LEAN && sizeof(CT) == 4) 
     constexpr int NL = LN::NL;
     constexpr int ES = (int)sizeof(CT);
     constexpr V VZ = V(0);
+    // FP64 lean: the own site's Tv of phase 2 (read from global memory, L2) is loaded before the block barrier that
+    // ends phase 1, so the loads are in flight while the block waits; the FP32 lean variant has no registers to spare.
+    constexpr bool PREF_TV = LEAN && sizeof(CT) == 8;
+    // Likewise its Kn of phase 1 is loaded at the top of the step, before the waits for the step's fills.
+    constexpr bool PREF_KN = LEAN && sizeof(CT) == 8;
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int NUS = u_slots(LEAN), NBAS = ba_slots(LEAN);
     constexpr int BTV = NUS, BKN = NUS + 2, NBAR = NUS + 4;  // mbarriers: u 0..NUS-1, Tv BTV.., Kn BKN..
@@ -346,6 +351,7 @@ __global__ void __launch_bounds__(pair_threads(LEAN), (LEAN && sizeof(CT) == 4) 
     CT tv_next[18];
 #pragma unroll
     for (int k = 0; k < 18; ++k) tv_next[k] = CT(0);
+    CT kn_pre[18];  // PREF_KN: the own site's Kn of the next phase 1
 
     // pm, p0, pp: the u slots of planes zp-1, zp, zp+1; bsl: the (B, A) slot of plane zp.
     auto site = [&](auto own_tag, auto mask_tag, int qx, int qy, const V* pm, const V* p0, const V* pp, BA* bsl,
@@ -377,7 +383,7 @@ __global__ void __launch_bounds__(pair_threads(LEAN), (LEAN && sizeof(CT) == 4) 
                     Tm0 = fma2(dup(tv), t, Tm0);
                 }
                 if constexpr (OWN) {
-                    const CT kn = LEAN ? __ldg(kns + k * kst) : kns[k * kst];
+                    const CT kn = PREF_KN ? kn_pre[k] : (LEAN ? __ldg(kns + k * kst) : kns[k * kst]);
                     fm[g.a] = fma2(dup(CT(2) * kn), t, fm[g.a]);  // f_a -= 2 Kn t
                     if (vb) {
                         s0[g.a] -= (CT)g.sa;
@@ -397,7 +403,7 @@ __global__ void __launch_bounds__(pair_threads(LEAN), (LEAN && sizeof(CT) == 4) 
                     Tm1 = fma2(dup(tv), t, Tm1);
                 }
                 if constexpr (OWN) {
-                    const CT kn = LEAN ? __ldg(kns + k * kst) : kns[k * kst];
+                    const CT kn = PREF_KN ? kn_pre[k] : (LEAN ? __ldg(kns + k * kst) : kns[k * kst]);
                     const V kn2 = dup(kn);
                     fm[g.a] = fma2(kn2, t, fm[g.a]);  // f_a -= sa Kn d' = Kn t
                     if (g.sa == g.sb)
@@ -478,6 +484,16 @@ __global__ void __launch_bounds__(pair_threads(LEAN), (LEAN && sizeof(CT) == 4) 
 
     using T_ = std::true_type;
     using F_ = std::false_type;
+    auto load_kn = [&](int zp) {  // PREF_KN: the own site's Kn of plane zp into kn_pre
+        if constexpr (PREF_KN) {
+            if (own_xy && zp >= 0 && zp < nz) {
+                const CT* kg = reinterpret_cast<const CT*>(P.Kn) + (int64_t)18 * set * P.N +
+                               ((int64_t)zp * ny + gy) * nx + gx;
+#pragma unroll
+                for (int k = 0; k < 18; ++k) kn_pre[k] = __ldg(kg + (int64_t)k * P.N);
+            }
+        }
+    };
     // Phase 1 of plane zp: pm, p0, pp are its u slots (planes zp-1, zp, zp+1), tvsl / knsl its Tv / Kn slots and bsl
     // its (B, A) slot.
     auto phase1 = [&](int zp, bool own, const V* pm, const V* p0, const V* pp, const CT* tvsl, const CT* knsl,
@@ -540,7 +556,7 @@ __global__ void __launch_bounds__(pair_threads(LEAN), (LEAN && sizeof(CT) == 4) 
             const SlotGeo g = slot_geo(k);
             const BA* pl = sc_dz(k) < 0 ? bm : (sc_dz(k) > 0 ? bp : b0);
             const BA v = pl[sc_shell(k) * PSPL + c0 + sc_dy(k) * PSW + sc_dx(k)];
-            const CT tvk = LEAN ? __ldg(tvg + (int64_t)k * P.N) : tv_cur[k];
+            const CT tvk = (LEAN && !PREF_TV) ? __ldg(tvg + (int64_t)k * P.N) : tv_cur[k];
             const V gw = fma2(dup(tvk), LN::b_of(v), LN::a_of(v));  // zero for bonds leaving the box
             f[g.a] = g.sa > 0 ? sub2(f[g.a], gw) : add2(f[g.a], gw);
             if (sc_shell(k) == 1) f[g.b] = g.sb > 0 ? sub2(f[g.b], gw) : add2(f[g.b], gw);
@@ -615,6 +631,7 @@ __global__ void __launch_bounds__(pair_threads(LEAN), (LEAN && sizeof(CT) == 4) 
                 else if (zbeg + 1 <= zend)
                     issue_tv(zbeg + 1);
             }
+            load_kn(zbeg);
             wait_planes(zbeg + 1, zbeg, zbeg);
             phase1(zbeg, true, u_slot(zbeg - 1), u_slot(zbeg), u_slot(zbeg + 1), tv_slot(zbeg), kn_slot(zbeg),
                    ba_slot(zbeg));
@@ -656,11 +673,20 @@ __global__ void __launch_bounds__(pair_threads(LEAN), (LEAN && sizeof(CT) == 4) 
                         if (z + 2 < zend) issue_kn(z + 2);
                     }
                 }
+                if (z + 1 < zend) load_kn(z + 1);
                 if (z + 2 < nz) wait_fill(iu2, pu2);
                 if (z + 1 < nz) wait_fill(BTV + itv, ptv);
                 if (!LEAN && z + 1 < zend) wait_fill(BKN + ikn, pkn);
                 phase1(z + 1, z + 1 < zend, uz, su + (size_t)iu1 * US, su + (size_t)iu2 * US, stv + (size_t)itv * TVS,
                        skn + (size_t)ikn * KNS, sba + (size_t)ib1 * BAS);
+                if constexpr (PREF_TV) {
+                    if (own_xy) {
+                        const CT* tvg = reinterpret_cast<const CT*>(P.Tv) + (int64_t)18 * set * P.N +
+                                        ((int64_t)z * ny + gy) * nx + gx;
+#pragma unroll
+                        for (int k = 0; k < 18; ++k) tv_cur[k] = __ldg(tvg + (int64_t)k * P.N);
+                    }
+                }
                 if (__syncthreads_or(lost)) {  // uniform: every thread leaves the loop at this barrier
                     ok = false;
                     break;

@@ -1,6 +1,6 @@
 """The bounded device waits of the TMA-fed operators made to run out, on purpose and safely: with the poll bound at 0
-(lpm_set_tma_wait_polls) every data wait expires at once, so the pair-packed FP32 operator (k_sc_pair) and the FP64
-TMA operator (k_sc_tma) take their abort path inside a CG solve: the block decides to stop at one barrier, lets the
+(lpm_set_tma_wait_polls) every data wait expires at once, so the pair-packed FP32 operator (k_sc_pair) and its FP64
+instantiation (one system per lane group) take their abort path inside a CG solve: the block decides to stop at one barrier, lets the
 copies it issued land with the full bound and returns, and the engine reports LPM_ERR_TIMEOUT.  Nothing hangs or
 faults: the next solve on the same GPU, with the default bound, gives the oracle's answer."""
 import numpy as np
