@@ -460,7 +460,8 @@ __global__ void __launch_bounds__(VB) k_pair_update(VecGeom G, int it_host, int 
     __shared__ bool last;
     const PairSys q = pair_of(G);
     const int64_t N = G.N;
-    const bool act0 = sc.act[q.s0] != 0, act1 = q.nl > 1 && sc.act[q.s0 + 1] != 0;
+    // q.nl < 1: a pair of a trailing partial set with no system behind it
+    const bool act0 = q.nl > 0 && sc.act[q.s0] != 0, act1 = q.nl > 1 && sc.act[q.s0 + 1] != 0;
     float vals[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
     // grid-stride over particles: few blocks per pair, so the reduction epilogue (fence, counter) is amortised
     for (int64_t i = (int64_t)blockIdx.x * VB + threadIdx.x; i < N && (act0 || act1); i += (int64_t)gridDim.x * VB) {
@@ -515,8 +516,9 @@ __global__ void __launch_bounds__(VB) k_pair_pupdate(VecGeom G, const uint8_t* _
     const int64_t i = (int64_t)blockIdx.x * VB + threadIdx.x;
     if (i >= N) return;
     const bool two = q.nl > 1;
-    const double a0d = sc.alpha[q.s0], a1d = two ? sc.alpha[q.s0 + 1] : 0.0;
-    const bool act0 = sc.act[q.s0] != 0, act1 = two && sc.act[q.s0 + 1] != 0;
+    const bool one = q.nl > 0;  // false for a pair of a trailing partial set with no system behind it
+    const double a0d = one ? sc.alpha[q.s0] : 0.0, a1d = two ? sc.alpha[q.s0 + 1] : 0.0;
+    const bool act0 = one && sc.act[q.s0] != 0, act1 = two && sc.act[q.s0 + 1] != 0;
     const bool mov = a0d != 0.0 || a1d != 0.0;
     if (!mov && !act0 && !act1) return;
     const int64_t po = ((int64_t)q.pr * N + i) * 6;

@@ -813,12 +813,14 @@ __global__ void k_pair_pack(const float* __restrict__ x, float* __restrict__ xp,
     if (i >= N) return;
     const int pr = blockIdx.y, set = pr / npp, jp = pr % npp;
     const int s0 = set * rps + 2 * jp;
-    const bool has1 = 2 * jp + 1 < rps && s0 + 1 < nsys;
+    // a trailing partial set leaves pairs (or second lanes) without a system: those lanes are written as zero and
+    // nothing past the batch is read
+    const bool has0 = s0 < nsys, has1 = 2 * jp + 1 < rps && s0 + 1 < nsys;
     const float* a0 = x + ((int64_t)s0 * N + i) * 3;
     const float* a1 = x + ((int64_t)(s0 + 1) * N + i) * 3;
     pair_t* o = reinterpret_cast<pair_t*>(xp + ((int64_t)pr * N + i) * 6);
 #pragma unroll
-    for (int a = 0; a < 3; ++a) o[a] = pk(a0[a], has1 ? a1[a] : 0.f);
+    for (int a = 0; a < 3; ++a) o[a] = pk(has0 ? a0[a] : 0.f, has1 ? a1[a] : 0.f);
 }
 
 __global__ void k_pair_unpack(const float* __restrict__ xp, float* __restrict__ x, int64_t N, int nsys, int rps,
@@ -828,6 +830,7 @@ __global__ void k_pair_unpack(const float* __restrict__ xp, float* __restrict__ 
     if (i >= N) return;
     const int pr = blockIdx.y, set = pr / npp, jp = pr % npp;
     const int s0 = set * rps + 2 * jp;
+    if (s0 >= nsys) return;  // a pair of a trailing partial set with no system behind it
     const bool has1 = 2 * jp + 1 < rps && s0 + 1 < nsys;
     const pair_t* v = reinterpret_cast<const pair_t*>(xp + ((int64_t)pr * N + i) * 6);
     float* a0 = x + ((int64_t)s0 * N + i) * 3;

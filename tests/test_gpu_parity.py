@@ -333,6 +333,35 @@ def test_fused_kmv(shape, rps, nset, dt):
         assert relmax(f[s], ref) < tol, s
 
 
+@pytest.mark.parametrize("dt", ["f64", "f32"])
+def test_fused_kmv_partial_last_set(dt):
+    """5 systems over coefficient sets of 3: the second set holds two systems, so the last pair group / lane of the
+    packed operators has no system behind it and must neither read past u nor write past out."""
+    from lpm_b200 import _lib
+    rng = np.random.default_rng(11)
+    lat = G.LatticeGeom(16, 12, 10)
+    dl = core.DeviceLattice(lat)
+    Kn = np.array([sym_params(lat, rng)[0] for _ in range(2)])
+    Tv = np.array([rng.uniform(-0.05, 0.05, (lat.N, 18)) * lat.valid for _ in range(2)])
+    u = rng.standard_normal((5, lat.N, 3))
+    tdt = torch.float64 if dt == "f64" else torch.float32
+    Kp, Tp = core.pack(T(Kn), tdt), core.pack(T(Tv), tdt)
+    import ctypes
+    uu = T(u, tdt).contiguous()
+    out = torch.full((6, lat.N, 3), 7.0, dtype=tdt, device=DEV)   # one spare system after the batch, to catch writes
+    lib = _lib.load()
+    prec = _lib.LPM_F64 if dt == "f64" else _lib.LPM_F32
+    scr = torch.empty(max(1, lib.lpm_kmv_scratch_bytes(dl.ref, prec, 5)), dtype=torch.uint8, device=DEV)
+    name = "lpm_kmv_sc_f64" if dt == "f64" else "lpm_kmv_sc_f32"
+    _lib.check(getattr(lib, name)(dl.ref, _lib.ptr(uu), _lib.ptr(Kp), _lib.ptr(Tp), _lib.LAYOUT_SOA,
+                                  ctypes.byref(core._batch(5, 3)), _lib.ptr(out), _lib.ptr(scr), scr.numel(),
+                                  _lib.stream_ptr(uu.device)), name)
+    tol = 1e-13 if dt == "f64" else 3e-6
+    for s in range(5):
+        assert relmax(out[s].cpu().numpy(), O.sc_apply(lat, u[s], Kn[s // 3], Tv[s // 3])) < tol, s
+    assert torch.all(out[5] == 7.0)
+
+
 @pytest.mark.parametrize("precond", [False, True])
 def test_fused_cg_fp64_matches_oracle(gsc, sc12, precond):
     """FP64 CG on the fused path (packed coefficients): same iteration counts as the reference at 1e-8."""
