@@ -62,9 +62,13 @@ constexpr int PNRING = PSPL - PNT;
 // Threads per CTA.  Lean: the 256 tile threads also take the 68 ring sites (threads 0..67).  Staged: three more warps
 // own the ring sites (threads 256..323), so the tile warps carry no ring work and phase 1 costs every warp about the
 // same; an idle lane of the last ring warp issues the TMA fills, off the tile warps' path.
-constexpr int PRING_THREADS = 96;
+#ifndef LPM_PAIR_RING_THREADS
+#define LPM_PAIR_RING_THREADS 96
+#endif
+constexpr int PRING_THREADS = LPM_PAIR_RING_THREADS;  // ring threads of the staged variant (a multiple of 32)
+constexpr int PRING_ITEMS = (PNRING + PRING_THREADS - 1) / PRING_THREADS;  // ring sites per ring thread (at most)
 __host__ __device__ constexpr int pair_threads(bool lean) { return lean ? PNT : PNT + PRING_THREADS; }
-static_assert(PNRING <= PRING_THREADS, "ring warps cover the ring");
+static_assert(PRING_THREADS % 32 == 0 && PRING_THREADS >= 32, "whole ring warps");
 constexpr unsigned FULL18 = 0x3FFFFu;
 
 constexpr size_t PU_SLOT = (size_t)PUH * PUW * 4;
@@ -462,25 +466,40 @@ __global__ void __launch_bounds__(pair_threads(LEAN), (LEAN && sizeof(CT) == 4) 
     const int gx = x0 + tx, gy = y0 + ty;
     const bool own_xy = tile_thr && gx < nx && gy < ny;
     const unsigned own_mxy = xy_mask(gx, gy);
-    const int rit = LEAN ? tid : tid - PNT;  // ring item of this thread
-    const bool has_item = rit >= 0 && rit < PNRING;
-    int rqx = 0, rqy = 0;
-    if (rit < PSW) {
-        rqx = rit;
-        rqy = 0;
-    } else if (rit < 2 * PSW) {
-        rqx = rit - PSW;
-        rqy = PSH - 1;
-    } else if (rit < 2 * PSW + PY) {
-        rqx = 0;
-        rqy = rit - 2 * PSW + 1;
-    } else {
-        rqx = PSW - 1;
-        rqy = rit - 2 * PSW - PY + 1;
-    }
-    const int rX = x0 - 1 + rqx, rY = y0 - 1 + rqy;
-    const bool ring_in = has_item && rX >= 0 && rX < nx && rY >= 0 && rY < ny;
-    const unsigned ring_mxy = xy_mask(rX, rY);
+    // Ring sites of this thread: items rit, rit + RSTR, ... (lean: the tile threads 0..67 take one each; staged: the
+    // ring threads take PRING_ITEMS at most).  Item geometry: position in the ring, inside the box, box-edge mask.
+    const int rit = LEAN ? tid : tid - PNT;
+    constexpr int RSTR = LEAN ? PNT : PRING_THREADS;
+    constexpr int RITEMS = LEAN ? 1 : PRING_ITEMS;
+    struct RingSite {
+        int qx, qy;
+        bool in;
+        unsigned mxy;
+    };
+    auto ring_site = [&](int it) {
+        RingSite r{0, 0, false, 0u};
+        if (it < 0 || it >= PNRING) return r;
+        if (it < PSW) {
+            r.qx = it;
+            r.qy = 0;
+        } else if (it < 2 * PSW) {
+            r.qx = it - PSW;
+            r.qy = PSH - 1;
+        } else if (it < 2 * PSW + PY) {
+            r.qx = 0;
+            r.qy = it - 2 * PSW + 1;
+        } else {
+            r.qx = PSW - 1;
+            r.qy = it - 2 * PSW - PY + 1;
+        }
+        const int X = x0 - 1 + r.qx, Y = y0 - 1 + r.qy;
+        r.in = X >= 0 && X < nx && Y >= 0 && Y < ny;
+        r.mxy = xy_mask(X, Y);
+        return r;
+    };
+    RingSite rs[RITEMS];
+#pragma unroll
+    for (int j = 0; j < RITEMS; ++j) rs[j] = ring_site(rit >= 0 ? rit + j * RSTR : -1);  // tile threads: none
 
     using T_ = std::true_type;
     using F_ = std::false_type;
@@ -529,7 +548,11 @@ __global__ void __launch_bounds__(pair_threads(LEAN), (LEAN && sizeof(CT) == 4) 
                     site(F_{}, T_{}, tx + 1, ty + 1, pm, p0, pp, bsl, vm, tvs, nullptr, 0);
             }
         }
-        const unsigned rvm = ring_mxy & zm;
+#pragma unroll
+        for (int j = 0; j < RITEMS; ++j) {
+        const int rqx = rs[j].qx, rqy = rs[j].qy;
+        const bool ring_in = rs[j].in;
+        const unsigned rvm = rs[j].mxy & zm;
         const bool runi = __all_sync(0xffffffffu, !ring_in || rvm == FULL18);
         if (ring_in) {
             const CT* tvs = tvsl + rqy * PTVW + rqx + 3;
@@ -537,6 +560,7 @@ __global__ void __launch_bounds__(pair_threads(LEAN), (LEAN && sizeof(CT) == 4) 
                 site(F_{}, F_{}, rqx, rqy, pm, p0, pp, bsl, rvm, tvs, nullptr, 0);
             else
                 site(F_{}, T_{}, rqx, rqy, pm, p0, pp, bsl, rvm, tvs, nullptr, 0);
+        }
         }
     };
 
