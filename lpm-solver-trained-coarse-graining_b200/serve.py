@@ -238,16 +238,16 @@ class Bucket:
             self.T32[s:s + 1] = core.pack(Tr, _F32)
             self.M32[s:s + 1] = core.block_jacobi(self.dl, Kr, Tr, _F32)
             rows = self.rows(s, req) - s * R          # the request's system slots within the specimen slot
-            free = torch.ones((R, N, d), dtype=torch.uint8)
-            up = torch.zeros((R, N, d), dtype=torch.float64)
-            if self.use_amg:
-                free.copy_(self.mask.cpu())
-            free[rows] = torch.as_tensor(req.free.reshape(req.nloads, N, d)).to(torch.uint8)
-            up[rows] = torch.as_tensor(req.up.reshape(req.nloads, N, d))
+            rows_t = torch.as_tensor(rows, device=dv)
+            # DOF masks and prescribed displacements of the slot's R systems, built on the device (only the
+            # request's own arrays cross from the host)
+            fr = self.mask.clone() if self.use_amg else torch.ones((R, N, d), dtype=torch.uint8, device=dv)
+            fr[rows_t] = torch.as_tensor(req.free.reshape(req.nloads, N, d)).to(dv, torch.uint8)
+            up = torch.zeros((R, N, d), dtype=torch.float64, device=dv)
+            up[rows_t] = torch.as_tensor(req.up.reshape(req.nloads, N, d)).to(dv)
             if not self.use_amg:
-                self.mask[sl].copy_(free.to(dv))
-            fr = free.to(dv)
-            self.up[sl].copy_((up * (1 - free.double())).to(dv))
+                self.mask[sl].copy_(fr)
+            self.up[sl].copy_(up * (1 - fr.double()))
             Ku = core.kmv(self.dl, self.up[sl], self.K64[s:s + 1], self.T64[s:s + 1], layout=L.LAYOUT_SOA,
                           rhs_per_set=R)
             used = torch.zeros(R, dtype=_F64, device=dv)
