@@ -973,23 +973,46 @@ __global__ void __launch_bounds__(GD_T, 3) k_galerkin0(BoxDev B, int a, int wm, 
             float sp[24];
             sums(lp, 0, sp);
             sums(lp, 1, sp + 12);
+            // p's own shell sums enter every slot of their shell: sum_k n_k (TS_p^c + Tv_pk S_p^c) / 2 =
+            // (s^c (x) TS_p^c + T^c (x) S_p^c) / 2 with s^c = sum n_k and T^c = sum Tv_pk n_k over the valid slots
+            float sv[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}}, tn[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
             gd_for<0>([&](auto kc) {
                 constexpr int k = decltype(kc)::value;
                 if (!((valid >> k) & 1u)) return;
                 constexpr int c = k < 6 ? 0 : 1;
-                float sq[12];
-                if ((qr1 >> k) & 1u) {
-                    sums(lp + sc_dx(k) + sc_dy(k) * sy1 + sc_dz(k) * sz1, c, sq);
-                } else {
+                constexpr float w = k < 6 ? 1.f : (float)INV_SQRT2;
+                constexpr int o3[3] = {sc_dx(k), sc_dy(k), sc_dz(k)};
 #pragma unroll
-                    for (int m = 0; m < 12; ++m) sq[m] = 0.f;
+                for (int ax = 0; ax < 3; ++ax) {
+                    if (o3[ax] == 0) continue;
+                    const float nk = -w * (float)o3[ax];
+                    sv[c][ax] += nk;
+                    tn[c][ax] = fmaf(tvp[k], nk, tn[c][ax]);
                 }
-                const float tvh = 0.5f * tvp[k];
-                float F[6];
+            });
 #pragma unroll
-                for (int m = 0; m < 6; ++m)
-                    F[m] = fmaf(tvh, sp[12 * c + m] + sq[m], 0.5f * (sp[12 * c + 6 + m] + sq[6 + m]));
-                if ((cross >> k) & 1u) {
+            for (int c = 0; c < 2; ++c)
+#pragma unroll
+                for (int ax = 0; ax < 3; ++ax)
+#pragma unroll
+                    for (int m = 0; m < 6; ++m)
+                        f[ax * 6 + m] = fmaf(0.5f * sv[c][ax], sp[12 * c + 6 + m],
+                                             fmaf(0.5f * tn[c][ax], sp[12 * c + m], f[ax * 6 + m]));
+            // the neighbour's shell sums and the bond stretch, per slot
+            gd_for<0>([&](auto kc) {
+                constexpr int k = decltype(kc)::value;
+                const bool qin = (qr1 >> k) & 1u, cr = (cross >> k) & 1u;
+                if (!qin && !cr) return;
+                constexpr int c = k < 6 ? 0 : 1;
+                float F[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                if (qin) {
+                    float sq[12];
+                    sums(lp + sc_dx(k) + sc_dy(k) * sy1 + sc_dz(k) * sz1, c, sq);
+                    const float tvh = 0.5f * tvp[k];
+#pragma unroll
+                    for (int m = 0; m < 6; ++m) F[m] = fmaf(tvh, sq[m], 0.5f * sq[6 + m]);
+                }
+                if (cr) {
                     constexpr float w = k < 6 ? 1.f : (float)INV_SQRT2;
                     float dl[6];
                     if (pj)
