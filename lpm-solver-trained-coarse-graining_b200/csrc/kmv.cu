@@ -180,9 +180,11 @@ __global__ void __launch_bounds__(sqtile::NT) k_sq_fused(int nx, int ny, int64_t
 }
 
 // Several systems sharing a coefficient set: one block per tile and set stages the tile's coefficients (tile + ring,
-// both arrays) in shared memory once and applies the operator to every system of the set in turn, so a set's
+// both arrays) in shared memory once and applies the operator to every system of the set, two per pass (one staging
+// of both systems' displacements, one barrier-separated shell-sum and force phase for the pair), so a set's
 // coefficients cross L2 once per tile instead of once per system.  Same arithmetic, output, epilogue and block
-// numbering as k_sq_fused.
+// numbering as k_sq_fused.  (Splitting a set's systems over more blocks, each staging the coefficients again, was
+// slower: 0.065 -> 0.091 ms for six systems on a 512^2 box.)
 template <typename T, bool EPI>
 __global__ void __launch_bounds__(sqtile::NT) k_sq_multi(int nx, int ny, int64_t N, int set0, const T* __restrict__ u,
                                                          const T* __restrict__ Kn, const T* __restrict__ Tv,
@@ -192,7 +194,7 @@ __global__ void __launch_bounds__(sqtile::NT) k_sq_multi(int nx, int ny, int64_t
                                                          unsigned* __restrict__ counter, const int* __restrict__ act)
 {
     constexpr int NC = 8 * sqtile::SH * sqtile::SW;
-    __shared__ sqtile::Smem<T> sm;
+    __shared__ sqtile::Smem<T> sm[2];
     __shared__ T ck[NC], ct[NC];
     __shared__ double sh[32];
     __shared__ bool last;
@@ -209,48 +211,66 @@ __global__ void __launch_bounds__(sqtile::NT) k_sq_multi(int nx, int ny, int64_t
     const sqtile::SharedCoef<T> kn{ck}, tv{ct};
     const int nblk = gridDim.x * gridDim.y;
     const int b = blockIdx.x + gridDim.x * blockIdx.y;
-    for (int j = 0; j < ns; ++j) {
-        const int s = s0 + j;
-        if (act && !act[s]) continue;
-        const T* us = u + (int64_t)s * N * 2;
-        auto load = [&](int64_t q, T* v) {
-            v[0] = us[2 * q];
-            v[1] = us[2 * q + 1];
-        };
-        __syncthreads();  // the coefficients are staged and the previous system's tile is no longer read
-        sqtile::stage(nx, ny, x0, y0, load, sm);
+    for (int j = 0; j < ns; j += 2) {
+        const int sa[2] = {s0 + j, s0 + j + 1};
+        const bool on[2] = {!act || act[sa[0]], j + 1 < ns && (!act || act[sa[1]])};
+        if (!on[0] && !on[1]) continue;  // the same for every thread of the block
+        __syncthreads();  // the coefficients are staged and the previous pass's tiles are no longer read
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (!on[h]) continue;
+            const T* us = u + (int64_t)sa[h] * N * 2;
+            sqtile::stage(nx, ny, x0, y0,
+                          [&](int64_t q, T* v) {
+                              v[0] = us[2 * q];
+                              v[1] = us[2 * q + 1];
+                          },
+                          sm[h]);
+        }
         __syncthreads();
-        sqtile::sums(nx, ny, x0, y0, tv, sm);
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+            if (on[h]) sqtile::sums(nx, ny, x0, y0, tv, sm[h]);
         __syncthreads();
-        double dot = 0.0;
-        sqtile::forces(nx, ny, x0, y0, kn, tv, sm, [&](int64_t i, T (&f)[2], const T* ui) {
-            if (EPI && mask) {
-                const uint8_t* m = mask + ((int64_t)(s % bt.nmask) * N + i) * 2;
-                f[0] = m[0] ? f[0] : T(0);
-                f[1] = m[1] ? f[1] : T(0);
-            }
-            T* o = out + ((int64_t)s * N + i) * 2;
-            o[0] = f[0];
-            o[1] = f[1];
-            dot += (double)ui[0] * (double)f[0] + (double)ui[1] * (double)f[1];
-        });
+        double dot[2] = {0.0, 0.0};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (!on[h]) continue;
+            const int s = sa[h];
+            sqtile::forces(nx, ny, x0, y0, kn, tv, sm[h], [&](int64_t i, T (&f)[2], const T* ui) {
+                if (EPI && mask) {
+                    const uint8_t* m = mask + ((int64_t)(s % bt.nmask) * N + i) * 2;
+                    f[0] = m[0] ? f[0] : T(0);
+                    f[1] = m[1] ? f[1] : T(0);
+                }
+                T* o = out + ((int64_t)s * N + i) * 2;
+                o[0] = f[0];
+                o[1] = f[1];
+                dot[h] += (double)ui[0] * (double)f[0] + (double)ui[1] * (double)f[1];
+            });
+        }
         if constexpr (EPI) {
             if (part == nullptr) continue;
-            const double v = block_sum(dot, sh);
-            if (threadIdx.x == 0) {
-                part[(int64_t)s * nblk + b] = v;
-                __threadfence();
-                last = atomicAdd(counter + s, 1u) == (unsigned)(nblk - 1);
-            }
-            __syncthreads();
-            if (last) {
-                double acc = 0.0;
-                for (int q = threadIdx.x; q < nblk; q += sqtile::NT) acc += __ldcg(part + (int64_t)s * nblk + q);
-                acc = block_sum(acc, sh);
+            for (int h = 0; h < 2; ++h) {
+                if (!on[h]) continue;
+                const int s = sa[h];
+                const double v = block_sum(dot[h], sh);
                 if (threadIdx.x == 0) {
-                    dot_final[s] = acc;
-                    counter[s] = 0u;
+                    part[(int64_t)s * nblk + b] = v;
+                    __threadfence();
+                    last = atomicAdd(counter + s, 1u) == (unsigned)(nblk - 1);
                 }
+                __syncthreads();
+                if (last) {
+                    double acc = 0.0;
+                    for (int q = threadIdx.x; q < nblk; q += sqtile::NT) acc += __ldcg(part + (int64_t)s * nblk + q);
+                    acc = block_sum(acc, sh);
+                    if (threadIdx.x == 0) {
+                        dot_final[s] = acc;
+                        counter[s] = 0u;
+                    }
+                }
+                __syncthreads();  // `last` and `sh` are reused by the next system
             }
         }
     }

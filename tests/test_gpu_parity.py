@@ -362,6 +362,39 @@ def test_fused_kmv_partial_last_set(dt):
     assert torch.all(out[5] == 7.0)
 
 
+@pytest.mark.parametrize("shape,rps,nsys", [((40, 17), 3, 6), ((33, 9), 2, 4), ((64, 24), 5, 10), ((36, 20), 3, 5),
+                                             ((70, 9), 4, 7), ((31, 8), 2, 3)])
+@pytest.mark.parametrize("dt", ["f64", "f32"])
+def test_fused_kmv_sq_sets(shape, rps, nsys, dt):
+    """Packed square-lattice K.u with several systems per coefficient set (FP32 applies them two per pass over one
+    staging of a tile's coefficients): even, odd and partly filled last sets, tiles cut by the box edge, and no
+    write past the batch (one spare system after it keeps its fill)."""
+    import ctypes
+    rng = np.random.default_rng(sum(shape) + rps)
+    lat = G.Lattice2D("square", *shape, 1.0)
+    dl = core.DeviceLattice(lat)
+    nset = -(-nsys // rps)
+    Kn = np.array([rng.uniform(0.5, 1.5, (lat.N, lat.NN)) * lat.valid for _ in range(nset)])
+    Tv = np.array([rng.uniform(-0.1, 0.1, (lat.N, lat.NN)) * lat.valid for _ in range(nset)])
+    u = rng.standard_normal((nsys, lat.N, 2))
+    tdt = torch.float64 if dt == "f64" else torch.float32
+    Kp, Tp = core.pack(T(Kn), tdt), core.pack(T(Tv), tdt)
+    uu = T(u, tdt).contiguous()
+    out = torch.full((nsys + 1, lat.N, 2), 7.0, dtype=tdt, device=DEV)
+    lib = L.load()
+    prec = L.LPM_F64 if dt == "f64" else L.LPM_F32
+    scr = torch.empty(max(1, lib.lpm_kmv_scratch_bytes(dl.ref, prec, nsys)), dtype=torch.uint8, device=DEV)
+    name = "lpm_kmv_sq_f64" if dt == "f64" else "lpm_kmv_sq_f32"
+    L.check(getattr(lib, name)(dl.ref, L.ptr(uu), L.ptr(Kp), L.ptr(Tp), L.LAYOUT_SOA,
+                               ctypes.byref(core._batch(nsys, rps)), L.ptr(out), L.ptr(scr), scr.numel(),
+                               L.stream_ptr(uu.device)), name)
+    tol = 1e-13 if dt == "f64" else 3e-6
+    for s in range(nsys):
+        ref = O.sq_kmv(lat, u[s].ravel(), Kn[s // rps], Tv[s // rps])
+        assert relmax(out[s].cpu().numpy().ravel(), ref) < tol, s
+    assert torch.all(out[nsys] == 7.0)
+
+
 @pytest.mark.parametrize("precond", [False, True])
 def test_fused_cg_fp64_matches_oracle(gsc, sc12, precond):
     """FP64 CG on the fused path (packed coefficients): same iteration counts as the reference at 1e-8."""

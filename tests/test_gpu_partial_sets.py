@@ -79,3 +79,49 @@ def test_amg_ir_partial_last_set(case):
     for s in range(NSYS):
         assert rel_l2(x[s].cpu().numpy(), case["ref"][s]) < 1e-6, s
     ab.close()
+
+
+@pytest.mark.parametrize("dt", ["f64", "f32"])
+def test_packed_cg_2d_partial_last_set(dt):
+    """Square-lattice CG on the packed operator (FP32: two systems per pass of the multi-system tile kernel) with 5
+    systems over sets of 3 and three grip loads, so systems leave the batch at different iterations; each against
+    the oracle's plain CG to 1e-12 (FP32 CG runs to 1e-6 here), and against the same systems given one coefficient
+    set each."""
+    nx, ny = 40, 28
+    lat = G.Lattice2D("square", nx, ny, 1.0)
+    dl = core.DeviceLattice(lat)
+    Kn, Tv = [], []
+    for seed in (0, 1):
+        ph = np.random.default_rng(seed).random(lat.N) < 0.3
+        C = G.iso_C2d(np.where(ph, 10.0, 1.0), 0.25, plane="stress")
+        k, t = G.bond_params_two_end_mean(lat, G.square_params_from_C(C))
+        Kn.append(k)
+        Tv.append(t)
+    loads = ["tb_ty", "tb_sx", "lr_tx"]
+    sys_set = [s // RPS for s in range(NSYS)]
+    fr, ups, b, ref = [], [], [], []
+    for s in range(NSYS):
+        fixed, up, _ = G.prescribed2d(loads[s % RPS], lat.x, lat.ij, nx, ny, 1, 1.0)
+        fd = np.repeat(fixed[:, None], 2, axis=1)
+        upm = np.where(fd, up, 0.0)
+        fr.append(~fd)
+        ups.append(upm)
+        b.append(-O.sq_kmv(lat, upm.ravel(), Kn[sys_set[s]], Tv[sys_set[s]]).reshape(-1, 2) * ~fd)
+        ref.append(O.sq_solve_cg(lat, Kn[sys_set[s]], Tv[sys_set[s]], fd, upm, tol=1e-12)[0] - upm)
+    tdt = torch.float64 if dt == "f64" else torch.float32
+    tol = 1e-10 if dt == "f64" else 1e-6
+    bd = torch.as_tensor(np.array(b), device=DEV, dtype=tdt)
+    fd = torch.as_tensor(np.array(fr), device=DEV, dtype=tdt)
+    xs = []
+    for sets in ([0, 1], sys_set):   # sets of 3 (the last partly filled), then one set per system
+        Kp = core.pack(torch.as_tensor(np.array(Kn)[sets], device=DEV), tdt)
+        Tp = core.pack(torch.as_tensor(np.array(Tv)[sets], device=DEV), tdt)
+        x, info = core.cg(dl, Kp, Tp, bd, free=fd, tol=tol, maxit=20000, check=1, layout=L.LAYOUT_SOA,
+                          rhs_per_set=RPS if len(sets) == 2 else 1, engine=L.ENGINE_LAUNCHED)
+        assert (info.status == 0).all()
+        xs.append(x.double().cpu().numpy())
+    bar = 1e-7 if dt == "f64" else 1e-4
+    for s in range(NSYS):
+        assert rel_l2(xs[0][s], ref[s]) < bar, (dt, s, rel_l2(xs[0][s], ref[s]))
+        # same arithmetic per system either way; FP32 CG may amplify last-bit differences of contracted products
+        assert rel_l2(xs[0][s], xs[1][s]) < (1e-12 if dt == "f64" else 1e-5), (dt, s, rel_l2(xs[0][s], xs[1][s]))
