@@ -537,7 +537,7 @@ def run_plain2d(a):
     torch.cuda.synchronize(dev)
     ms_e2e = ev0.elapsed_time(ev1)
     # comparator: the same solves on the graph-launched engine (one launch per step, host polls)
-    engine = "persistent" if L.load().lpm_cg_persistent_fits(dl.ref, core._batch(B, 1, B)) else "launched"
+    engine = "persistent" if L.load().lpm_cg_persistent_fits(dl.ref, core._batch(B, 1, B), L.LPM_F64) else "launched"
     step(Kn, Tv, free, up, L.ENGINE_LAUNCHED)
     torch.cuda.synchronize(dev)
     ev0.record()

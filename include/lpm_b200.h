@@ -164,11 +164,12 @@ int lpm_cg_batched_f32(const lpm_lattice* lat, const float* Kn, const float* Tv,
                        int32_t x_is_zero, const lpm_cg_opts* opts, void* workspace, size_t workspace_bytes,
                        int32_t* iters, double* relres, int32_t* status, void* stream);
 
-/* 1 if the automatic engine choice runs this batch on the persistent engine: square-lattice batches of at most 2^20
- * particle-systems that fit on teams of co-resident blocks (every system's particles on one team).  The persistent engine keeps the launched engine's algorithm, tests and
+/* 1 if the automatic engine choice runs this batch in `precision` (LPM_F64 / LPM_F32) on the persistent engine:
+ * square-lattice batches of at most 2^17 (FP64) or 2^19 (FP32) particle-systems that fit on teams of co-resident
+ * blocks (every system's particles on one team).  The persistent engine keeps the launched engine's algorithm, tests and
  * freezing (same iteration counts up to the rounding of its reductions) and runs one cooperative kernel per solve:
  * three team barriers per iteration, each wait bounded in time (LPM_ERR_TIMEOUT on expiry). */
-int lpm_cg_persistent_fits(const lpm_lattice* lat, const lpm_batch* batch);
+int lpm_cg_persistent_fits(const lpm_lattice* lat, const lpm_batch* batch, int32_t precision);
 
 /* Bound of one team-barrier wait of the persistent engine, in ns (process-wide, default 2e9); returns the previous
  * bound.  A wait that exceeds it records LPM_ERR_TIMEOUT, the kernel's blocks return and the solve reports that code.

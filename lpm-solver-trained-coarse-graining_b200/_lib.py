@@ -60,7 +60,7 @@ _SIGS = {
     "lpm_block_jacobi_f64": ([_P(Lattice), _c_p, _c_p, _c_i32, _c_i32, _c_p, _c_p, _c_p], ctypes.c_int),
     "lpm_block_jacobi_f32": ([_P(Lattice), _c_p, _c_p, _c_i32, _c_i32, _c_p, _c_p, _c_p], ctypes.c_int),
     "lpm_cg_workspace_bytes": ([_P(Lattice), _P(Batch), _c_i32, _c_i32], _c_i64),
-    "lpm_cg_persistent_fits": ([_P(Lattice), _P(Batch)], ctypes.c_int),
+    "lpm_cg_persistent_fits": ([_P(Lattice), _P(Batch), ctypes.c_int32], ctypes.c_int),
     "lpm_cg_batched_f64": ([_P(Lattice), _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p, _c_p, _c_p, _c_i32, _P(CgOpts),
                             _c_p, _c_sz, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
     "lpm_cg_batched_f32": ([_P(Lattice), _c_p, _c_p, _c_i32, _P(Batch), _c_p, _c_p, _c_p, _c_p, _c_i32, _P(CgOpts),

@@ -221,12 +221,13 @@ int64_t lpm_cg_workspace_bytes(const lpm_lattice* lat, const lpm_batch* batch, i
     return (int64_t)cg_workspace_bytes(L, bt, precision, precond) + 256;
 }
 
-int lpm_cg_persistent_fits(const lpm_lattice* lat, const lpm_batch* batch)
+int lpm_cg_persistent_fits(const lpm_lattice* lat, const lpm_batch* batch, int32_t precision)
 {
     Lattice L;
     Batch bt;
     if (to_lattice(lat, L) || to_batch(batch, bt)) return LPM_ERR_ARG;
-    return persist_auto(L, bt) ? 1 : 0;
+    if (precision != LPM_F64 && precision != LPM_F32) return LPM_ERR_ARG;
+    return persist_auto(L, bt, precision == LPM_F64 ? 8 : 4) ? 1 : 0;
 }
 
 int lpm_cg_batched_f64(const lpm_lattice* lat, const double* Kn, const double* Tv, int32_t coef_layout,

@@ -451,7 +451,7 @@ int cg_solve(const Lattice& L, const T* Kn, const T* Tv, const CoefLayout& cl, c
 {
     if (o.maxit < 0 || o.check < 1 || o.poll < 1 || bt.nsys < 1) return LPM_ERR_ARG;
     if (o.engine < LPM_ENGINE_AUTO || o.engine > LPM_ENGINE_PERSISTENT) return LPM_ERR_ARG;
-    if (o.engine == LPM_ENGINE_PERSISTENT || (o.engine == LPM_ENGINE_AUTO && !o.prof && persist_auto(L, bt)))
+    if (o.engine == LPM_ENGINE_PERSISTENT || (o.engine == LPM_ENGINE_AUTO && !o.prof && persist_auto(L, bt, (int)sizeof(T))))
         return cg_solve_persist<T>(L, Kn, Tv, cl, bt, Minv, mask, b, x, x_is_zero, o, ws, ws_bytes, iters, relres,
                                    status, st);
     if (fused_ok(L, cl, (int)sizeof(T)) && tma_aligned(Kn, Tv, b))

@@ -653,12 +653,17 @@ bool persist_fits(const Lattice& L, const Batch& bt)
     return team_shape(bt.nsys, L.N, sms).nteam > 0;
 }
 
-// The automatic choice: 2D batches of up to 2^20 particle-systems (the 3D operator's fused TMA kernels are faster
-// than the persistent kernel's per-particle passes at every size measured).
-bool persist_auto(const Lattice& L, const Batch& bt)
+// The automatic choice: 2D batches of up to 2^17 (FP64) or 2^19 (FP32) particle-systems.  Plain CG per iteration on
+// one B200, packed coefficients, persistent vs launched: FP64 14.6 vs 22.9 us at 4 x 128^2, 30.3 vs 26.0 at
+// 10 x 128^2, 131 vs 88 at 40 x 128^2; FP32 24.3 vs 26.7 at 10 x 128^2, 54.1 vs 54.3 at 40 x 128^2, 119 vs 98 at
+// 16 x 256^2.  A persistent block takes its team's tiles one after another, while the launched operator has every
+// tile of the batch in flight.  (3D: the operator's fused TMA kernels are faster than the persistent kernel's
+// per-particle passes at every size measured.)
+bool persist_auto(const Lattice& L, const Batch& bt, int elem_bytes)
 {
     const int64_t units = (int64_t)bt.nsys * L.N;
-    return L.dim == 2 && units <= ((int64_t)1 << 20) && persist_fits(L, bt);
+    const int64_t cap = (int64_t)1 << (elem_bytes == 8 ? 17 : 19);
+    return L.dim == 2 && units <= cap && persist_fits(L, bt);
 }
 
 size_t persist_workspace_bytes(const Lattice& L, const Batch& bt, int elem_bytes)

@@ -14,6 +14,7 @@
 // int32 neighbour table.  The fused single-pass z-marching SC kernel for full boxes lives in kmv_fused.cu.
 #include "lpm_kernels.h"
 #include "lpm_sqtile.cuh"
+#include <atomic>
 #include "lpm_stencil.cuh"
 
 namespace lpm {
@@ -117,9 +118,14 @@ __global__ void __launch_bounds__(256) k_apply(NB nb, int nx, int ny, int nz, in
     }
 }
 
-// Full 2D boxes: both passes in one kernel (lpm_sqtile.cuh), one 32 x 8 tile of one system per block.  The
-// optional epilogue masks the output and reduces u.out per system like k_apply (same block numbering).
-template <typename T, bool EPI>
+// Full 2D boxes: both passes in one kernel (lpm_sqtile.cuh), one 32 x 8 tile of one system per block.  SC: the
+// tile's Kn and Tv (tile + ring) are staged in shared memory with the displacements, in one phase with coalesced
+// reads, and the shell sums and forces read no global memory; taken for the reference layout, whose per-site slot
+// runs make the direct per-slot reads of a warp touch one sector per lane.  Without SC (packed layout, where a warp's
+// per-slot reads are contiguous) the coefficients are read from global memory / L1 in the passes, which keeps the
+// block at 18 KB of shared memory (FP64) and the SM at five blocks.  The optional epilogue masks the output and
+// reduces u.out per system like k_apply (same block numbering).
+template <typename T, bool EPI, bool SC>
 __global__ void __launch_bounds__(sqtile::NT) k_sq_fused(int nx, int ny, int64_t N, int sys0, const T* __restrict__ u,
                                                          const T* __restrict__ Kn, const T* __restrict__ Tv,
                                                          CoefLayout cl, Batch bt, T* __restrict__ out,
@@ -127,7 +133,13 @@ __global__ void __launch_bounds__(sqtile::NT) k_sq_fused(int nx, int ny, int64_t
                                                          double* __restrict__ dot_final,
                                                          unsigned* __restrict__ counter, const int* __restrict__ act)
 {
-    __shared__ sqtile::Smem<T> sm;
+    extern __shared__ __align__(16) unsigned char sq_dyn[];
+    __shared__ std::conditional_t<SC, char, sqtile::Smem<T>> sm_static;
+    sqtile::CoefSmem<T>& cs = *reinterpret_cast<sqtile::CoefSmem<T>*>(sq_dyn);
+    sqtile::Smem<T>& sm = *[&]() {
+        if constexpr (SC) return &cs.t;
+        else return &sm_static;
+    }();
     const int s = sys0 + blockIdx.z;
     if (act && !act[s]) return;
     const int x0 = blockIdx.x * sqtile::TX, y0 = blockIdx.y * sqtile::TY;
@@ -137,8 +149,19 @@ __global__ void __launch_bounds__(sqtile::NT) k_sq_fused(int nx, int ny, int64_t
         v[0] = us[2 * q];
         v[1] = us[2 * q + 1];
     };
-    const sqtile::GlobalCoef<T> kn{Kn + cbase, cl, nx, x0, y0}, tv{Tv + cbase, cl, nx, x0, y0};
-    sqtile::stage(nx, ny, x0, y0, load, sm);
+    using KA = std::conditional_t<SC, sqtile::SharedCoef<T>, sqtile::GlobalCoef<T>>;
+    KA kn, tv;
+    if constexpr (SC) {
+        sqtile::stage(nx, ny, x0, y0, load, sm);
+        sqtile::stage_coef(nx, ny, x0, y0, Tv + cbase, cl, cs.tv);
+        sqtile::stage_coef(nx, ny, x0, y0, Kn + cbase, cl, cs.kn);
+        kn = KA{cs.kn};
+        tv = KA{cs.tv};
+    } else {
+        sqtile::stage(nx, ny, x0, y0, load, sm);
+        kn = KA{Kn + cbase, cl, nx, x0, y0};
+        tv = KA{Tv + cbase, cl, nx, x0, y0};
+    }
     __syncthreads();
     sqtile::sums(nx, ny, x0, y0, tv, sm);
     __syncthreads();
@@ -295,6 +318,22 @@ cudaError_t run_sq_multi(const Lattice& L, const T* u, const T* Kn, const T* Tv,
     return cudaGetLastError();
 }
 
+// Opt-in to k_sq_fused's dynamic shared memory (61 KB for FP64), once per device.
+template <typename T, bool EPI>
+cudaError_t sq_fused_attr()  // the SC instantiation
+{
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if ((done.load() >> dev) & 1ull) return cudaSuccess;
+    e = cudaFuncSetAttribute(k_sq_fused<T, EPI, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(sqtile::CoefSmem<T>));
+    if (e == cudaSuccess) done.fetch_or(1ull << dev);
+    return e;
+}
+
 template <typename T>
 cudaError_t run_sq_fused(const Lattice& L, const T* u, const T* Kn, const T* Tv, const CoefLayout& cl,
                          const Batch& bt, T* out, const MvEpilogue* ep, cudaStream_t st)
@@ -305,16 +344,32 @@ cudaError_t run_sq_fused(const Lattice& L, const T* u, const T* Kn, const T* Tv,
     }
     const bool epi = ep && (ep->mask || ep->dot_part);
     const int* act = ep ? ep->act : nullptr;
+    const bool sc = cl.slot_stride == 1;  // reference layout: coefficients staged in shared memory
+    if (sc) {
+        cudaError_t e = epi ? sq_fused_attr<T, true>() : sq_fused_attr<T, false>();
+        if (e != cudaSuccess) return e;
+    }
+    const size_t smem = sc ? sizeof(sqtile::CoefSmem<T>) : 0;
     const dim3 grid(sqtile::tiles_x(L.nx), sqtile::tiles_y(L.ny), 1);
     for (int s0 = 0; s0 < bt.nsys; s0 += 65535) {
         dim3 g = grid;
         g.z = bt.nsys - s0 < 65535 ? bt.nsys - s0 : 65535;
-        if (epi)
-            k_sq_fused<T, true><<<g, sqtile::NT, 0, st>>>(L.nx, L.ny, L.N, s0, u, Kn, Tv, cl, bt, out, ep->mask,
-                                                          ep->dot_part, ep->dot_final, ep->counter, act);
+        const uint8_t* mk = epi ? ep->mask : nullptr;
+        double* dp = epi ? ep->dot_part : nullptr;
+        double* df = epi ? ep->dot_final : nullptr;
+        unsigned* ct = epi ? ep->counter : nullptr;
+        if (epi && sc)
+            k_sq_fused<T, true, true><<<g, sqtile::NT, smem, st>>>(L.nx, L.ny, L.N, s0, u, Kn, Tv, cl, bt, out, mk, dp,
+                                                                   df, ct, act);
+        else if (epi)
+            k_sq_fused<T, true, false><<<g, sqtile::NT, 0, st>>>(L.nx, L.ny, L.N, s0, u, Kn, Tv, cl, bt, out, mk, dp,
+                                                                 df, ct, act);
+        else if (sc)
+            k_sq_fused<T, false, true><<<g, sqtile::NT, smem, st>>>(L.nx, L.ny, L.N, s0, u, Kn, Tv, cl, bt, out,
+                                                                    nullptr, nullptr, nullptr, nullptr, act);
         else
-            k_sq_fused<T, false><<<g, sqtile::NT, 0, st>>>(L.nx, L.ny, L.N, s0, u, Kn, Tv, cl, bt, out, nullptr,
-                                                           nullptr, nullptr, nullptr, act);
+            k_sq_fused<T, false, false><<<g, sqtile::NT, 0, st>>>(L.nx, L.ny, L.N, s0, u, Kn, Tv, cl, bt, out,
+                                                                  nullptr, nullptr, nullptr, nullptr, act);
     }
     return cudaGetLastError();
 }

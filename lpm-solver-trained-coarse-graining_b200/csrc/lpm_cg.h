@@ -100,7 +100,7 @@ int cg_solve(const Lattice& L, const T* Kn, const T* Tv, const CoefLayout& cl, c
 // Sets the bound of one team-barrier wait of the persistent engine (ns, process-wide); returns the previous bound.
 unsigned long long persist_wait_limit(unsigned long long ns);
 bool persist_fits(const Lattice& L, const Batch& bt);
-bool persist_auto(const Lattice& L, const Batch& bt);
+bool persist_auto(const Lattice& L, const Batch& bt, int elem_bytes);
 size_t persist_workspace_bytes(const Lattice& L, const Batch& bt, int elem_bytes);
 template <typename T>
 int cg_solve_persist(const Lattice& L, const T* Kn, const T* Tv, const CoefLayout& cl, const Batch& bt,

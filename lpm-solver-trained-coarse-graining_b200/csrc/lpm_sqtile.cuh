@@ -134,19 +134,44 @@ __device__ __forceinline__ void forces(int nx, int ny, int x0, int y0, const KNA
     emit(i, f, ui);
 }
 
-// Stage the coefficients of the tile and its 1-site ring (slot-major, zero outside the box) for SharedCoef.
+// Stage the coefficients of the tile and its 1-site ring (slot-major, zero outside the box) for SharedCoef.  The
+// reads run along the contiguous direction of the layout: in the packed layout (unit site stride) a ring row of one
+// slot is contiguous; in the reference layout (unit slot stride) a ring row's slots are, site after site, so
+// consecutive threads take consecutive slots of a site.
 template <typename T>
 __device__ __forceinline__ void stage_coef(int nx, int ny, int x0, int y0, const T* __restrict__ c,
                                            const CoefLayout& cl, T* sc)
 {
-    for (int e = threadIdx.x; e < 8 * SH * SW; e += NT) {
-        const int k = e / (SH * SW), r = e - k * (SH * SW);
-        const int gx = x0 - 1 + r % SW, gy = y0 - 1 + r / SW;
-        sc[e] = (gx >= 0 && gx < nx && gy >= 0 && gy < ny)
-                    ? c[((int64_t)gy * nx + gx) * cl.site_stride + k * cl.slot_stride]
-                    : T(0);
+    if (cl.slot_stride == 1) {
+#pragma unroll 4
+        for (int e = threadIdx.x; e < 8 * SH * SW; e += NT) {
+            const int ly = e / (8 * SW), rem = e - ly * (8 * SW);
+            const int lx = rem >> 3, k = rem & 7;
+            const int gx = x0 - 1 + lx, gy = y0 - 1 + ly;
+            sc[k * (SH * SW) + ly * SW + lx] = (gx >= 0 && gx < nx && gy >= 0 && gy < ny)
+                                                   ? c[((int64_t)gy * nx + gx) * cl.site_stride + k]
+                                                   : T(0);
+        }
+    } else {
+#pragma unroll 4
+        for (int e = threadIdx.x; e < 8 * SH * SW; e += NT) {
+            const int k = e / (SH * SW), r = e - k * (SH * SW);
+            const int gx = x0 - 1 + r % SW, gy = y0 - 1 + r / SW;
+            sc[e] = (gx >= 0 && gx < nx && gy >= 0 && gy < ny)
+                        ? c[((int64_t)gy * nx + gx) * cl.site_stride + k * cl.slot_stride]
+                        : T(0);
+        }
     }
 }
+
+// Shared memory of a tile with both coefficient arrays staged (k_sq_fused): the displacement / shell-sum tile, then
+// Kn and Tv of the tile and its ring, slot-major.
+template <typename T>
+struct CoefSmem {
+    Smem<T> t;
+    T kn[8 * SH * SW];
+    T tv[8 * SH * SW];
+};
 
 }  // namespace sqtile
 }  // namespace lpm

@@ -125,3 +125,39 @@ def test_packed_cg_2d_partial_last_set(dt):
         assert rel_l2(xs[0][s], ref[s]) < bar, (dt, s, rel_l2(xs[0][s], ref[s]))
         # same arithmetic per system either way; FP32 CG may amplify last-bit differences of contracted products
         assert rel_l2(xs[0][s], xs[1][s]) < (1e-12 if dt == "f64" else 1e-5), (dt, s, rel_l2(xs[0][s], xs[1][s]))
+
+
+@pytest.mark.parametrize("dt", ["f64", "f32"])
+def test_cg_2d_reference_layout_staged(dt):
+    """Square-lattice CG on reference-layout coefficients without packing (the operator stages both coefficient
+    arrays of each tile in shared memory) against the same solve on packed coefficients and against the oracle."""
+    nx, ny = 45, 30
+    lat = G.Lattice2D("square", nx, ny, 1.0)
+    dl = core.DeviceLattice(lat)
+    ph = np.random.default_rng(4).random(lat.N) < 0.3
+    C = G.iso_C2d(np.where(ph, 10.0, 1.0), 0.25, plane="stress")
+    k, t = G.bond_params_two_end_mean(lat, G.square_params_from_C(C))
+    fr, b, ref = [], [], []
+    for ld in ("tb_ty", "lr_tx"):
+        fixed, up, _ = G.prescribed2d(ld, lat.x, lat.ij, nx, ny, 1, 1.0)
+        fd = np.repeat(fixed[:, None], 2, axis=1)
+        upm = np.where(fd, up, 0.0)
+        fr.append(~fd)
+        b.append(-O.sq_kmv(lat, upm.ravel(), k, t).reshape(-1, 2) * ~fd)
+        ref.append(O.sq_solve_cg(lat, k, t, fd, upm, tol=1e-12)[0] - upm)
+    tdt = torch.float64 if dt == "f64" else torch.float32
+    Kd = torch.as_tensor(k, device=DEV, dtype=tdt)[None]
+    Td = torch.as_tensor(t, device=DEV, dtype=tdt)[None]
+    bd = torch.as_tensor(np.array(b), device=DEV, dtype=tdt)
+    fd_ = torch.as_tensor(np.array(fr), device=DEV, dtype=tdt)
+    tol = 1e-10 if dt == "f64" else 1e-6
+    xs = []
+    for pk in (False, True):
+        x, info = core.cg(dl, Kd, Td, bd, free=fd_, tol=tol, maxit=20000, check=1, engine=L.ENGINE_LAUNCHED,
+                          pack2d=pk)
+        assert (info.status == 0).all()
+        xs.append(x.double().cpu().numpy())
+    bar = 1e-7 if dt == "f64" else 1e-4
+    for s in range(2):
+        assert rel_l2(xs[0][s], ref[s]) < bar, (dt, s, rel_l2(xs[0][s], ref[s]))
+        assert rel_l2(xs[0][s], xs[1][s]) < (1e-12 if dt == "f64" else 1e-5), (dt, s)

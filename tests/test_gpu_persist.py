@@ -59,7 +59,7 @@ def test_persistent_2d_plain_fp64_cfg1_shape():
     dl = core.DeviceLattice(lat)
     free = T(~fixed)
     b = -core.kmv(dl, T(up)[None].expand(3, -1, -1), T(Kn), T(Tv)) * free
-    assert L.load().lpm_cg_persistent_fits(dl.ref, core._batch(3, 1, 1)) == 1
+    assert L.load().lpm_cg_persistent_fits(dl.ref, core._batch(3, 1, 1), L.LPM_F64) == 1
     xa, ia, xp, ip = both(dl, T(Kn), T(Tv), b, free=free, tol=1e-10, maxit=100000, check=1, precheck=True)
     assert (ia.status == 0).all() and (ip.status == 0).all() and (ip.relres <= 1e-10).all()
     assert close_iters(ia, ip)
