@@ -123,6 +123,7 @@ __global__ void __launch_bounds__(VB) k_cg_init(int64_t N, int sys0, Batch bt, c
     sc.bn[s] = bn;
     sc.rz[s] = tot[1];
     sc.rr[s] = tot[2];
+    sc.beta[s] = 0.0;  // the fused p-update's first p' = z + 0 p
     sc.act[s] = act;
     sc.iters[s] = 0;
     sc.relres[s] = rel;
@@ -131,19 +132,24 @@ __global__ void __launch_bounds__(VB) k_cg_init(int64_t N, int sys0, Batch bt, c
 }
 
 // ----------------------------------------------------------------------------------------------------- update
-template <typename T, int DIM, bool PREC>
+// PF (fused p-update, full 2D boxes): the operator formed p' = z + beta p into one of the buffers p / p1 by the
+// parity of pk[s], the system's count of completed iterations; this kernel reads p' from there, takes its iteration
+// number from pk[s], and its last block advances pk[s] (every block of the system has read it by then).
+template <typename T, int DIM, bool PREC, bool PF = false>
 __global__ void __launch_bounds__(VB) k_cg_update(int64_t N, int sys0, Batch bt, int it_host, int check,
                                                   int maxit, double tol, const uint8_t* __restrict__ mask,
                                                   const T* __restrict__ Minv, T* __restrict__ x, T* __restrict__ r,
-                                                  T* __restrict__ z, const T* __restrict__ p,
-                                                  const T* __restrict__ Ap, CgScalars sc)
+                                                  T* __restrict__ z, const T* __restrict__ p0,
+                                                  const T* __restrict__ Ap, CgScalars sc,
+                                                  const T* __restrict__ p1 = nullptr, int* __restrict__ pk = nullptr)
 {
     __shared__ double sh[32];
-    const int it = sc.itp ? *sc.itp : it_host;
     const int s = sys0 + blockIdx.y;
-    const int cur = (it - 1) & 1, nxt = it & 1;
     // a frozen system: every block of it leaves before the reduction, so its counter stays at zero
     if (!sc.act[s]) return;
+    const int it = PF ? pk[s] + 1 : (sc.itp ? *sc.itp : it_host);
+    const T* __restrict__ p = PF && (pk[s] & 1) == 0 ? p1 : p0;
+    const int cur = (it - 1) & 1, nxt = it & 1;
     const double pAp = sc.pAp[s];
     const double rzc = sc.rz[cur * bt.nsys + s];
     const bool good = pAp > 0.0 && isfinite(pAp) && isfinite(rzc);
@@ -180,6 +186,7 @@ __global__ void __launch_bounds__(VB) k_cg_update(int64_t N, int sys0, Batch bt,
     }
     double tot[2];
     if (!reduce_last<2>(v, sc.part, sc.cnt, s, bt.nsys, blockIdx.x, gridDim.x, sh, tot) || threadIdx.x != 0) return;
+    if constexpr (PF) pk[s] = it;
     const double rzn = tot[0], rrn = tot[1];
     sc.rz[nxt * bt.nsys + s] = rzn;
     sc.rr[s] = rrn;
@@ -310,7 +317,16 @@ struct CgWork {
     double* mv_part;
     double* mv_final;
     unsigned* mv_cnt;
+    int* pk;  // completed iterations per system (the fused p-update's buffer parity)
 };
+
+// The fused p-update runs where the operator is k_sq_fused: full 2D boxes (FP32 batches with several systems per set
+// keep the multi-system tile kernel and the separate p-update).  Its second p buffer is the shell-sum scratch `st`,
+// which the 2D tile operator does not use.
+inline bool pfused(const Lattice& L, const Batch& bt, int elem_bytes)
+{
+    return L.dim == 2 && L.nbr == nullptr && (elem_bytes == 8 || bt.rhs_per_set == 1);
+}
 
 template <typename T>
 void carve_cg(Carver& cv, const Lattice& L, int nsys, bool precond, CgWork<T>& w)
@@ -336,6 +352,7 @@ void carve_cg(Carver& cv, const Lattice& L, int nsys, bool precond, CgWork<T>& w
     w.mv_cnt = cv.take<unsigned>(nsys);
     w.mv_final = w.sc.pAp;
     w.sc.itp = cv.take<int>(1);
+    w.pk = cv.take<int>(nsys);
 }
 
 template <typename T>
@@ -386,9 +403,18 @@ inline int update_blocks(int nb, int ns)
 
 template <typename T, int DIM>
 void launch_update(dim3 g, cudaStream_t st, bool precond, const Batch& bt, int64_t N, int s0, int it,
-                   const lpm_cg_opts& o, const uint8_t* mask, const T* Minv, T* x, CgWork<T>& w)
+                   const lpm_cg_opts& o, const uint8_t* mask, const T* Minv, T* x, CgWork<T>& w, bool pf = false)
 {
     const dim3 gu(update_blocks((int)g.x, (int)g.y), g.y);
+    if (pf) {  // p' comes from the operator: no p-update kernel
+        if (precond)
+            k_cg_update<T, DIM, true, true><<<gu, VB, 0, st>>>(N, s0, bt, it, o.check, o.maxit, o.tol, mask, Minv,
+                                                               x, w.r, w.z, w.p, w.Ap, w.sc, w.st, w.pk);
+        else
+            k_cg_update<T, DIM, false, true><<<gu, VB, 0, st>>>(N, s0, bt, it, o.check, o.maxit, o.tol, mask, Minv,
+                                                                x, w.r, w.z, w.p, w.Ap, w.sc, w.st, w.pk);
+        return;
+    }
     if (precond)
         k_cg_update<T, DIM, true><<<gu, VB, 0, st>>>(N, s0, bt, it, o.check, o.maxit, o.tol, mask, Minv, x, w.r,
                                                      w.z, w.p, w.Ap, w.sc);
@@ -473,6 +499,7 @@ int cg_solve(const Lattice& L, const T* Kn, const T* Tv, const CoefLayout& cl, c
     cudaError_t e = cudaMemsetAsync(w.sc.cnt, 0, sizeof(unsigned) * bt.nsys, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.mv_cnt, 0, sizeof(unsigned) * bt.nsys, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.sc.nconv, 0, sizeof(unsigned), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w.pk, 0, sizeof(int) * bt.nsys, st);
     if (e != cudaSuccess) return (int)e;
     if (!x_is_zero) {
         e = launch_kmv<T>(L, x, Kn, Tv, cl, bt, w.Ap, w.st, nullptr, st);
@@ -491,6 +518,14 @@ int cg_solve(const Lattice& L, const T* Kn, const T* Tv, const CoefLayout& cl, c
     if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
 
     MvEpilogue ep{mask, w.mv_part, w.mv_final, w.mv_cnt, w.sc.act};
+    const bool pf = pfused(L, bt, (int)sizeof(T));
+    if (pf) {
+        ep.pz = precond ? w.z : w.r;
+        ep.p0 = w.p;
+        ep.p1 = w.st;
+        ep.beta = w.sc.beta;
+        ep.pk = w.pk;
+    }
     KmvTimer timer(o.prof, st);
     unsigned nconv = 0;
     e = cudaMemcpyAsync(&nconv, w.sc.nconv, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
@@ -509,7 +544,7 @@ int cg_solve(const Lattice& L, const T* Kn, const T* Tv, const CoefLayout& cl, c
             if (L.dim == 3)
                 launch_update<T, 3>(g, s, precond, bt, N, s0, it, o, mask, Minv, x, w);
             else
-                launch_update<T, 2>(g, s, precond, bt, N, s0, it, o, mask, Minv, x, w);
+                launch_update<T, 2>(g, s, precond, bt, N, s0, it, o, mask, Minv, x, w, pf);
         }
         return cudaGetLastError();
     };

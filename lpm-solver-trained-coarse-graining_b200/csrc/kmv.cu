@@ -118,6 +118,16 @@ __global__ void __launch_bounds__(256) k_apply(NB nb, int nx, int ny, int nz, in
     }
 }
 
+// Kernel-side view of the fused CG p-update of MvEpilogue.
+template <typename T>
+struct PUpdate {
+    const T* z;
+    T* p0;  // read as the previous p, written as p' (the other buffer) by the tile's own sites
+    T* p1;
+    const double* beta;
+    const int* pk;
+};
+
 // Full 2D boxes: both passes in one kernel (lpm_sqtile.cuh), one 32 x 8 tile of one system per block.  SC: the
 // tile's Kn and Tv (tile + ring) are staged in shared memory with the displacements, in one phase with coalesced
 // reads, and the shell sums and forces read no global memory; taken for the reference layout, whose per-site slot
@@ -125,13 +135,14 @@ __global__ void __launch_bounds__(256) k_apply(NB nb, int nx, int ny, int nz, in
 // per-slot reads are contiguous) the coefficients are read from global memory / L1 in the passes, which keeps the
 // block at 18 KB of shared memory (FP64) and the SM at five blocks.  The optional epilogue masks the output and
 // reduces u.out per system like k_apply (same block numbering).
-template <typename T, bool EPI, bool SC>
+template <typename T, bool EPI, bool SC, bool PF>
 __global__ void __launch_bounds__(sqtile::NT) k_sq_fused(int nx, int ny, int64_t N, int sys0, const T* __restrict__ u,
                                                          const T* __restrict__ Kn, const T* __restrict__ Tv,
                                                          CoefLayout cl, Batch bt, T* __restrict__ out,
                                                          const uint8_t* __restrict__ mask, double* __restrict__ part,
                                                          double* __restrict__ dot_final,
-                                                         unsigned* __restrict__ counter, const int* __restrict__ act)
+                                                         unsigned* __restrict__ counter, const int* __restrict__ act,
+                                                         PUpdate<T> pu)
 {
     extern __shared__ __align__(16) unsigned char sq_dyn[];
     __shared__ std::conditional_t<SC, char, sqtile::Smem<T>> sm_static;
@@ -143,11 +154,21 @@ __global__ void __launch_bounds__(sqtile::NT) k_sq_fused(int nx, int ny, int64_t
     const int s = sys0 + blockIdx.z;
     if (act && !act[s]) return;
     const int x0 = blockIdx.x * sqtile::TX, y0 = blockIdx.y * sqtile::TY;
-    const T* us = u + (int64_t)s * N * 2;
     const int64_t cbase = (int64_t)(s / bt.rhs_per_set) * cl.set_stride;
+    // PF: p' = z + beta p from the previous p buffer; p' of the own sites goes to the other one
+    const bool odd = PF && (pu.pk[s] & 1);
+    const T* us = PF ? (odd ? pu.p1 : pu.p0) + (int64_t)s * N * 2 : u + (int64_t)s * N * 2;
+    const T* zs = PF ? pu.z + (int64_t)s * N * 2 : nullptr;
+    T* pn = PF ? (odd ? pu.p0 : pu.p1) + (int64_t)s * N * 2 : nullptr;
+    const T be = PF ? (T)pu.beta[s] : T(0);
     auto load = [&](int64_t q, T* v) {
-        v[0] = us[2 * q];
-        v[1] = us[2 * q + 1];
+        if constexpr (PF) {
+            v[0] = zs[2 * q] + be * us[2 * q];
+            v[1] = zs[2 * q + 1] + be * us[2 * q + 1];
+        } else {
+            v[0] = us[2 * q];
+            v[1] = us[2 * q + 1];
+        }
     };
     using KA = std::conditional_t<SC, sqtile::SharedCoef<T>, sqtile::GlobalCoef<T>>;
     KA kn, tv;
@@ -175,6 +196,10 @@ __global__ void __launch_bounds__(sqtile::NT) k_sq_fused(int nx, int ny, int64_t
         T* o = out + ((int64_t)s * N + i) * 2;
         o[0] = f[0];
         o[1] = f[1];
+        if constexpr (PF) {
+            pn[2 * i] = ui[0];
+            pn[2 * i + 1] = ui[1];
+        }
         dot += (double)ui[0] * (double)f[0] + (double)ui[1] * (double)f[1];
     });
     if constexpr (EPI) {
@@ -319,7 +344,7 @@ cudaError_t run_sq_multi(const Lattice& L, const T* u, const T* Kn, const T* Tv,
 }
 
 // Opt-in to k_sq_fused's dynamic shared memory (61 KB for FP64), once per device.
-template <typename T, bool EPI>
+template <typename T, bool EPI, bool PF>
 cudaError_t sq_fused_attr()  // the SC instantiation
 {
     static std::atomic<unsigned long long> done{0};
@@ -328,7 +353,7 @@ cudaError_t sq_fused_attr()  // the SC instantiation
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if ((done.load() >> dev) & 1ull) return cudaSuccess;
-    e = cudaFuncSetAttribute(k_sq_fused<T, EPI, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_sq_fused<T, EPI, true, PF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(sqtile::CoefSmem<T>));
     if (e == cudaSuccess) done.fetch_or(1ull << dev);
     return e;
@@ -340,16 +365,27 @@ cudaError_t run_sq_fused(const Lattice& L, const T* u, const T* Kn, const T* Tv,
 {
     // FP32 only: an FP64 tile's coefficients (43 KB) with its staging exceed the 48 KB of static shared memory
     if constexpr (sizeof(T) == 4) {
-        if (bt.rhs_per_set > 1) return run_sq_multi<T>(L, u, Kn, Tv, cl, bt, out, ep, st);
+        if (bt.rhs_per_set > 1 && !(ep && ep->pz)) return run_sq_multi<T>(L, u, Kn, Tv, cl, bt, out, ep, st);
     }
     const bool epi = ep && (ep->mask || ep->dot_part);
     const int* act = ep ? ep->act : nullptr;
     const bool sc = cl.slot_stride == 1;  // reference layout: coefficients staged in shared memory
+    const bool pf = ep && ep->pz;
+    if (pf && !epi) return cudaErrorInvalidValue;
     if (sc) {
-        cudaError_t e = epi ? sq_fused_attr<T, true>() : sq_fused_attr<T, false>();
+        cudaError_t e = !epi ? sq_fused_attr<T, false, false>()
+                             : (pf ? sq_fused_attr<T, true, true>() : sq_fused_attr<T, true, false>());
         if (e != cudaSuccess) return e;
     }
     const size_t smem = sc ? sizeof(sqtile::CoefSmem<T>) : 0;
+    PUpdate<T> pu{};
+    if (pf) {
+        pu.z = static_cast<const T*>(ep->pz);
+        pu.p0 = static_cast<T*>(ep->p0);
+        pu.p1 = static_cast<T*>(ep->p1);
+        pu.beta = ep->beta;
+        pu.pk = ep->pk;
+    }
     const dim3 grid(sqtile::tiles_x(L.nx), sqtile::tiles_y(L.ny), 1);
     for (int s0 = 0; s0 < bt.nsys; s0 += 65535) {
         dim3 g = grid;
@@ -358,18 +394,26 @@ cudaError_t run_sq_fused(const Lattice& L, const T* u, const T* Kn, const T* Tv,
         double* dp = epi ? ep->dot_part : nullptr;
         double* df = epi ? ep->dot_final : nullptr;
         unsigned* ct = epi ? ep->counter : nullptr;
-        if (epi && sc)
-            k_sq_fused<T, true, true><<<g, sqtile::NT, smem, st>>>(L.nx, L.ny, L.N, s0, u, Kn, Tv, cl, bt, out, mk, dp,
-                                                                   df, ct, act);
-        else if (epi)
-            k_sq_fused<T, true, false><<<g, sqtile::NT, 0, st>>>(L.nx, L.ny, L.N, s0, u, Kn, Tv, cl, bt, out, mk, dp,
-                                                                 df, ct, act);
-        else if (sc)
-            k_sq_fused<T, false, true><<<g, sqtile::NT, smem, st>>>(L.nx, L.ny, L.N, s0, u, Kn, Tv, cl, bt, out,
-                                                                    nullptr, nullptr, nullptr, nullptr, act);
-        else
-            k_sq_fused<T, false, false><<<g, sqtile::NT, 0, st>>>(L.nx, L.ny, L.N, s0, u, Kn, Tv, cl, bt, out,
-                                                                  nullptr, nullptr, nullptr, nullptr, act);
+#define LPM_SQ_LAUNCH(E, S, P)                                                                                    \
+    k_sq_fused<T, E, S, P><<<g, sqtile::NT, S ? smem : 0, st>>>(L.nx, L.ny, L.N, s0, u, Kn, Tv, cl, bt, out, mk, dp, \
+                                                               df, ct, act, pu)
+        if (!epi) {
+            if (sc)
+                LPM_SQ_LAUNCH(false, true, false);
+            else
+                LPM_SQ_LAUNCH(false, false, false);
+        } else if (pf) {
+            if (sc)
+                LPM_SQ_LAUNCH(true, true, true);
+            else
+                LPM_SQ_LAUNCH(true, false, true);
+        } else {
+            if (sc)
+                LPM_SQ_LAUNCH(true, true, false);
+            else
+                LPM_SQ_LAUNCH(true, false, false);
+        }
+#undef LPM_SQ_LAUNCH
     }
     return cudaGetLastError();
 }
@@ -379,6 +423,7 @@ cudaError_t run_kmv(NB nb, const Lattice& L, const T* u, const T* Kn, const T* T
                     const Batch& bt, T* out, T* scratch, const MvEpilogue* ep, cudaStream_t st)
 {
     if constexpr (DIM == 2 && NB::structured) return run_sq_fused<T>(L, u, Kn, Tv, cl, bt, out, ep, st);
+    if (ep && ep->pz) return cudaErrorNotSupported;  // the fused p-update exists for full 2D boxes only
     const int nz = DIM == 3 ? L.nz : 1;
     const bool epi = ep && (ep->mask || ep->dot_part);  // act alone needs no epilogue
     int chunk, nblk;
