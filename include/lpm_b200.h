@@ -165,7 +165,7 @@ int lpm_cg_batched_f32(const lpm_lattice* lat, const float* Kn, const float* Tv,
                        int32_t* iters, double* relres, int32_t* status, void* stream);
 
 /* 1 if the automatic engine choice runs this batch in `precision` (LPM_F64 / LPM_F32) on the persistent engine:
- * square-lattice batches of at most 2^17 (FP64) or 2^19 (FP32) particle-systems that fit on teams of co-resident
+ * square-lattice batches of at most 2^17 particle-systems (either precision) that fit on teams of co-resident
  * blocks (every system's particles on one team).  The persistent engine keeps the launched engine's algorithm, tests and
  * freezing (same iteration counts up to the rounding of its reductions) and runs one cooperative kernel per solve:
  * three team barriers per iteration, each wait bounded in time (LPM_ERR_TIMEOUT on expiry). */

@@ -653,16 +653,18 @@ bool persist_fits(const Lattice& L, const Batch& bt)
     return team_shape(bt.nsys, L.N, sms).nteam > 0;
 }
 
-// The automatic choice: 2D batches of up to 2^17 (FP64) or 2^19 (FP32) particle-systems.  Plain CG per iteration on
-// one B200, packed coefficients, persistent vs launched: FP64 14.6 vs 22.9 us at 4 x 128^2, 30.3 vs 26.0 at
-// 10 x 128^2, 131 vs 88 at 40 x 128^2; FP32 24.3 vs 26.7 at 10 x 128^2, 54.1 vs 54.3 at 40 x 128^2, 119 vs 98 at
-// 16 x 256^2.  A persistent block takes its team's tiles one after another, while the launched operator has every
-// tile of the batch in flight.  (3D: the operator's fused TMA kernels are faster than the persistent kernel's
+// The automatic choice: 2D batches of up to 2^17 particle-systems (the precision is kept in the interface; both
+// thresholds are 2^17 today).  Plain CG per iteration on one B200, packed coefficients, persistent vs launched (the
+// launched operator forming the p-update): FP64 15.0 vs 21.5 us at 4 x 128^2, 31.7 vs 24.8 at 10 x 128^2, 132 vs 86
+// at 40 x 128^2; FP32 14.5 vs 18.7 at 4 x 128^2, 24.7 vs 23.9 at 10 x 128^2, 23.8 vs 20.8 at 40 x 64^2.  A
+// persistent block takes its team's tiles one after another, while the launched operator has every tile of the
+// batch in flight.  (3D: the operator's fused TMA kernels are faster than the persistent kernel's
 // per-particle passes at every size measured.)
 bool persist_auto(const Lattice& L, const Batch& bt, int elem_bytes)
 {
     const int64_t units = (int64_t)bt.nsys * L.N;
-    const int64_t cap = (int64_t)1 << (elem_bytes == 8 ? 17 : 19);
+    (void)elem_bytes;
+    const int64_t cap = (int64_t)1 << 17;
     return L.dim == 2 && units <= cap && persist_fits(L, bt);
 }
 

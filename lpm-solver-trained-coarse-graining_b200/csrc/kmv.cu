@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(sqtile::NT) k_sq_fused(int nx, int ny, int64_t
             v[1] = us[2 * q + 1];
         }
     };
-    using KA = std::conditional_t<SC, sqtile::SharedCoef<T>, sqtile::GlobalCoef<T>>;
+    using KA = std::conditional_t<SC, sqtile::SharedCoef<T>, sqtile::SoaCoef<T>>;
     KA kn, tv;
     if constexpr (SC) {
         sqtile::stage(nx, ny, x0, y0, load, sm);
@@ -180,8 +180,8 @@ __global__ void __launch_bounds__(sqtile::NT) k_sq_fused(int nx, int ny, int64_t
         tv = KA{cs.tv};
     } else {
         sqtile::stage(nx, ny, x0, y0, load, sm);
-        kn = KA{Kn + cbase, cl, nx, x0, y0};
-        tv = KA{Tv + cbase, cl, nx, x0, y0};
+        kn = KA(Kn + cbase, cl.slot_stride, nx, x0, y0);
+        tv = KA(Tv + cbase, cl.slot_stride, nx, x0, y0);
     }
     __syncthreads();
     sqtile::sums(nx, ny, x0, y0, tv, sm);
@@ -369,7 +369,7 @@ cudaError_t run_sq_fused(const Lattice& L, const T* u, const T* Kn, const T* Tv,
     }
     const bool epi = ep && (ep->mask || ep->dot_part);
     const int* act = ep ? ep->act : nullptr;
-    const bool sc = cl.slot_stride == 1;  // reference layout: coefficients staged in shared memory
+    const bool sc = cl.site_stride != 1;  // all but the packed layout: coefficients staged in shared memory
     const bool pf = ep && ep->pz;
     if (pf && !epi) return cudaErrorInvalidValue;
     if (sc) {

@@ -54,6 +54,20 @@ struct GlobalCoef {  // a coefficient set in global memory (any layout)
     }
 };
 template <typename T>
+struct SoaCoef {  // the packed layout in global memory: slot k of site q at c[k * N + q]
+    const T* c;
+    int64_t N;
+    int64_t o0;  // site index of ring coordinates (0, 0), (y0 - 1) * nx + x0 - 1 (negative on the first row)
+    int nx;
+    __device__ __forceinline__ SoaCoef() = default;
+    __device__ __forceinline__ SoaCoef(const T* c_, int64_t N_, int nx_, int x0, int y0)
+        : c(c_), N(N_), o0((int64_t)(y0 - 1) * nx_ + (x0 - 1)), nx(nx_)
+    {
+    }
+    // the site part in 32 bits (ly * nx + lx < 2^31 for any box the library accepts) and one 64-bit slot offset
+    __device__ __forceinline__ T operator()(int lx, int ly, int k) const { return c[o0 + (ly * nx + lx) + k * N]; }
+};
+template <typename T>
 struct SharedCoef {  // the ring region's coefficients staged in shared memory, slot-major
     const T* c;
     __device__ __forceinline__ T operator()(int lx, int ly, int k) const { return c[k * (SH * SW) + ly * SW + lx]; }
