@@ -320,12 +320,13 @@ struct CgWork {
     int* pk;  // completed iterations per system (the fused p-update's buffer parity)
 };
 
-// The fused p-update runs where the operator is k_sq_fused: full 2D boxes (FP32 batches with several systems per set
-// keep the multi-system tile kernel and the separate p-update).  Its second p buffer is the shell-sum scratch `st`,
-// which the 2D tile operator does not use.
+// The fused p-update runs where the operator is a 2D tile kernel (k_sq_fused, k_sq_multi): full 2D boxes.  Its
+// second p buffer is the shell-sum scratch `st`, which the 2D tile operators do not use.
 inline bool pfused(const Lattice& L, const Batch& bt, int elem_bytes)
 {
-    return L.dim == 2 && L.nbr == nullptr && (elem_bytes == 8 || bt.rhs_per_set == 1);
+    (void)bt;
+    (void)elem_bytes;
+    return L.dim == 2 && L.nbr == nullptr;
 }
 
 template <typename T>

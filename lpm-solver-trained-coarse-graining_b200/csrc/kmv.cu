@@ -233,13 +233,15 @@ __global__ void __launch_bounds__(sqtile::NT) k_sq_fused(int nx, int ny, int64_t
 // coefficients cross L2 once per tile instead of once per system.  Same arithmetic, output, epilogue and block
 // numbering as k_sq_fused.  (Splitting a set's systems over more blocks, each staging the coefficients again, was
 // slower: 0.065 -> 0.091 ms for six systems on a 512^2 box.)
-template <typename T, bool EPI>
+// PF: the fused CG p-update of k_sq_fused, per system of the set.
+template <typename T, bool EPI, bool PF = false>
 __global__ void __launch_bounds__(sqtile::NT) k_sq_multi(int nx, int ny, int64_t N, int set0, const T* __restrict__ u,
                                                          const T* __restrict__ Kn, const T* __restrict__ Tv,
                                                          CoefLayout cl, Batch bt, T* __restrict__ out,
                                                          const uint8_t* __restrict__ mask, double* __restrict__ part,
                                                          double* __restrict__ dot_final,
-                                                         unsigned* __restrict__ counter, const int* __restrict__ act)
+                                                         unsigned* __restrict__ counter, const int* __restrict__ act,
+                                                         PUpdate<T> pu = PUpdate<T>{})
 {
     constexpr int NC = 8 * sqtile::SH * sqtile::SW;
     __shared__ sqtile::Smem<T> sm[2];
@@ -267,13 +269,26 @@ __global__ void __launch_bounds__(sqtile::NT) k_sq_multi(int nx, int ny, int64_t
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             if (!on[h]) continue;
-            const T* us = u + (int64_t)sa[h] * N * 2;
-            sqtile::stage(nx, ny, x0, y0,
-                          [&](int64_t q, T* v) {
-                              v[0] = us[2 * q];
-                              v[1] = us[2 * q + 1];
-                          },
-                          sm[h]);
+            if constexpr (PF) {
+                const int64_t so = (int64_t)sa[h] * N * 2;
+                const T* us = ((pu.pk[sa[h]] & 1) ? pu.p1 : pu.p0) + so;
+                const T* zs = pu.z + so;
+                const T be = (T)pu.beta[sa[h]];
+                sqtile::stage(nx, ny, x0, y0,
+                              [&](int64_t q, T* v) {
+                                  v[0] = zs[2 * q] + be * us[2 * q];
+                                  v[1] = zs[2 * q + 1] + be * us[2 * q + 1];
+                              },
+                              sm[h]);
+            } else {
+                const T* us = u + (int64_t)sa[h] * N * 2;
+                sqtile::stage(nx, ny, x0, y0,
+                              [&](int64_t q, T* v) {
+                                  v[0] = us[2 * q];
+                                  v[1] = us[2 * q + 1];
+                              },
+                              sm[h]);
+            }
         }
         __syncthreads();
 #pragma unroll
@@ -285,6 +300,7 @@ __global__ void __launch_bounds__(sqtile::NT) k_sq_multi(int nx, int ny, int64_t
         for (int h = 0; h < 2; ++h) {
             if (!on[h]) continue;
             const int s = sa[h];
+            T* pn = PF ? ((pu.pk[s] & 1) ? pu.p0 : pu.p1) + (int64_t)s * N * 2 : nullptr;
             sqtile::forces(nx, ny, x0, y0, kn, tv, sm[h], [&](int64_t i, T (&f)[2], const T* ui) {
                 if (EPI && mask) {
                     const uint8_t* m = mask + ((int64_t)(s % bt.nmask) * N + i) * 2;
@@ -294,6 +310,10 @@ __global__ void __launch_bounds__(sqtile::NT) k_sq_multi(int nx, int ny, int64_t
                 T* o = out + ((int64_t)s * N + i) * 2;
                 o[0] = f[0];
                 o[1] = f[1];
+                if constexpr (PF) {
+                    pn[2 * i] = ui[0];
+                    pn[2 * i + 1] = ui[1];
+                }
                 dot[h] += (double)ui[0] * (double)f[0] + (double)ui[1] * (double)f[1];
             });
         }
@@ -330,10 +350,18 @@ cudaError_t run_sq_multi(const Lattice& L, const T* u, const T* Kn, const T* Tv,
 {
     const bool epi = ep && (ep->mask || ep->dot_part);
     const int* act = ep ? ep->act : nullptr;
+    const bool pf = ep && ep->pz;
+    if (pf && !epi) return cudaErrorInvalidValue;
     const int nset = (bt.nsys + bt.rhs_per_set - 1) / bt.rhs_per_set;
     for (int c0 = 0; c0 < nset; c0 += 65535) {
         const dim3 g(sqtile::tiles_x(L.nx), sqtile::tiles_y(L.ny), nset - c0 < 65535 ? nset - c0 : 65535);
-        if (epi)
+        if (pf) {
+            PUpdate<T> pu{static_cast<const T*>(ep->pz), static_cast<T*>(ep->p0), static_cast<T*>(ep->p1), ep->beta,
+                          ep->pk};
+            k_sq_multi<T, true, true><<<g, sqtile::NT, 0, st>>>(L.nx, L.ny, L.N, c0, u, Kn, Tv, cl, bt, out,
+                                                                ep->mask, ep->dot_part, ep->dot_final, ep->counter,
+                                                                act, pu);
+        } else if (epi)
             k_sq_multi<T, true><<<g, sqtile::NT, 0, st>>>(L.nx, L.ny, L.N, c0, u, Kn, Tv, cl, bt, out, ep->mask,
                                                           ep->dot_part, ep->dot_final, ep->counter, act);
         else
@@ -365,7 +393,7 @@ cudaError_t run_sq_fused(const Lattice& L, const T* u, const T* Kn, const T* Tv,
 {
     // FP32 only: an FP64 tile's coefficients (43 KB) with its staging exceed the 48 KB of static shared memory
     if constexpr (sizeof(T) == 4) {
-        if (bt.rhs_per_set > 1 && !(ep && ep->pz)) return run_sq_multi<T>(L, u, Kn, Tv, cl, bt, out, ep, st);
+        if (bt.rhs_per_set > 1) return run_sq_multi<T>(L, u, Kn, Tv, cl, bt, out, ep, st);
     }
     const bool epi = ep && (ep->mask || ep->dot_part);
     const int* act = ep ? ep->act : nullptr;

@@ -28,8 +28,8 @@ struct MvEpilogue {
     double* dot_final;
     unsigned* counter;
     const int* act;       // optional per-system activity flags: inactive systems are skipped (output untouched)
-    // Optional fused CG p-update (full 2D boxes through k_sq_fused; the launcher reports cudaErrorNotSupported
-    // elsewhere): the operator's input is p' = z + beta[s] p, formed while staging the tile, with p and p' in the two
+    // Optional fused CG p-update (full 2D boxes through the 2D tile kernels; the launcher reports
+    // cudaErrorNotSupported elsewhere): the operator's input is p' = z + beta[s] p, formed while staging the tile, with p and p' in the two
     // buffers p0 / p1 (the previous p in p0 when pk[s] is even), and p' of the tile's own sites is stored.  The
     // input pointer u of the launch is then unused.
     const void* pz = nullptr;      // z (r for plain CG), (nsys, N, d)
