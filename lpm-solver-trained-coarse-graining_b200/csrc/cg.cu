@@ -322,12 +322,7 @@ struct CgWork {
 
 // The fused p-update runs where the operator is a 2D tile kernel (k_sq_fused, k_sq_multi): full 2D boxes.  Its
 // second p buffer is the shell-sum scratch `st`, which the 2D tile operators do not use.
-inline bool pfused(const Lattice& L, const Batch& bt, int elem_bytes)
-{
-    (void)bt;
-    (void)elem_bytes;
-    return L.dim == 2 && L.nbr == nullptr;
-}
+inline bool pfused(const Lattice& L) { return L.dim == 2 && L.nbr == nullptr; }
 
 template <typename T>
 void carve_cg(Carver& cv, const Lattice& L, int nsys, bool precond, CgWork<T>& w)
@@ -519,7 +514,7 @@ int cg_solve(const Lattice& L, const T* Kn, const T* Tv, const CoefLayout& cl, c
     if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
 
     MvEpilogue ep{mask, w.mv_part, w.mv_final, w.mv_cnt, w.sc.act};
-    const bool pf = pfused(L, bt, (int)sizeof(T));
+    const bool pf = pfused(L);
     if (pf) {
         ep.pz = precond ? w.z : w.r;
         ep.p0 = w.p;
