@@ -41,21 +41,43 @@ __device__ __forceinline__ void block_mv(const T* __restrict__ M, const T* r, T*
     }
 }
 
+// Block sums of NV values at once: the arithmetic of block_sum (a shuffle tree per warp, then one over the warp
+// sums) for each value, with one pair of barriers for all of them; results valid in thread 0.
+template <int NV>
+__device__ __forceinline__ void block_sum_n(double (&v)[NV], double* sh)
+{
+    const int tid = threadIdx.x, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) v[j] = warp_sum(v[j]);
+    __syncthreads();  // sh is no longer read by an earlier reduction
+    if ((tid & 31) == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) sh[j * 32 + (tid >> 5)] = v[j];
+    }
+    __syncthreads();
+    if (tid < 32) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) v[j] = warp_sum(tid < nw ? sh[j * 32 + tid] : 0.0);
+    }
+}
+
 // Deterministic reduction of NV per-thread values per system.  Every block writes its NV block sums to
 // part[(j*nsys + s)*nblk + b]; the last block of system s (one counter per system) sums the rows in fixed order.
 // Returns true in that block; totals valid in thread 0.
 template <int NV>
 __device__ __forceinline__ bool reduce_last(const double (&v)[NV], double* part, unsigned* cnt, int s, int nsys,
-                                            int b, int nblk, double* sh, double (&tot)[NV])
+                                            int b, int nblk, double (&tot)[NV])
 {
     __shared__ bool is_last;
+    __shared__ double shn[NV * 32];
     const int tid = threadIdx.x;
+    double bs[NV];
 #pragma unroll
-    for (int j = 0; j < NV; ++j) {
-        const double bs = block_sum(v[j], sh);
-        if (tid == 0) part[((int64_t)j * nsys + s) * nblk + b] = bs;
-    }
+    for (int j = 0; j < NV; ++j) bs[j] = v[j];
+    block_sum_n<NV>(bs, shn);
     if (tid == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) part[((int64_t)j * nsys + s) * nblk + b] = bs[j];
         __threadfence();
         is_last = atomicAdd(cnt + s, 1u) == (unsigned)(nblk - 1);
     }
@@ -66,8 +88,9 @@ __device__ __forceinline__ bool reduce_last(const double (&v)[NV], double* part,
         double acc = 0.0;
         const double* row = part + ((int64_t)j * nsys + s) * nblk;
         for (int k = tid; k < nblk; k += blockDim.x) acc += __ldcg(row + k);
-        tot[j] = block_sum(acc, sh);
+        tot[j] = acc;
     }
+    block_sum_n<NV>(tot, shn);
     if (tid == 0) cnt[s] = 0u;
     return true;
 }
@@ -79,7 +102,6 @@ __global__ void __launch_bounds__(VB) k_cg_init(int64_t N, int sys0, Batch bt, c
                                                 const T* __restrict__ Minv, T* __restrict__ r, T* __restrict__ z,
                                                 T* __restrict__ p, CgScalars sc, double tol, int precheck)
 {
-    __shared__ double sh[32];
     const int s = sys0 + blockIdx.y;
     const int64_t i = (int64_t)blockIdx.x * VB + threadIdx.x;
     double v[3] = {0.0, 0.0, 0.0};  // b.b, r.z, r.r
@@ -114,7 +136,7 @@ __global__ void __launch_bounds__(VB) k_cg_init(int64_t N, int sys0, Batch bt, c
         }
     }
     double tot[3];
-    if (!reduce_last<3>(v, sc.part, sc.cnt, s, bt.nsys, blockIdx.x, gridDim.x, sh, tot) || threadIdx.x != 0) return;
+    if (!reduce_last<3>(v, sc.part, sc.cnt, s, bt.nsys, blockIdx.x, gridDim.x, tot) || threadIdx.x != 0) return;
     const double bn = sqrt(tot[0]);
     const double rel = bn > 0.0 ? sqrt(tot[2]) / bn : 0.0;
     const bool finite = isfinite(bn) && isfinite(tot[1]) && isfinite(tot[2]);
@@ -143,7 +165,6 @@ __global__ void __launch_bounds__(VB) k_cg_update(int64_t N, int sys0, Batch bt,
                                                   const T* __restrict__ Ap, CgScalars sc,
                                                   const T* __restrict__ p1 = nullptr, int* __restrict__ pk = nullptr)
 {
-    __shared__ double sh[32];
     const int s = sys0 + blockIdx.y;
     // a frozen system: every block of it leaves before the reduction, so its counter stays at zero
     if (!sc.act[s]) return;
@@ -185,7 +206,7 @@ __global__ void __launch_bounds__(VB) k_cg_update(int64_t N, int sys0, Batch bt,
         }
     }
     double tot[2];
-    if (!reduce_last<2>(v, sc.part, sc.cnt, s, bt.nsys, blockIdx.x, gridDim.x, sh, tot) || threadIdx.x != 0) return;
+    if (!reduce_last<2>(v, sc.part, sc.cnt, s, bt.nsys, blockIdx.x, gridDim.x, tot) || threadIdx.x != 0) return;
     if constexpr (PF) pk[s] = it;
     const double rzn = tot[0], rrn = tot[1];
     sc.rz[nxt * bt.nsys + s] = rzn;
@@ -236,7 +257,6 @@ __global__ void __launch_bounds__(VB) k_ir_residual(int64_t N, int sys0, Batch b
                                                     const uint8_t* __restrict__ mask, double* __restrict__ r,
                                                     double* part, unsigned* cnt, double* rn2, double* bn2)
 {
-    __shared__ double sh[32];
     const int s = sys0 + blockIdx.y;
     const int64_t i = (int64_t)blockIdx.x * VB + threadIdx.x;
     double v[2] = {0.0, 0.0};
@@ -254,7 +274,7 @@ __global__ void __launch_bounds__(VB) k_ir_residual(int64_t N, int sys0, Batch b
         }
     }
     double tot[2];
-    if (reduce_last<2>(v, part, cnt, s, bt.nsys, blockIdx.x, gridDim.x, sh, tot) && threadIdx.x == 0) {
+    if (reduce_last<2>(v, part, cnt, s, bt.nsys, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
         rn2[s] = tot[0];
         bn2[s] = tot[1];
     }
